@@ -1,0 +1,104 @@
+"""Pins the FP64 oracle against fixtures produced by the reference itself.
+
+The reference run and the oracle consume identical Philox variates, so switch sequences,
+counters, time and RNG call counts must agree exactly and energies to FP64 round-off."""
+import numpy as np
+import pytest
+
+from cases import build_oracle, load_fixture, load_specs, rel_err
+from oracle.philox import PhiloxStream, philox4x32_10, uniform53
+
+SPECS = load_specs()
+
+
+def test_philox_known_answers():
+    """Random123 known-answer vectors for philox4x32-10."""
+    cases = [((0, 0, 0, 0), (0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
+             ((0xffffffff,) * 4, (0xffffffff, 0xffffffff), (0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd)),
+             ((0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344), (0xa4093822, 0x299f31d0),
+              (0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1))]
+    for ctr, key, want in cases:
+        got = tuple(int(w) for w in philox4x32_10(*ctr, *key))
+        assert got == want
+
+
+def test_stream_transforms():
+    s = PhiloxStream(123)
+    u = uniform53(123, 0, 5)
+    assert np.array_equal(s.random(5), u)
+    assert s.call == 1
+    assert s.randint(10) == int(np.floor(uniform53(123, 1, 1)[0] * 10))
+    c = s.choice(7, 4)
+    assert np.array_equal(c, np.floor(uniform53(123, 2, 4) * 7).astype(np.int64))
+    e = s.exponential(scale=np.full((2, 3), 2.0), size=(2, 3))
+    assert np.allclose(e, 2.0 * -np.log1p(-uniform53(123, 3, 6).reshape(2, 3)))
+    assert np.all((u >= 0) & (u < 1))
+
+
+@pytest.mark.parametrize('name', [n for n in SPECS if not SPECS[n].get('progress')])
+def test_oracle_matches_reference(name):
+    spec, fx = SPECS[name], load_fixture(name)
+    mm = build_oracle(name, spec, fx)
+    assert np.array_equal(mm.occupation, fx['occupation'])
+    assert tuple(mm.unitcell) == tuple(fx['unitcell'])
+    assert mm.PBC == bool(fx['PBC'])
+    dip = mm.get_energy('dipolar')
+    if dip is not None:
+        assert dip.kernels.shape == fx['kernels'].shape
+        assert rel_err(dip.kernels, fx['kernels']) < 1e-13
+        assert rel_err(dip.kernels_perpself, fx['kernels_perpself']) < 1e-13
+        assert rel_err(dip.kernels_perpother, fx['kernels_perpother']) < 1e-13
+        assert np.array_equal(dip.kernel_index, fx['kernel_index'])
+        assert rel_err(dip.E, fx['E_dip_init']) < 1e-12
+        assert rel_err(dip.E_perp, fx['E_dip_perp_init']) < 1e-12
+    assert rel_err(mm.E, fx['E_init']) < 1e-12
+    sw_y, sw_x, sw_step = [], [], []
+    for s in range(spec.get('steps', 0)):
+        idx = mm.update(**spec.get('update_kw', {}))
+        if idx is not None:
+            a = np.asarray(idx).reshape(2, -1)
+            sw_y += a[0].tolist(); sw_x += a[1].tolist(); sw_step += [s] * a.shape[1]
+        assert mm.rng.call == fx['calls'][s], f'RNG call count diverged at step {s}'
+        assert mm.attempted_switches == fx['attempted'][s]
+        assert mm.switches == fx['switches'][s]
+        # t = tau * exp(b_min * beta) amplifies FP64 energy round-off by beta*|b| (~1e3)
+        assert mm.t == pytest.approx(fx["t"][s], rel=1e-9, abs=0)
+    assert np.array_equal(sw_y, fx['sw_y']) and np.array_equal(sw_x, fx['sw_x'])
+    assert np.array_equal(sw_step, fx['sw_step'])
+    assert np.array_equal(mm.m, fx['m_final'])
+    assert rel_err(mm.E, fx['E_final']) < 1e-11
+    if dip is not None:
+        assert rel_err(dip.E, fx['E_dip_final']) < 1e-11
+        assert rel_err(dip.E_perp, fx['E_dip_perp_final']) < 1e-11
+
+
+@pytest.mark.parametrize('name', [n for n in SPECS if SPECS[n].get('progress')])
+def test_oracle_progress_matches_reference(name):
+    spec, fx = SPECS[name], load_fixture(name)
+    mm = build_oracle(name, spec, fx)
+    dt, dmc = mm.progress(**spec['progress'])
+    assert dt == pytest.approx(fx["progress"][0], rel=1e-9)
+    assert dmc == pytest.approx(fx['progress'][1], rel=1e-12)
+    assert mm.rng.call == int(fx['progress_calls'])
+    assert np.array_equal(mm.m, fx['m_final'])
+    assert rel_err(mm.E, fx['E_final']) < 1e-11
+
+
+def test_hexagon_known_answer():
+    """The reference's own known-answer test (tests/test_hexagon.py): every magnet of a
+    kagome hexagon in a vortex state has E = -1e-7 m^2/a^3 (29 + 20 sqrt(3)/9)."""
+    from oracle.geometry import ip_kagome
+    from oracle.hotspice_oracle import OracleDipolar, OracleMagnets
+    z = load_fixture('hexagon_kat')
+    E_th = float(z['E_theory'])
+    l, mom = 470e-9, 1.1278401e-15
+    a = l / np.tan(30 * np.pi / 180)
+    for nx in range(5, 11):
+        for ny in range(3, 11):
+            g = ip_kagome(a, nx, ny)
+            m_ref, occ_ref, E_ref = (z[f'{nx}x{ny}_{i}'] for i in range(3))
+            g.occupation = occ_ref.astype(int)
+            dd = OracleDipolar()
+            mm = OracleMagnets(g, m_ref, T=300, moment=mom, energies=[dd], m_perp_factor=0)
+            assert np.allclose(dd.E[m_ref.astype(bool)], E_th)
+            assert rel_err(dd.E, E_ref) < 1e-12
