@@ -1,0 +1,945 @@
+"""Magnets / SimParams / Scheme with the reference API (hotspice/core.py:29-1006), running the
+kinetic Monte Carlo hot path on the sm_100a kernels of libhotspice_sm100.so.
+
+Geometry, kernels and parameter fields are prepared on the host in FP64 (as the reference
+does); the simulation state (spins, energies, counters, simulated time) lives on the GPU.
+``update()`` is the plain, one-step-per-call form (it returns the switched indices and so
+synchronises once per call). ``progress()`` runs whole chunks of steps on the device, with
+the stopping rule of hotspice/core.py:753-760 evaluated by the kernels, replayed from
+captured CUDA graphs, and synchronises only once per chunk.
+
+All random variates come from the Philox4x32-10 stream keyed by ``seed`` (one stream call
+per vectorised reference draw, see include/hotspice_b200.h), so a run is reproducible and
+comparable draw-for-draw with the reference fed the same stream.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import warnings
+from abc import ABC
+from dataclasses import dataclass, field
+from enum import Enum, auto
+from functools import lru_cache
+from textwrap import dedent
+from typing import Literal
+
+import numpy as np
+import torch
+
+from . import _lib, config
+from .energies import DipolarEnergy, Energy, ExchangeEnergy, ZeemanEnergy
+from .utils import as_2D_array, check_repetition, full_obj_name, lower_than
+
+__all__ = ['kB', 'SimParams', 'Magnets', 'Scheme', 'EngineConfig', 'Unitcell']
+
+kB = 1.380649e-23
+
+
+class Scheme(Enum):
+    NEEL = auto()
+    METROPOLIS = auto()
+    WOLFF = auto()
+
+
+@dataclass(slots=True)
+class SimParams:
+    """hotspice/core.py:34-53 (same fields, defaults and validation)."""
+    SIMULTANEOUS_SWITCHES_CONVOLUTION_OR_SUM_CUTOFF: int = 20
+    REDUCED_KERNEL_SIZE: int = 20
+    UPDATE_SCHEME: Scheme | str = Scheme.NEEL
+    MULTISAMPLING_SCHEME: Literal['single', 'grid', 'Poisson', 'cluster'] = 'grid'
+    ENERGY_BARRIER_METHOD: Literal['simple', 'parabolic'] = 'simple'
+    METROPOLIS_TIME: bool = False
+
+    def __post_init__(self):
+        self.SIMULTANEOUS_SWITCHES_CONVOLUTION_OR_SUM_CUTOFF = int(self.SIMULTANEOUS_SWITCHES_CONVOLUTION_OR_SUM_CUTOFF)
+        self.REDUCED_KERNEL_SIZE = int(self.REDUCED_KERNEL_SIZE)
+        if not isinstance(self.UPDATE_SCHEME, Scheme):
+            allowed = {'Néel': Scheme.NEEL, 'Neel': Scheme.NEEL, 'Metropolis': Scheme.METROPOLIS,
+                       'Glauber': Scheme.METROPOLIS, 'Wolff': Scheme.WOLFF}
+            if self.UPDATE_SCHEME not in allowed.keys():
+                raise ValueError(f"UPDATE_SCHEME='{self.UPDATE_SCHEME}' is invalid: allowed values are {allowed.keys()}.")
+            self.UPDATE_SCHEME = allowed[self.UPDATE_SCHEME]
+        if self.MULTISAMPLING_SCHEME not in (allowed := ['single', 'grid', 'Poisson', 'cluster']):
+            raise ValueError(f"MULTISAMPLING_SCHEME='{self.MULTISAMPLING_SCHEME}' is invalid: allowed values are {allowed}.")
+
+
+@dataclass
+class EngineConfig:
+    """Engine knobs that are not part of the reference's SimParams."""
+    resync_every: int = 0          # full dipolar recompute every N progress() steps (0: never)
+    recompute: str = 'auto'        # 'auto' | 'direct64' | 'direct32' | 'igemm'
+    direct_max_pairs: float = 4e11 # 'auto' uses the FP64 direct sum up to this many (cell, window) pairs
+    use_graphs: bool = True        # replay progress() chunks from captured CUDA graphs
+    graph_steps: int = 64          # steps per captured chunk
+    igemm_splits: int = 3          # BF16 terms of the split kernel in the implicit GEMM
+
+
+@dataclass(slots=True)
+class Unitcell:
+    x: int
+    y: int
+
+
+@dataclass
+class History:
+    E: list = field(default_factory=list)
+    T: list = field(default_factory=list)
+    t: list = field(default_factory=list)
+    m: list = field(default_factory=list)
+
+    def entry(self, mm: 'Magnets'):
+        self.E.append(mm.E_tot)
+        self.T.append(mm.T_avg)
+        self.t.append(mm.t if mm.t != 0 else mm.switches)
+        self.m.append(mm.m_avg)
+
+    def clear(self):
+        self.E.clear(); self.T.clear(); self.t.clear(); self.m.clear()
+
+
+def _ptr(t):
+    return None if t is None else t.data_ptr()
+
+
+class Magnets(ABC):
+    """hotspice/core.py:56-980. See the module docstring for what runs where."""
+
+    def __init__(self, nx: int, ny: int, dx, dy, *, T=300, E_B=0., moment=None, Msat=800e3, V=2e-22,
+                 pattern=None, energies=None, PBC: bool = False, m_perp_factor: float = None, E_B_std: float = None,
+                 major_axis: float = 0, minor_axis: float = None, angle: float = 0., params: SimParams = None,
+                 in_plane: bool = False, seed: int | None = None, engine: EngineConfig | None = None,
+                 device=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError('hotspice_b200 runs on a CUDA device (sm_100a); none is available')
+        self._lib = _lib.load()
+        if device is None:
+            device = torch.device('cuda', config.DEVICE_ID if config.DEVICE_ID is not None else torch.cuda.current_device())
+        self.device = torch.device(device)
+        self.params = SimParams() if params is None else params
+        self.engine = EngineConfig() if engine is None else engine
+        self.seed = int.from_bytes(os.urandom(8), 'little') if seed is None else int(seed) & (2 ** 64 - 1)
+        self._energies: list[Energy] = []
+        self._version = 0
+        self._L = None
+        self._graphs = {}
+        self._plans = {}
+        self._scratch = {}
+        self.in_plane = in_plane
+        self.nx, self.ny = int(nx), int(ny)
+        self.ixx, self.iyy = np.meshgrid(np.arange(self.nx), np.arange(self.ny))
+        self._dx_set(dx)
+        self._dy_set(dy)
+        self.occupation = self._get_occupation().astype(bool).astype(int)
+        with np.errstate(invalid='ignore', divide='ignore'):
+            self._occupation_inf = 1 / self.occupation
+        self.nonzero = np.nonzero(self.occupation)
+        self._nonzero_array = np.asarray(self.nonzero).reshape(2, -1)
+        self.n = int(np.sum(self.occupation))
+        if self.n == 0:
+            raise ValueError(f"Can not initialize {full_obj_name(self)} of size {self.nx}x{self.ny}, as this does not contain any spins.")
+        if self.in_plane:
+            self._initialize_ip(angle=angle)
+        self.unitcell = self._get_unitcell()
+        self._PBC = False
+        self.PBC = PBC
+        # device state
+        dev = self.device
+        self._occ_dev = torch.as_tensor(self.occupation, device=dev, dtype=torch.int8).contiguous()
+        self._nonzero_dev = torch.as_tensor(np.flatnonzero(self.occupation), device=dev, dtype=torch.int32)
+        self._m_dev = torch.zeros((self.ny, self.nx), device=dev, dtype=torch.int8)
+        self._mm_dev = torch.zeros((self.ny, self.nx), device=dev, dtype=torch.float32)
+        self._counters = torch.zeros(ctypes.sizeof(_lib.HsCounters), device=dev, dtype=torch.uint8)
+        self._orient_dev = torch.as_tensor(self.orientation, device=dev, dtype=torch.float32).contiguous() if self.in_plane else None
+        self._moment_np = np.ones((self.ny, self.nx))
+        self._mom_dev = torch.ones((self.ny, self.nx), device=dev, dtype=torch.float32)
+        self.initialize_m(self._get_groundstate() if pattern is None else pattern, update_energy=False)
+        self.T = T
+        self.E_B = E_B
+        if E_B_std is not None:
+            g = np.random.Generator(np.random.PCG64(self.seed))
+            self.E_B = self._EB_np * g.normal(1, E_B_std, size=self._EB_np.shape)
+        self.moment = Msat * V if moment is None else moment
+        self._m_perp_factor = 0.0
+        self.m_perp_factor = in_plane if m_perp_factor is None else m_perp_factor
+        self.major_axis = major_axis
+        self.minor_axis = major_axis if minor_axis is None else minor_axis
+        self.history = History()
+        if energies is None:
+            energies = (DipolarEnergy(),)
+        elif isinstance(energies, Energy):
+            energies = (energies,)
+        else:
+            energies = tuple(energies)
+        for energy in energies:
+            self.add_energy(energy)
+
+    # ------------------------------------------------------------------ geometry (host)
+    def _dx_set(self, value):
+        value = np.asarray(value, dtype=float).reshape(-1)
+        self._dx = np.tile(value, math.ceil(self.nx / value.size))[:self.nx]
+        self.x = np.zeros(self.nx)
+        self.x[1:] = np.cumsum(self._dx)[:-1]
+        self.xx, _ = np.meshgrid(self.x, np.empty(self.ny))
+        self.x_min, self.x_max = float(self.x[0]), float(self.x[-1])
+
+    def _dy_set(self, value):
+        value = np.asarray(value, dtype=float).reshape(-1)
+        self._dy = np.tile(value, math.ceil(self.ny / value.size))[:self.ny]
+        self.y = np.zeros(self.ny)
+        self.y[1:] = np.cumsum(self._dy)[:-1]
+        _, self.yy = np.meshgrid(np.empty(self.nx), self.y)
+        self.y_min, self.y_max = float(self.y[0]), float(self.y[-1])
+
+    @property
+    def dx(self):
+        return self._dx
+
+    @dx.setter
+    def dx(self, value):
+        self._dx_set(value)
+        self._reinit_energies()
+
+    @property
+    def dy(self):
+        return self._dy
+
+    @dy.setter
+    def dy(self, value):
+        self._dy_set(value)
+        self._reinit_energies()
+
+    def _initialize_ip(self, angle: float = 0.):
+        """hotspice/core.py:182-193."""
+        self.original_angles = self._get_angles() + angle
+        self.angles = self.original_angles * self.occupation
+        self.orientation = np.zeros(self.ixx.shape + (2,))
+        self.orientation[:, :, 0] = np.cos(self.angles) * self.occupation
+        self.orientation[:, :, 1] = np.sin(self.angles) * self.occupation
+
+    def _get_unitcell(self, max_cell=100):
+        """hotspice/core.py:146-161."""
+        dx, dy = self.dx.reshape(1, -1), self.dy.reshape(-1, 1)
+        for n in range(1, min(self.nx + self.ny + 1, max_cell + 1)):
+            for uy in range(max(0, n - self.nx) + 1, min(n, self.ny) + 1):
+                ux = n - uy + 1
+                if check_repetition(self.orientation if self.in_plane else self.occupation, ux, uy):
+                    if check_repetition(dx, ux, 1) and check_repetition(dy, 1, uy):
+                        return Unitcell(ux, uy)
+        warnings.warn(dedent(f"""
+            Could not detect a reasonably sized unit cell. Defaulting to entire domain {self.nx}x{self.ny}."""), stacklevel=2)
+        return Unitcell(self.nx, self.ny)
+
+    def _get_closest_dist(self):
+        sl = np.where(self.occupation[:self.unitcell.y * 2, :self.unitcell.x * 2])
+        pos = np.asarray([self.xx[sl], self.yy[sl]]).T
+        d = np.sqrt(((pos[:, None, :] - pos[None, :, :]) ** 2).sum(-1))
+        return float(d[np.triu_indices(len(pos), 1)].min())
+
+    @property
+    def shape(self):
+        return (self.ny, self.nx)
+
+    @property
+    def PBC(self):
+        return self._PBC
+
+    @PBC.setter
+    def PBC(self, value: bool):
+        if hasattr(self, 'unitcell') and value and (self.nx % self.unitcell.x != 0 or self.ny % self.unitcell.y != 0):
+            warnings.warn(dedent(f"""
+                WARNING: PBC can not be enabled, because there is a non-integer number of unit cells along the x- and/or y-axis,
+                         so the boundaries do not match (unit cell has size {self.unitcell.x}x{self.unitcell.y})."""), stacklevel=2)
+            self._PBC = False
+            return
+        self._PBC = bool(value)
+        self._reinit_energies()
+
+    def _reinit_energies(self):
+        for energy in getattr(self, '_energies', []):
+            energy.initialize(self)
+        if hasattr(self, '_version'):
+            self._state_changed()
+
+    # ------------------------------------------------------------------ state
+    def _state_changed(self):
+        self._version += 1
+        self._L = None
+        self._graphs.clear()
+
+    def _stream(self):
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def _field(self, value):
+        return as_2D_array(value, self.shape)
+
+    @property
+    def m(self) -> torch.Tensor:
+        """Spins as a float64 tensor (-1, 0, +1). Assign to ``m`` (or call initialize_m) to
+        change them; the returned tensor is a copy."""
+        return self._m_dev.double()
+
+    @m.setter
+    def m(self, value):
+        self._set_m_array(as_2D_array(value, self.shape))
+
+    def _set_m_array(self, arr):
+        arr = np.sign(np.asarray(arr, dtype=float))
+        self._m_dev.copy_(torch.as_tensor(arr, dtype=torch.int8))
+        self._mm_dev.copy_(self._m_dev.float() * self._mom_dev)
+
+    def initialize_m(self, pattern='random', *, angle: float = 0, update_energy: bool = True):
+        """hotspice/core.py:163-180."""
+        if isinstance(pattern, str):
+            m = self._set_m(pattern)
+        else:
+            try:
+                m = as_2D_array(pattern, self.shape)
+            except (ValueError, TypeError):
+                raise ValueError("Argument <pattern> could not be parsed as a valid array for <self.m>.")
+        m = np.sign(np.asarray(m, dtype=float)) * self.occupation
+        flip = self._get_m_uniform() != self._get_m_uniform(angle)
+        m[flip] *= -1
+        self._set_m_array(m)
+        if update_energy:
+            self.update_energy()
+
+    def _get_m_uniform(self, angle=0):
+        angle += 1e-6
+        if self.in_plane:
+            return self.occupation * (2 * ((self.orientation[:, :, 0] * np.cos(angle) + self.orientation[:, :, 1] * np.sin(angle)) >= 0) - 1)
+        return np.ones_like(self.xx) * ((np.floor(angle / math.pi - .5) % 2) * 2 - 1)
+
+    def _random_pm1(self):
+        """rng.integers(0, 2, size) * 2 - 1 (hotspice/core.py:951) from the Philox stream."""
+        n = self.nx * self.ny
+        u = torch.empty(n, device=self.device, dtype=torch.float64)
+        call = int(self._read_counters()['rng_call'])
+        _lib.check(self._lib.hs_philox_uniform(self.seed, call, n, u.data_ptr(), self._stream()), 'hs_philox_uniform')
+        self._write_counters(rng_call=call + 1)
+        return (torch.floor(u * 2) * 2 - 1).reshape(self.shape).cpu().numpy()
+
+    def _set_m(self, pattern: str):
+        """hotspice/core.py:924-952 (common patterns); subclasses add 'afm' etc."""
+        match str(pattern).strip().lower():
+            case 'uniform':
+                return self._get_m_uniform()
+            case 'vortex':
+                m = np.ones_like(self.xx)
+                if self.in_plane:
+                    dxv = self.xx - (self.x_max - self.x_min) / 2
+                    dyv = self.yy - (self.y_max - self.y_min) / 2
+                    desired = (dxv + 1j * dyv) * (-1j + 1e-6)
+                    dot = desired.real * self.orientation[:, :, 0] + desired.imag * self.orientation[:, :, 1]
+                    dot[dot == 0] = 1
+                    occ = np.where(self.occupation == 1)
+                    m[occ] = np.sign(dot)[occ]
+                else:
+                    m[np.where(self.xx >= (self.x_max - self.x_min) / 2)] *= -1
+                return m
+            case str(unknown):
+                if unknown != 'random':
+                    warnings.warn(f"Pattern '{unknown}'' not recognized, defaulting to 'random'.", stacklevel=2)
+                return self._random_pm1()
+
+    # fields ------------------------------------------------------------------------
+    @property
+    def T(self):
+        return torch.as_tensor(self._T_np, device=self.device)
+
+    @T.setter
+    def T(self, value):
+        self._T_np = as_2D_array(value, self.shape)
+        self.kBT = kB * self._T_np
+        with np.errstate(divide='ignore'):
+            self.beta = 1 / self.kBT
+        self._T_zero = bool(np.any(self._T_np == 0))
+        occ = self.occupation.astype(bool)
+        bu = self.beta[occ] if occ.any() else self.beta.reshape(-1)
+        self._beta_uniform = float(bu[0]) if (np.all(bu == bu[0]) and np.isfinite(bu[0])) else 0.0
+        b = np.where(np.isfinite(self.beta), self.beta, 0.0)
+        self._beta_dev = torch.as_tensor(b, device=self.device, dtype=torch.float32).contiguous()
+        if hasattr(self, '_version'):
+            self._state_changed()
+
+    def set_T(self, f, /, *, center=False, crystalunits=False):
+        xx = self.ixx if crystalunits else self.xx
+        yy = self.iyy if crystalunits else self.yy
+        lx = self.nx - 1 if crystalunits else self.x_max - self.x_min
+        ly = self.ny - 1 if crystalunits else self.y_max - self.y_min
+        self.T = f(xx - center * lx / 2, yy - center * ly / 2)
+
+    @property
+    def E_B(self):
+        return torch.as_tensor(self._EB_np, device=self.device)
+
+    @E_B.setter
+    def E_B(self, value):
+        self._EB_np = as_2D_array(value, self.shape)
+        self._EB_dev = torch.as_tensor(self._EB_np, device=self.device, dtype=torch.float32).contiguous()
+        self._state_changed()
+
+    @property
+    def moment(self):
+        return torch.as_tensor(self._moment_np, device=self.device)
+
+    @moment.setter
+    def moment(self, value):
+        self._moment_np = as_2D_array(value, self.shape)
+        self._momentSq = self._moment_np * self._moment_np
+        self._mom_dev = torch.as_tensor(self._moment_np, device=self.device, dtype=torch.float32).contiguous()
+        self._mm_dev.copy_(self._m_dev.float() * self._mom_dev)
+        for e in self._energies:
+            if isinstance(e, ZeemanEnergy):
+                e.set_field()
+        self._state_changed()
+
+    @property
+    def USE_PERP_ENERGY(self):
+        return bool(self.m_perp_factor) and self.in_plane
+
+    @property
+    def m_perp_factor(self):
+        return self._m_perp_factor
+
+    @m_perp_factor.setter
+    def m_perp_factor(self, value):
+        if not isinstance(value, (int, float, bool)):
+            raise ValueError("m_perp_factor must be scalar. It is not currently supported as a 2D array.")
+        if value and not self.in_plane:
+            warnings.warn("You set a nonzero `m_perp_energy`, but this has no effect for an OOP ASI.")
+        used = self.USE_PERP_ENERGY
+        self._m_perp_factor = float(value)
+        self._state_changed()
+        if not used and self.USE_PERP_ENERGY and self._energies:
+            self.update_energy()
+
+    # counters -----------------------------------------------------------------------
+    def _read_counters(self):
+        raw = self._counters.cpu().numpy()
+        return np.frombuffer(raw.tobytes(), dtype=_lib.COUNTERS_DTYPE)[0]
+
+    def _write_counters(self, **fields):
+        rec = np.frombuffer(self._counters.cpu().numpy().tobytes(), dtype=_lib.COUNTERS_DTYPE).copy()
+        for k, v in fields.items():
+            rec[0][k] = v
+        self._counters.copy_(torch.from_numpy(rec.view(np.uint8).copy()))
+
+    @property
+    def t(self) -> float:
+        return float(self._read_counters()['t'])
+
+    @t.setter
+    def t(self, value):
+        self._write_counters(t=float(value))
+
+    @property
+    def switches(self) -> int:
+        return int(self._read_counters()['switches'])
+
+    @switches.setter
+    def switches(self, value):
+        self._write_counters(switches=int(value))
+
+    @property
+    def attempted_switches(self) -> int:
+        return int(self._read_counters()['attempted'])
+
+    @attempted_switches.setter
+    def attempted_switches(self, value):
+        self._write_counters(attempted=int(value))
+
+    @property
+    def MCsteps(self):
+        return self.attempted_switches / self.n
+
+    def reset_stats(self):
+        self._write_counters(t=0.0, switches=0, attempted=0)
+
+    @property
+    def status(self) -> int:
+        """Device status bits (HS_ST_*): bounded loops that gave up, capacity overflows."""
+        return int(self._read_counters()['status'])
+
+    @property
+    def near_threshold(self) -> int:
+        """Metropolis decisions whose margin |u - p| was within a 1e-6 relative energy change."""
+        return int(self._read_counters()['near_threshold'])
+
+    # energies -----------------------------------------------------------------------
+    def add_energy(self, energy: Energy, exist_ok=False, verbose=True):
+        energy.initialize(self)
+        for i, e in enumerate(self._energies):
+            if type(e) is type(energy):
+                if exist_ok:
+                    return e
+                if verbose:
+                    warnings.warn(f"An instance of {type(energy).__name__} was already included in the simulation, and has now been overwritten.", stacklevel=2)
+                self._energies[i] = energy
+                self._state_changed()
+                return
+        self._energies.append(energy)
+        self._state_changed()
+        return energy
+
+    def remove_energy(self, name: str, verbose=True):
+        name = name.lower().replace('energy', '')
+        for i, e in enumerate(self._energies):
+            if name == e.shortname:
+                self._energies.pop(i)
+                self._state_changed()
+                return
+        if verbose:
+            warnings.warn(f"There is no '{name}' energy associated with this Magnets object.", stacklevel=2)
+
+    def has_energy(self, name: str):
+        name = name.lower().replace('energy', '')
+        return any(name == e.shortname for e in self._energies)
+
+    def get_energy(self, name: str, verbose=True):
+        name = name.lower().replace('energy', '')
+        for e in self._energies:
+            if name == e.shortname:
+                return e
+        if verbose:
+            warnings.warn(f"There is no '{name}' energy associated with this Magnets object. Valid energies are: {[e.shortname for e in self._energies]}", stacklevel=2)
+        return None
+
+    def update_energy(self, index=None):
+        """hotspice/core.py:241-253."""
+        for energy in self._energies:
+            if index is None:
+                energy.update()
+            else:
+                idx = np.asarray(index).reshape(2, -1)
+                if idx[0].size == 1:
+                    energy.update_single(idx)
+                elif idx[0].size > 1:
+                    energy.update_multiple(idx)
+
+    def switch_energy(self, indices2D=None):
+        return sum(e.energy_switch(indices2D) for e in self._energies)
+
+    def perp_energy(self, indices2D=None):
+        if not self.USE_PERP_ENERGY:
+            z = torch.zeros(self.shape, device=self.device, dtype=torch.float64)
+            return z if indices2D is None else torch.zeros(np.asarray(indices2D).shape[1], device=self.device, dtype=torch.float64)
+        tot = sum(e.E_perp for e in self._energies) * self.m_perp_factor
+        if indices2D is None:
+            return tot
+        idx = torch.as_tensor(np.asarray(indices2D), device=self.device, dtype=torch.long)
+        return tot[idx[0], idx[1]]
+
+    @property
+    def E(self):
+        return sum(e.E for e in self._energies)
+
+    @property
+    def E_perp(self):
+        return sum(e.E_perp for e in self._energies) * self.m_perp_factor
+
+    @property
+    def E_tot(self) -> float:
+        return float(sum(e.E_tot for e in self._energies))
+
+    def E_barrier(self, idx=None, min_only=False):
+        """hotspice/core.py:625-656, evaluated on the device in FP64."""
+        occ_inf = torch.as_tensor(self._occupation_inf, device=self.device)
+        EB = torch.as_tensor(self._EB_np, device=self.device)
+        dE = self.switch_energy() * occ_inf
+        E = -dE / 2
+        if not self.USE_PERP_ENERGY:
+            if self.params.ENERGY_BARRIER_METHOD == 'simple':
+                b = torch.maximum(dE, EB - E)
+            else:
+                b = torch.where(dE > 4 * EB, dE, torch.minimum(EB * (dE * (.25 / EB) + 1) ** 2, dE + 4 * EB))
+            b1 = b2 = b
+        else:
+            Ep = self.perp_energy()
+            b1 = torch.maximum(dE, EB + Ep - E)
+            b2 = torch.maximum(dE, EB - Ep - E)
+        if idx is not None:
+            i = torch.as_tensor(np.asarray(idx), device=self.device, dtype=torch.long)
+            b1, b2 = b1[i[0], i[1]], b2[i[0], i[1]]
+        return torch.minimum(b1, b2) if min_only else (b1, b2)
+
+    # observables ----------------------------------------------------------------------
+    @property
+    def m_avg_x(self) -> float:
+        if not self.in_plane:
+            return 0
+        return float(torch.mean(self.m * torch.as_tensor(self.orientation[:, :, 0], device=self.device))) * self.nx * self.ny / self.n
+
+    @property
+    def m_avg_y(self) -> float:
+        if not self.in_plane:
+            return 0
+        return float(torch.mean(self.m * torch.as_tensor(self.orientation[:, :, 1], device=self.device))) * self.nx * self.ny / self.n
+
+    @property
+    def m_avg(self) -> float:
+        return (self.m_avg_x ** 2 + self.m_avg_y ** 2) ** 0.5 if self.in_plane else float(torch.mean(self.m))
+
+    @property
+    def m_avg_angle(self) -> float:
+        return math.atan2(self.m_avg_y, self.m_avg_x) if self.in_plane else 0. + (self.m_avg < 0) * math.pi
+
+    @property
+    def T_avg(self) -> float:
+        return float(np.mean(self._T_np))
+
+    @property
+    def E_B_avg(self) -> float:
+        return float(np.mean(self._EB_np))
+
+    @property
+    def moment_avg(self) -> float:
+        return float(np.mean(self._moment_np))
+
+    def history_save(self, *, E_tot=None, t=None, T_avg=None, m_avg=None):
+        self.history.entry(self)
+        if E_tot is not None: self.history.E[-1] = float(E_tot)
+        if t is not None: self.history.t[-1] = float(t)
+        if T_avg is not None: self.history.T[-1] = float(T_avg)
+        if m_avg is not None: self.history.m[-1] = float(m_avg)
+
+    @lru_cache
+    def calc_r(self, Q, as_scalar=True):
+        """hotspice/core.py:720-733."""
+        with np.errstate(divide='ignore'):
+            r = (8e-7 * self._momentSq / (Q * self.kBT)) ** (1 / 3)
+        r = np.clip(r, 0, (self.x_max - self.x_min) + (self.y_max - self.y_min))
+        return float(np.max(r)) if as_scalar else r
+
+    # ------------------------------------------------------------------ device plumbing
+    def _dipolar(self):
+        for e in self._energies:
+            if isinstance(e, DipolarEnergy):
+                return e
+        return None
+
+    def _lattice_struct(self, dip: DipolarEnergy | None = None):
+        """HsLattice of the current state. ``dip`` overrides the registered dipolar energy
+        (used while an energy is being initialised, before add_energy registers it)."""
+        override = dip is not None and dip is not self._dipolar()
+        if self._L is not None and not override:
+            return self._L
+        L = _lib.HsLattice()
+        L.m = self._m_dev.data_ptr(); L.occ = self._occ_dev.data_ptr(); L.mm = self._mm_dev.data_ptr()
+        L.moment = self._mom_dev.data_ptr(); L.nonzero = self._nonzero_dev.data_ptr()
+        L.E_B = self._EB_dev.data_ptr(); L.beta = self._beta_dev.data_ptr()
+        L.beta_uniform = self._beta_uniform
+        L.m_perp_factor = self.m_perp_factor
+        L.seed = self.seed
+        L.nx, L.ny, L.ux, L.uy = self.nx, self.ny, self.unitcell.x, self.unitcell.y
+        L.pbc = int(self.PBC); L.in_plane = int(self.in_plane); L.use_perp = int(self.USE_PERP_ENERGY)
+        L.n_occ = self.n
+        L.barrier_method = _lib.HS_BARRIER_SIMPLE if self.params.ENERGY_BARRIER_METHOD == 'simple' else _lib.HS_BARRIER_PARABOLIC
+        L.trunc_cutoff = self.params.SIMULTANEOUS_SWITCHES_CONVOLUTION_OR_SUM_CUTOFF
+        L.trunc_size = self.params.REDUCED_KERNEL_SIZE
+        L.orient = _ptr(self._orient_dev)
+        d = dip if override else self._dipolar()
+        if d is not None:
+            ks = d.kernel_set
+            L.has_dipolar = 1
+            L.K = d._K.data_ptr(); L.Kpo = _ptr(d._Kpo); L.Kps = _ptr(d._Kps)
+            L.E_dip = d._E.data_ptr(); L.E_dip_perp = _ptr(d._Ep)
+            L.sub_of = d._sub_of.data_ptr()
+            L.dip_wx, L.dip_wy, L.dip_wrap, L.n_sub = ks.wx, ks.wy, int(ks.wrap), ks.K.shape[0]
+            L.dip_pref = float(d.prefactor)
+        else:
+            if not hasattr(self, '_sub_of_dummy'):
+                self._sub_of_dummy = torch.full((self.unitcell.x * self.unitcell.y,), -1, device=self.device, dtype=torch.int32)
+            L.sub_of = self._sub_of_dummy.data_ptr()
+        for e in self._energies:
+            if isinstance(e, ZeemanEnergy):
+                L.zee = e._ef32.data_ptr()
+                L.zee_perp = e._efp32.data_ptr()
+            elif isinstance(e, ExchangeEnergy):
+                nn = np.asarray(e.local_interaction, dtype=np.int64)
+                L.has_exchange = 1
+                L.J = float(e.J)
+                L.nn_h, L.nn_w = nn.shape
+                for i, v in enumerate(nn.reshape(-1)):
+                    L.nn[i] = int(v)
+                if self._beta_uniform > 0:
+                    counts = np.arange(25, dtype=float)
+                    kbt = np.full(25, kB * float(self._T_np[self.occupation.astype(bool)][0]))
+                    bond = 1 - np.exp(-2 * e.J / kbt * counts)
+                    self._bond_dev = torch.as_tensor(bond, device=self.device, dtype=torch.float64)
+                    L.wolff_bond = self._bond_dev.data_ptr()
+        if not override:
+            self._L = L
+        return L
+
+    def _switch_list(self, cap):
+        sl = getattr(self, '_sw', None)
+        if sl is None or sl[0].numel() < cap:
+            cap = max(cap, 64)
+            t = torch.zeros((3, cap), device=self.device, dtype=torch.int32)
+            s = _lib.HsSwitchList()
+            s.y, s.x, s.mode, s.cap = t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr(), cap
+            self._sw = (t, s)
+            self._graphs.clear()
+        return self._sw
+
+    def _get_scratch(self, key, nbytes):
+        buf = self._scratch.get(key)
+        if buf is None or buf.numel() < nbytes:
+            buf = torch.zeros(max(int(nbytes), 256), device=self.device, dtype=torch.uint8)
+            self._scratch[key] = buf
+            self._graphs.clear()
+        return buf
+
+    # -- full recompute and manual updates ----------------------------------------------
+    def _full_recompute(self, d: DipolarEnergy, method=None):
+        L = self._lattice_struct(d)
+        method = method or self.engine.recompute
+        ks = d.kernel_set
+        N = self.nx * self.ny
+        W = N if ks.full else (2 * ks.wx + 1) * (2 * ks.wy + 1)
+        if method == 'auto':
+            method = 'direct64' if N * W <= self.engine.direct_max_pairs else 'igemm'
+        if method == 'direct64':
+            E64 = torch.empty((self.ny, self.nx), device=self.device, dtype=torch.float64)
+            Ep64 = torch.empty_like(E64) if self.USE_PERP_ENERGY else None
+            _lib.check(self._lib.hs_dipolar_full_direct(L, 1, E64.data_ptr(), _ptr(Ep64), self._stream()),
+                       'hs_dipolar_full_direct')
+            d._E.copy_(E64)
+            if Ep64 is not None:
+                d._Ep.copy_(Ep64)
+        elif method == 'direct32':
+            _lib.check(self._lib.hs_dipolar_full_direct(L, 0, None, None, self._stream()), 'hs_dipolar_full_direct')
+        elif method == 'igemm':
+            nbytes = self._lib.hs_igemm_scratch_bytes(L, self.engine.igemm_splits)
+            buf = self._get_scratch('igemm', max(nbytes, 1))
+            _lib.check(self._lib.hs_dipolar_full_igemm(L, self.engine.igemm_splits, buf.data_ptr(), buf.numel(),
+                                                        self._stream()), 'hs_dipolar_full_igemm')
+        else:
+            raise ValueError(f"unknown recompute method '{method}'")
+
+    def _dipolar_apply(self, d, indices2D, semantics):
+        idx = np.asarray(indices2D, dtype=np.int64).reshape(2, -1)
+        k = idx.shape[1]
+        if k == 0:
+            return
+        t, s = self._switch_list(k)
+        t[0, :k].copy_(torch.as_tensor(idx[0], dtype=torch.int32))
+        t[1, :k].copy_(torch.as_tensor(idx[1], dtype=torch.int32))
+        if semantics == _lib.HS_UPDATE_MULTIPLE:
+            ux, uy = self.unitcell.x, self.unitcell.y
+            sub = (idx[1] % ux) + (idx[0] % uy) * ux
+            counts = np.bincount(sub)
+            mode = (counts[sub] > self.params.SIMULTANEOUS_SWITCHES_CONVOLUTION_OR_SUM_CUTOFF).astype(np.int32)
+        else:
+            mode = np.zeros(k, dtype=np.int32)
+        t[2, :k].copy_(torch.as_tensor(mode))
+        L = self._lattice_struct(d)
+        _lib.check(self._lib.hs_dipolar_update(L, s, None, k, semantics, None, self._stream()), 'hs_dipolar_update')
+
+    # ------------------------------------------------------------------ hot path
+    def _grid_plan(self, r, scheme):
+        key = (scheme, float(r))
+        plan = self._plans.get(key)
+        if plan is not None:
+            return plan
+        P = _lib.HsGridPlan()
+        ux, uy = self.unitcell.x, self.unitcell.y
+        tensors = []
+        if scheme == 'grid':
+            Rx = math.ceil(r / np.min(self.dx)) - 1
+            Ry = math.ceil(r / np.min(self.dy)) - 1
+            Rx, Ry = ux * math.ceil(Rx / ux), uy * math.ceil(Ry / uy)
+            Rx, Ry = min(Rx, self.nx), min(Ry, self.ny)
+            Rx, Ry = max(Rx, 2), max(Ry, 2)
+            snx, sny = self.nx // Rx + 1, self.ny // Ry + 1
+            n_sc = len(range(0, min(snx, self.nx), 2)) * len(range(0, min(sny, self.ny), 2))
+            offs, packed = [0], []
+            for ddy in range(uy):
+                for ddx in range(ux):
+                    oy, ox = self.occupation[ddy:ddy + Ry, ddx:ddx + Rx].nonzero()
+                    packed.extend(((oy.astype(np.int64) << 16) | ox).tolist())
+                    offs.append(len(packed))
+            t_off = torch.as_tensor(np.asarray(offs, dtype=np.int32), device=self.device)
+            t_yx = torch.as_tensor(np.asarray(packed if packed else [0], dtype=np.int32), device=self.device)
+            tensors = [t_off, t_yx]
+            P.phase_off, P.phase_yx = t_off.data_ptr(), t_yx.data_ptr()
+            P.Rx, P.Ry, P.snx, P.sny, P.n_sc = Rx, Ry, snx, sny, n_sc
+            P.sample_scheme = _lib.HS_SAMPLE_GRID
+        elif scheme == 'single':
+            P.sample_scheme = _lib.HS_SAMPLE_SINGLE
+            P.n_sc = 1
+        elif scheme == 'Poisson':
+            P.sample_scheme = _lib.HS_SAMPLE_POISSON
+            P.r_cells = float(r / min(np.min(self.dx), np.min(self.dy)))
+            P.poisson_k = 4
+            P.n_sc = 1
+        else:
+            raise ValueError(scheme)
+        plan = (P, tensors)
+        self._plans[key] = plan
+        return plan
+
+    def _step_args(self, kw):
+        """Resolve the per-scheme launch arguments of one update step."""
+        sch = self.params.UPDATE_SCHEME
+        L = self._lattice_struct()
+        if sch == Scheme.NEEL:
+            af = float(kw.get('attempt_freq', 1e10))
+            nbytes = self._lib.hs_neel_scratch_bytes(L)
+            buf = self._get_scratch('neel', nbytes)
+            t, s = self._switch_list(1)
+            return ('neel', L, s, af, buf)
+        if sch == Scheme.METROPOLIS:
+            if kw.get('idx') is not None:
+                raise NotImplementedError('_update_Metropolis(idx=...) with caller-chosen indices is not on the device path')
+            ms = self.params.MULTISAMPLING_SCHEME
+            if ms == 'cluster':
+                raise ValueError("MULTISAMPLING_SCHEME='cluster' needs UPDATE_SCHEME=Wolff")
+            Q = kw.get('Q', 0.05)
+            r = kw.get('r', 0)
+            r = self.calc_r(Q) if r == 0 else r
+            P, _ = self._grid_plan(r, ms)
+            P.metropolis_time = int(self.params.METROPOLIS_TIME)
+            P.attempt_freq = float(kw.get('attempt_freq', 1e10))
+            nbytes = self._lib.hs_metropolis_scratch_bytes(L, P)
+            buf = self._get_scratch(('metro', ms, float(r)), nbytes)
+            cap = max(P.n_sc, 1)
+            if ms == 'Poisson':
+                cap = max(cap, (nbytes // 20) + 1)
+            t, s = self._switch_list(cap)
+            return ('metro', L, s, P, buf)
+        if sch == Scheme.WOLFF:
+            nbytes = self._lib.hs_wolff_scratch_bytes(L)
+            buf = self._get_scratch('wolff', nbytes)
+            t, s = self._switch_list(self.nx * self.ny)
+            return ('wolff', L, s, None, buf)
+        raise ValueError(f"The Magnets.params object has an invalid value for UPDATE_SCHEME='{sch}'.")
+
+    def _launch(self, args, stream):
+        kind, L, s, extra, buf = args
+        C = self._counters.data_ptr()
+        if kind == 'neel':
+            rc = self._lib.hs_neel_step(L, C, s, extra, buf.data_ptr(), buf.numel(), stream)
+        elif kind == 'metro':
+            rc = self._lib.hs_metropolis_step(L, C, s, extra, buf.data_ptr(), buf.numel(), stream)
+        else:
+            rc = self._lib.hs_wolff_step(L, C, s, buf.data_ptr(), buf.numel(), stream)
+        _lib.check(rc, f'hs_{kind}_step')
+
+    def update(self, *args, **kwargs):
+        """One update step (hotspice/core.py:604-622). Returns the switched index/indices."""
+        if self._T_zero:
+            if self.params.UPDATE_SCHEME != Scheme.METROPOLIS:
+                warnings.warn("T=0 somewhere in the domain, so no switch will be simulated to prevent DIV/0 errors.", stacklevel=2)
+            else:
+                warnings.warn("T=0 somewhere in the domain, so ergodicity can not be guaranteed. Proceed with caution.", stacklevel=2)
+            return None
+        if self.params.UPDATE_SCHEME == Scheme.NEEL:
+            self._write_counters(t_max=float(kwargs.get('t_max', 1)), progress=0, done=0)
+        args_ = self._step_args(kwargs)
+        self._launch(args_, self._stream())
+        c = self._read_counters()
+        n = int(c['n_sw'])
+        t, _ = self._sw
+        if self.params.UPDATE_SCHEME == Scheme.NEEL:
+            if n == 0:
+                return None
+            yx = t[:2, 0].cpu().numpy()
+            return (int(yx[0]), int(yx[1]))
+        idx = t[:2, :n].cpu().numpy().astype(np.int64)
+        if self.params.UPDATE_SCHEME == Scheme.WOLFF:
+            order = np.lexsort((idx[1], idx[0]))
+            idx = idx[:, order]
+        return idx
+
+    def progress(self, t_max: float = 1, MCsteps_max: float = 4., stepwise: bool = False, **kwargs):
+        """hotspice/core.py:736-760. Non-stepwise runs execute on the device in chunks of
+        ``EngineConfig.graph_steps`` steps (CUDA-graph replays) and synchronise per chunk."""
+        if stepwise:
+            return self._progress_stepwise(t_max=t_max, MCsteps_max=MCsteps_max, **kwargs)
+        if self._T_zero:
+            raise RuntimeError('progress() with T=0 somewhere in the domain would never advance')
+        c = self._read_counters()
+        t0 = float(c['t'])
+        mc0 = float(c['attempted']) / self.n
+        self._write_counters(t0=t0, mc0=mc0, t_max=float(t_max), mc_max=float(MCsteps_max), progress=1, done=0)
+        self._run_until_done(kwargs)
+        c = self._read_counters()
+        self._write_counters(progress=0, done=0)
+        return float(c['t']) - t0, float(c['attempted']) / self.n - mc0
+
+    def _run_until_done(self, kw, max_chunks=10 ** 9):
+        args_ = self._step_args(kw)
+        K = max(1, int(self.engine.graph_steps))
+        off_done = _lib.HsCounters.done.offset
+        steps_since_resync = 0
+        for _ in range(max_chunks):
+            self._run_chunk(args_, K)
+            steps_since_resync += K
+            if self.engine.resync_every and steps_since_resync >= self.engine.resync_every:
+                d = self._dipolar()
+                if d is not None:
+                    self._full_recompute(d)
+                steps_since_resync = 0
+            flag = int(self._counters[off_done:off_done + 4].cpu().view(torch.int32)[0])
+            if flag:
+                break
+            st = int(self._counters[_lib.HsCounters.status.offset:_lib.HsCounters.status.offset + 4].cpu().view(torch.int32)[0])
+            if st:
+                raise RuntimeError(f'device step reported status {st} (HS_ST_* bits)')
+
+    def _run_chunk(self, args_, K):
+        if not self.engine.use_graphs:
+            st = self._stream()
+            for _ in range(K):
+                self._launch(args_, st)
+            return
+        extra = args_[3]
+        extra_key = extra if isinstance(extra, float) or extra is None else (extra.sample_scheme, extra.Rx, extra.Ry,
+                                                                            extra.r_cells, extra.metropolis_time,
+                                                                            extra.attempt_freq, extra.phase_yx)
+        key = (args_[0], extra_key, args_[4].data_ptr(), self._sw[0].data_ptr(), self._version, K)
+        g = self._graphs.get(key)
+        if g is None:
+            # warm-up launch outside capture is not needed: every launch is a plain kernel
+            g = torch.cuda.CUDAGraph()
+            s = torch.cuda.Stream(self.device)
+            s.wait_stream(torch.cuda.current_stream(self.device))
+            with torch.cuda.graph(g, stream=s):
+                for _ in range(K):
+                    self._launch(args_, s.cuda_stream)
+            torch.cuda.current_stream(self.device).wait_stream(s)
+            self._graphs[key] = g
+        g.replay()
+
+    def _progress_stepwise(self, t_max: float = 1, MCsteps_max: float = 4., **kwargs):
+        t_0, MCsteps_0 = self.t, self.MCsteps
+        while lower_than(dt := self.t - t_0, t_max) and lower_than(self.MCsteps - MCsteps_0, MCsteps_max):
+            if self.params.UPDATE_SCHEME == Scheme.NEEL:
+                self.update(t_max=(t_max - dt), **kwargs)
+            else:
+                self.update(**kwargs)
+            yield
+        return self.t - t_0, self.MCsteps - MCsteps_0
+
+    # ------------------------------------------------------------------ subclass hooks
+    def _get_angles(self):
+        return np.zeros_like(self.ixx, dtype=float)
+
+    def _get_occupation(self):
+        return np.ones_like(self.ixx)
+
+    def _get_groundstate(self):
+        return 'random'
+
+    def _get_nearest_neighbors(self):
+        return np.array([[0, 1, 0], [1, 0, 1], [0, 1, 0]])
+
+    def _get_appropriate_avg(self):
+        return 'cross'
+
+    def _get_AFMmask(self):
+        return np.array([[1, 0, -1], [0, 0, 0], [-1, 0, 1]], dtype='float')

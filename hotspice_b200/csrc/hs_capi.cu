@@ -1,0 +1,208 @@
+// extern "C" entry points of libhotspice_sm100.so (declared in include/hotspice_b200.h).
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "hs_common.cuh"
+#include "hs_internal.h"
+
+namespace {
+thread_local char g_err[512] = "";
+
+__global__ void philox_kernel(uint64_t seed, uint64_t call, int32_t n, double *out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = hs_u53(seed, call, (uint32_t)i);
+}
+
+__global__ void exchange_energy_kernel(HsLattice L, float *E, float *Ep) {
+    const int64_t N = (int64_t)L.nx * L.ny;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        double e, ep;
+        hs_exchange_at(L, (int)(i / L.nx), (int)(i % L.nx), e, ep);
+        E[i] = (float)e;
+        if (Ep) Ep[i] = (float)ep;
+    }
+}
+
+__global__ void switch_energy_kernel(HsLattice L, float *dE) {
+    const int64_t N = (int64_t)L.nx * L.ny;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        double e, ep;
+        hs_energy_at(L, (int)(i / L.nx), (int)(i % L.nx), e, ep);
+        dE[i] = (float)(-2.0 * e);
+    }
+}
+
+int grid_for(int64_t n, int threads) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads, 148 * 16));
+}
+
+int check_lattice(const HsLattice *L, const char *who) {
+    if (!L) { hs_set_error("%s: null lattice", who); return HS_EINVAL; }
+    if (L->nx <= 0 || L->ny <= 0 || L->ux <= 0 || L->uy <= 0) { hs_set_error("%s: bad lattice size", who); return HS_EINVAL; }
+    if ((int64_t)L->nx * L->ny >= (1LL << 31)) { hs_set_error("%s: lattice larger than 2^31 cells", who); return HS_ERANGE; }
+    if (!L->m || !L->occ || !L->mm || !L->E_B) { hs_set_error("%s: missing state array", who); return HS_EINVAL; }
+    if (L->has_dipolar && (!L->K || !L->E_dip || !L->sub_of)) { hs_set_error("%s: missing dipolar arrays", who); return HS_EINVAL; }
+    if (L->has_dipolar && L->use_perp && (!L->Kpo || !L->E_dip_perp)) { hs_set_error("%s: missing perp arrays", who); return HS_EINVAL; }
+    if (L->has_exchange && (L->nn_h * L->nn_w > 28 || L->nn_h % 2 == 0 || L->nn_w % 2 == 0)) {
+        hs_set_error("%s: exchange mask must be odd-sized and at most 28 cells", who); return HS_EINVAL;
+    }
+    if (L->has_exchange && L->in_plane && !L->orient) { hs_set_error("%s: in-plane exchange needs orientation", who); return HS_EINVAL; }
+    if (L->beta_uniform <= 0.0 && !L->beta) { hs_set_error("%s: missing beta", who); return HS_EINVAL; }
+    if (L->n_occ <= 0 || !L->nonzero) { hs_set_error("%s: lattice has no magnets", who); return HS_EINVAL; }
+    return HS_OK;
+}
+}  // namespace
+
+void hs_set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+int hs_check_launch(const char *what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        hs_set_error("%s: %s", what, cudaGetErrorString(e));
+        return HS_ECUDA;
+    }
+    return HS_OK;
+}
+
+int hs_launch_philox(uint64_t seed, uint64_t call, int32_t n, double *out, cudaStream_t st) {
+    philox_kernel<<<grid_for(n, 256), 256, 0, st>>>(seed, call, n, out);
+    return hs_check_launch("philox_kernel");
+}
+
+int hs_launch_exchange_energy(const HsLattice &L, float *E, float *Ep, cudaStream_t st) {
+    exchange_energy_kernel<<<grid_for((int64_t)L.nx * L.ny, 256), 256, 0, st>>>(L, E, Ep);
+    return hs_check_launch("exchange_energy_kernel");
+}
+
+int hs_launch_switch_energy(const HsLattice &L, float *dE, cudaStream_t st) {
+    switch_energy_kernel<<<grid_for((int64_t)L.nx * L.ny, 256), 256, 0, st>>>(L, dE);
+    return hs_check_launch("switch_energy_kernel");
+}
+
+extern "C" {
+
+int hs_version(void) { return 1; }
+
+int hs_last_error(char *buf, int len) {
+    if (!buf || len <= 0) return HS_EINVAL;
+    strncpy(buf, g_err, (size_t)len - 1);
+    buf[len - 1] = '\0';
+    return HS_OK;
+}
+
+int hs_struct_sizes(int32_t *out, int n) {
+    const int32_t s[5] = {(int32_t)sizeof(HsLattice), (int32_t)sizeof(HsCounters), (int32_t)sizeof(HsSwitchList),
+                          (int32_t)sizeof(HsGridPlan), (int32_t)offsetof(HsLattice, nx)};
+    for (int i = 0; i < n && i < 5; ++i) out[i] = s[i];
+    return HS_OK;
+}
+
+int hs_philox_uniform(uint64_t seed, uint64_t call, int32_t n, double *out, void *stream) {
+    if (n < 0 || (n > 0 && !out)) { hs_set_error("hs_philox_uniform: bad arguments"); return HS_EINVAL; }
+    if (n == 0) return HS_OK;
+    return hs_launch_philox(seed, call, n, out, (cudaStream_t)stream);
+}
+
+int hs_dipolar_update(const HsLattice *L, const HsSwitchList *sw, const int32_t *n_sw_dev, int32_t n_host,
+                      int32_t semantics, const HsCounters *C, void *stream) {
+    int rc = check_lattice(L, "hs_dipolar_update");
+    if (rc) return rc;
+    if (!L->has_dipolar) { hs_set_error("hs_dipolar_update: lattice has no dipolar energy"); return HS_EINVAL; }
+    if (!sw || (!n_sw_dev && n_host < 0) || (n_host > sw->cap && !n_sw_dev)) {
+        hs_set_error("hs_dipolar_update: bad switch list"); return HS_EINVAL;
+    }
+    if (semantics != HS_UPDATE_SINGLE && semantics != HS_UPDATE_MULTIPLE) {
+        hs_set_error("hs_dipolar_update: bad semantics"); return HS_EINVAL;
+    }
+    if (!n_sw_dev && n_host == 0) return HS_OK;
+    return hs_launch_dipolar_update(*L, *sw, n_sw_dev, n_host, semantics, C, (cudaStream_t)stream);
+}
+
+int hs_dipolar_full_direct(const HsLattice *L, int32_t fp64, double *E64, double *Ep64, void *stream) {
+    int rc = check_lattice(L, "hs_dipolar_full_direct");
+    if (rc) return rc;
+    if (!L->has_dipolar) { hs_set_error("hs_dipolar_full_direct: lattice has no dipolar energy"); return HS_EINVAL; }
+    if (L->use_perp && !L->Kps) { hs_set_error("hs_dipolar_full_direct: missing perp-self kernels"); return HS_EINVAL; }
+    if (fp64 && (!E64 || (L->use_perp && !Ep64))) { hs_set_error("hs_dipolar_full_direct: missing FP64 outputs"); return HS_EINVAL; }
+    return hs_launch_dipolar_full_direct(*L, fp64, E64, Ep64, (cudaStream_t)stream);
+}
+
+int64_t hs_igemm_scratch_bytes(const HsLattice *L, int32_t nsplit) {
+    if (check_lattice(L, "hs_igemm_scratch_bytes")) return -1;
+    return hs_igemm_scratch(*L, nsplit);
+}
+
+int hs_dipolar_full_igemm(const HsLattice *L, int32_t nsplit, void *scratch, int64_t scratch_bytes, void *stream) {
+    int rc = check_lattice(L, "hs_dipolar_full_igemm");
+    if (rc) return rc;
+    if (!L->has_dipolar) { hs_set_error("hs_dipolar_full_igemm: lattice has no dipolar energy"); return HS_EINVAL; }
+    return hs_launch_igemm(*L, nsplit, scratch, scratch_bytes, (cudaStream_t)stream);
+}
+
+int64_t hs_neel_scratch_bytes(const HsLattice *L) {
+    if (check_lattice(L, "hs_neel_scratch_bytes")) return -1;
+    return hs_neel_scratch(*L);
+}
+
+int hs_neel_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, double attempt_freq, void *scratch,
+                 int64_t scratch_bytes, void *stream) {
+    int rc = check_lattice(L, "hs_neel_step");
+    if (rc) return rc;
+    if (!C || !sw || !scratch) { hs_set_error("hs_neel_step: null argument"); return HS_EINVAL; }
+    if (!(attempt_freq > 0.0)) { hs_set_error("hs_neel_step: attempt_freq must be > 0"); return HS_EINVAL; }
+    return hs_launch_neel(*L, C, *sw, attempt_freq, scratch, scratch_bytes, (cudaStream_t)stream);
+}
+
+int64_t hs_metropolis_scratch_bytes(const HsLattice *L, const HsGridPlan *P) {
+    if (check_lattice(L, "hs_metropolis_scratch_bytes") || !P) return -1;
+    return hs_metropolis_scratch(*L, *P);
+}
+
+int hs_metropolis_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, const HsGridPlan *P, void *scratch,
+                       int64_t scratch_bytes, void *stream) {
+    int rc = check_lattice(L, "hs_metropolis_step");
+    if (rc) return rc;
+    if (!C || !sw || !P || !scratch) { hs_set_error("hs_metropolis_step: null argument"); return HS_EINVAL; }
+    if (P->sample_scheme == HS_SAMPLE_GRID && (!P->phase_off || !P->phase_yx || P->Rx < 1 || P->Ry < 1 || P->n_sc < 1)) {
+        hs_set_error("hs_metropolis_step: bad grid plan"); return HS_EINVAL;
+    }
+    if (P->sample_scheme == HS_SAMPLE_POISSON && !(P->r_cells >= 0.0)) {
+        hs_set_error("hs_metropolis_step: bad Poisson radius"); return HS_EINVAL;
+    }
+    return hs_launch_metropolis(*L, C, *sw, *P, scratch, scratch_bytes, (cudaStream_t)stream);
+}
+
+int64_t hs_wolff_scratch_bytes(const HsLattice *L) {
+    if (check_lattice(L, "hs_wolff_scratch_bytes")) return -1;
+    return hs_wolff_scratch(*L);
+}
+
+int hs_wolff_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, void *scratch, int64_t scratch_bytes,
+                  void *stream) {
+    int rc = check_lattice(L, "hs_wolff_step");
+    if (rc) return rc;
+    if (!C || !sw || !scratch) { hs_set_error("hs_wolff_step: null argument"); return HS_EINVAL; }
+    return hs_launch_wolff(*L, C, *sw, scratch, scratch_bytes, (cudaStream_t)stream);
+}
+
+int hs_exchange_energy(const HsLattice *L, float *E, float *E_perp, void *stream) {
+    int rc = check_lattice(L, "hs_exchange_energy");
+    if (rc) return rc;
+    if (!L->has_exchange || !E) { hs_set_error("hs_exchange_energy: no exchange energy / output"); return HS_EINVAL; }
+    return hs_launch_exchange_energy(*L, E, E_perp, (cudaStream_t)stream);
+}
+
+int hs_switch_energy(const HsLattice *L, float *dE, void *stream) {
+    int rc = check_lattice(L, "hs_switch_energy");
+    if (rc) return rc;
+    if (!dE) { hs_set_error("hs_switch_energy: null output"); return HS_EINVAL; }
+    return hs_launch_switch_energy(*L, dE, (cudaStream_t)stream);
+}
+
+}  // extern "C"

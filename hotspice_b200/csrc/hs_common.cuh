@@ -1,0 +1,192 @@
+// Shared device helpers of the sm_100a kinetic Monte Carlo kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <math.h>
+
+#include "../../include/hotspice_b200.h"
+
+#define HS_DEV __device__ __forceinline__
+
+// ---------------------------------------------------------------------------------------
+// Philox4x32-10 (Salmon et al., SC'11). Counter = (element, call_lo, call_hi, 0),
+// key = (seed_lo, seed_hi); u53 = ((w0 >> 5) * 2^26 + (w1 >> 6)) * 2^-53.
+// Must stay bit-identical to oracle/philox.py.
+// ---------------------------------------------------------------------------------------
+struct HsU4 { uint32_t x, y, z, w; };
+
+HS_DEV HsU4 hs_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+        const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+    return HsU4{c0, c1, c2, c3};
+}
+
+HS_DEV double hs_u53(uint64_t seed, uint64_t call, uint32_t element) {
+    HsU4 w = hs_philox(element, (uint32_t)call, (uint32_t)(call >> 32), 0u,
+                       (uint32_t)seed, (uint32_t)(seed >> 32));
+    const double hi = (double)(w.x >> 5), lo = (double)(w.y >> 6);
+    return (hi * 67108864.0 + lo) * (1.0 / 9007199254740992.0);
+}
+
+// Exponential variate E1 = -log1p(-u), accurate for small u and for u near 1.
+HS_DEV double hs_exp1_f64(double u) { return -log1p(-u); }
+
+// log(E1) in single precision (used only for the argmin key).
+HS_DEV float hs_log_exp1_f32(double u) {
+    float e1;
+    if (u < 0.5) e1 = -log1pf(-(float)u);
+    else e1 = -logf((float)(1.0 - u));
+    return logf(e1);
+}
+
+// ---------------------------------------------------------------------------------------
+// Lattice helpers
+// ---------------------------------------------------------------------------------------
+HS_DEV int hs_sub(const HsLattice &L, int y, int x) {
+    return L.sub_of[(y % L.uy) * L.ux + (x % L.ux)];
+}
+
+HS_DEV int hs_wrap(int v, int n) { v %= n; return v < 0 ? v + n : v; }
+
+// Minimum-image offset of d for period n, in [-(n/2), n - n/2 - 1].
+HS_DEV int hs_minimage(int d, int n) {
+    int r = hs_wrap(d, n);
+    return (2 * r >= n) ? r - n : r;
+}
+
+// Kernel value of sublattice `s` at (non-wrapped) offset (dy, dx), both in [-(n-1), n-1].
+// Window storage: (2wy+1, 2wx+1), centre at (wy, wx). In wrap mode the stored window is the
+// minimum-image crop of the periodically folded kernel.
+HS_DEV float hs_kval(const HsLattice &L, const float *K, int s, int dy, int dx) {
+    if (L.dip_wrap) { dy = hs_minimage(dy, L.ny); dx = hs_minimage(dx, L.nx); }
+    if (dy < -L.dip_wy || dy > L.dip_wy || dx < -L.dip_wx || dx > L.dip_wx) return 0.f;
+    const int64_t W = (int64_t)(2 * L.dip_wx + 1), H = (int64_t)(2 * L.dip_wy + 1);
+    return __ldg(K + (int64_t)s * H * W + (int64_t)(dy + L.dip_wy) * W + (dx + L.dip_wx));
+}
+
+// Exchange energy at cell (y, x) from the spins (hotspice/energies.py:771-781), convolution
+// semantics with 'wrap' (PBC) or zero fill. Returns E and, for in-plane lattices, E_perp.
+HS_DEV void hs_exchange_at(const HsLattice &L, int y, int x, double &E, double &Ep) {
+    const int ch = L.nn_h / 2, cw = L.nn_w / 2;
+    E = 0.0; Ep = 0.0;
+    const int64_t i = (int64_t)y * L.nx + x;
+    if (!L.in_plane) {
+        int s = 0;
+        for (int a = 0; a < L.nn_h; ++a)
+            for (int b = 0; b < L.nn_w; ++b) {
+                const int w = L.nn[a * L.nn_w + b];
+                if (!w) continue;
+                int yy = y + ch - a, xx = x + cw - b;
+                if (L.pbc) { yy = hs_wrap(yy, L.ny); xx = hs_wrap(xx, L.nx); }
+                else if (yy < 0 || yy >= L.ny || xx < 0 || xx >= L.nx) continue;
+                s += w * (int)L.m[(int64_t)yy * L.nx + xx];
+            }
+        E = -L.J * ((double)s * (double)L.m[i]);
+    } else {
+        double smx = 0.0, smy = 0.0;
+        for (int a = 0; a < L.nn_h; ++a)
+            for (int b = 0; b < L.nn_w; ++b) {
+                const int w = L.nn[a * L.nn_w + b];
+                if (!w) continue;
+                int yy = y + ch - a, xx = x + cw - b;
+                if (L.pbc) { yy = hs_wrap(yy, L.ny); xx = hs_wrap(xx, L.nx); }
+                else if (yy < 0 || yy >= L.ny || xx < 0 || xx >= L.nx) continue;
+                const int64_t j = (int64_t)yy * L.nx + xx;
+                const double mj = (double)L.m[j];
+                smx += w * (double)L.orient[2 * j] * mj;
+                smy += w * (double)L.orient[2 * j + 1] * mj;
+            }
+        const double mi = (double)L.m[i];
+        const double mx = (double)L.orient[2 * i] * mi, my = (double)L.orient[2 * i + 1] * mi;
+        E = -L.J * (smx * mx + smy * my);
+        Ep = -L.J * (smy * mx - smx * my);
+    }
+}
+
+// Total energy E and perpendicular energy (before m_perp_factor) of cell i.
+HS_DEV void hs_energy_at(const HsLattice &L, int y, int x, double &E, double &Ep) {
+    const int64_t i = (int64_t)y * L.nx + x;
+    E = 0.0; Ep = 0.0;
+    if (L.has_dipolar) {
+        E += (double)L.E_dip[i];
+        if (L.use_perp) Ep += (double)L.E_dip_perp[i];
+    }
+    if (L.zee) {
+        const double mi = (double)L.m[i];
+        E += mi * (double)L.zee[i];
+        if (L.use_perp) Ep += mi * (double)L.zee_perp[i];
+    }
+    if (L.has_exchange) {
+        double e, ep;
+        hs_exchange_at(L, y, x, e, ep);
+        E += e;
+        if (L.use_perp) Ep += ep;
+    }
+}
+
+HS_DEV double hs_beta(const HsLattice &L, int64_t i) {
+    return L.beta_uniform > 0.0 ? L.beta_uniform : (double)L.beta[i];
+}
+
+// Effective barrier(s) of hotspice/core.py:625-656 for one occupied cell.
+HS_DEV void hs_barriers(const HsLattice &L, int y, int x, double &b1, double &b2) {
+    double E, Ep;
+    hs_energy_at(L, y, x, E, Ep);
+    const int64_t i = (int64_t)y * L.nx + x;
+    const double dE = -2.0 * E;      // switch_energy
+    const double Ecur = -dE / 2.0;    // E = -delta_E/2
+    const double EB = (double)L.E_B[i];
+    if (!L.use_perp) {
+        double b;
+        if (L.barrier_method == HS_BARRIER_SIMPLE) {
+            b = fmax(dE, EB - Ecur);
+        } else {
+            const double inv4 = 0.25 / EB;
+            const double q = dE * inv4 + 1.0;
+            b = (dE > 4.0 * EB) ? dE : fmin(EB * q * q, dE + 4.0 * EB);
+        }
+        b1 = b2 = b;
+    } else {
+        const double Ept = L.m_perp_factor * Ep;
+        b1 = fmax(dE, (EB + Ept) - Ecur);
+        b2 = fmax(dE, (EB - Ept) - Ecur);
+    }
+}
+
+// progress() stop rule of hotspice/core.py:753-760 with utils.lower_than (rtol 1e-10).
+HS_DEV bool hs_lower_than(double x, double y) {
+    return x < y && !(fabs(x - y) <= 1e-10 * fabs(y));
+}
+
+HS_DEV bool hs_progress_continue(const HsCounters *C, int n_occ) {
+    if (!C->progress) return true;
+    const double dt = C->t - C->t0;
+    const double dmc = (double)C->attempted / (double)n_occ - C->mc0;
+    return hs_lower_than(dt, C->t_max) && hs_lower_than(dmc, C->mc_max);
+}
+
+// Arg-min helpers: smaller key wins, ties go to the smaller index (numpy nanargmin).
+struct HsKeyIdx { double key; int idx; };
+HS_DEV HsKeyIdx hs_kmin(HsKeyIdx a, HsKeyIdx b) {
+    if (b.idx < 0) return a;
+    if (a.idx < 0) return b;
+    if (b.key < a.key || (b.key == a.key && b.idx < a.idx)) return b;
+    return a;
+}
+HS_DEV HsKeyIdx hs_warp_kmin(HsKeyIdx v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        HsKeyIdx w;
+        w.key = __shfl_xor_sync(0xffffffffu, v.key, o);
+        w.idx = __shfl_xor_sync(0xffffffffu, v.idx, o);
+        v = hs_kmin(v, w);
+    }
+    return v;
+}

@@ -1,0 +1,33 @@
+// Internal host-side declarations shared by the .cu translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <stdint.h>
+
+#include "../../include/hotspice_b200.h"
+
+// error reporting (hs_capi.cu)
+void hs_set_error(const char *fmt, ...);
+int hs_check_launch(const char *what);
+
+// launchers
+int hs_launch_dipolar_update(const HsLattice &L, const HsSwitchList &sw, const int32_t *n_sw_dev, int n_host,
+                             int semantics, const HsCounters *C, cudaStream_t st);
+int hs_launch_dipolar_full_direct(const HsLattice &L, int fp64, double *E64, double *Ep64, cudaStream_t st);
+int64_t hs_neel_scratch(const HsLattice &L);
+int hs_launch_neel(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, double attempt_freq,
+                   void *scratch, int64_t scratch_bytes, cudaStream_t st);
+int64_t hs_metropolis_scratch(const HsLattice &L, const HsGridPlan &P);
+int hs_launch_metropolis(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, const HsGridPlan &P,
+                         void *scratch, int64_t scratch_bytes, cudaStream_t st);
+int64_t hs_wolff_scratch(const HsLattice &L);
+int hs_launch_wolff(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, void *scratch,
+                    int64_t scratch_bytes, cudaStream_t st);
+int hs_launch_exchange_energy(const HsLattice &L, float *E, float *Ep, cudaStream_t st);
+int hs_launch_switch_energy(const HsLattice &L, float *dE, cudaStream_t st);
+int hs_launch_philox(uint64_t seed, uint64_t call, int32_t n, double *out, cudaStream_t st);
+int64_t hs_igemm_scratch(const HsLattice &L, int nsplit);
+int hs_launch_igemm(const HsLattice &L, int nsplit, void *scratch, int64_t scratch_bytes, cudaStream_t st);
+
+inline int64_t hs_align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }

@@ -1,0 +1,124 @@
+"""FP64 host construction of the dipolar interaction kernels and their device windows.
+
+Restates DipolarEnergy._initialize (hotspice/energies.py:176-288): one kernel per occupied
+unit-cell site, K_s[d] for every offset d = (dy, dx) in [-(n-1), n-1]^2, built from the
+distances accumulated along the (possibly non-uniform, unit-cell periodic) cell spacings,
+with the finite-size ("moment of inertia") correction of Politi & Pini (2002), scaled by
+mu0/4pi = 1e-7, and with the 8 neighbouring periodic images folded in when PBC is on.
+
+For the device the kernels are stored as float32 windows of half-width (wy, wx) around
+offset 0. A finite cutoff gives a small window (the bounding box of the non-zero kernel
+entries). With PBC and a window narrower than half the lattice, the *unfolded* window is
+stored and applied with minimum-image wrapping, which equals the folded kernel entry by
+entry because at most one periodic image lies inside the cutoff.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass
+class KernelSet:
+    K: np.ndarray            # (U, 2wy+1, 2wx+1) float64
+    Kps: np.ndarray          # perp-self
+    Kpo: np.ndarray          # perp-other
+    sub_of: np.ndarray       # (uy, ux) int32 kernel number or -1
+    wx: int
+    wy: int
+    wrap: bool
+    full: bool               # window spans every offset of the lattice
+
+
+def _site_kernels(nx, ny, ux, uy, y, x, dx_cell, dy_cell, ori, occ, in_plane, cutoff, decay, I):
+    """Unfolded FP64 kernels (normal, perp-self, perp-other) of unit-cell site (y, x)."""
+    H, W = 2 * ny - 1, 2 * nx - 1
+    # unit-cell phase of kernel column 0 / row 0 (so that column nx-1 is site x itself)
+    cols = (x - (nx - 1) + np.arange(W)) % ux
+    rows = (y - (ny - 1) + np.arange(H)) % uy
+    # positions relative to the centre, accumulated over the phase-shifted spacings
+    cx = np.cumsum(dx_cell[cols])
+    cy = np.cumsum(dy_cell[rows])
+    rx = (cx - cx[nx - 1])[None, :]
+    ry = (cy - cy[ny - 1])[:, None]
+    r2 = rx * rx + ry * ry
+    r2[ny - 1, nx - 1] = np.inf
+    r2 = np.where(r2 > cutoff * cutoff, np.inf, r2)
+    rinv = r2 ** -0.5
+    r3 = rinv ** (-decay)
+    r5 = rinv ** (-decay + 2)
+    ex, ey = rx * rinv, ry * rinv
+    if not in_plane:
+        o2 = occ[rows[:, None], cols[None, :]].astype(float)
+        k = o2 * (r3 + 9 * I / 2 * r5)
+        z = np.zeros_like(k)
+        return k, z, z
+    ox1, oy1 = ori[y, x]
+    ox2 = ori[rows[:, None], cols[None, :], 0]
+    oy2 = ori[rows[:, None], cols[None, :], 1]
+
+    def pair(ax, ay, bx, by):
+        a = ax * bx * (3 * ex * ex - 1) + ay * by * (3 * ey * ey - 1) + 3 * (ex * ey) * (ax * by + ay * bx)
+        c = ax * bx * (5 * ex * ex - 1) + ay * by * (5 * ey * ey - 1) + 5 * (ex * ey) * (ax * by + ay * bx)
+        return -r3 * a - 1.5 * I * r5 * c
+    return pair(ox1, oy1, ox2, oy2), pair(-oy1, ox1, ox2, oy2), pair(ox1, oy1, -oy2, ox2)
+
+
+def _fold(k, nx, ny):
+    """Add the 8 neighbouring periodic images (array-range limited), in place."""
+    src = k.copy()
+    H, W = 2 * ny - 1, 2 * nx - 1
+    for sy in (-1, 0, 1):
+        for sx in (-1, 0, 1):
+            if sy == 0 and sx == 0:
+                continue
+            # destination offsets d with d - (sy*ny, sx*nx) inside the array
+            d_y0, d_y1 = max(0, sy * ny), min(H, H + sy * ny)
+            d_x0, d_x1 = max(0, sx * nx), min(W, W + sx * nx)
+            k[d_y0:d_y1, d_x0:d_x1] += src[d_y0 - sy * ny:d_y1 - sy * ny, d_x0 - sx * nx:d_x1 - sx * nx]
+
+
+def build_kernels(mm, cutoff=np.inf, decay_exponent=-3) -> KernelSet:
+    nx, ny = mm.nx, mm.ny
+    ux, uy = mm.unitcell.x, mm.unitcell.y
+    I = (mm.major_axis ** 2 + mm.minor_axis ** 2) / 16
+    dx_cell = np.asarray(mm.dx[:ux], dtype=float)
+    dy_cell = np.asarray(mm.dy[:uy], dtype=float)
+    ori = mm.orientation[:uy, :ux] if mm.in_plane else None
+    occ = mm.occupation[:uy, :ux]
+    sub_of = -np.ones((uy, ux), dtype=np.int32)
+    ks, kps, kpo = [], [], []
+    for y in range(uy):
+        for x in range(ux):
+            if mm.in_plane:
+                if ori[y, x, 0] == 0 and ori[y, x, 1] == 0:
+                    continue
+            elif occ[y, x] == 0:
+                continue
+            k, a, b = _site_kernels(nx, ny, ux, uy, y, x, dx_cell, dy_cell, ori, occ, mm.in_plane,
+                                    cutoff, decay_exponent, I)
+            sub_of[y, x] = len(ks)
+            ks.append(k); kps.append(a); kpo.append(b)
+    if not ks:
+        raise ValueError('no occupied unit-cell site: nothing to build a dipolar kernel for')
+    K, Kps, Kpo = np.asarray(ks), np.asarray(kps), np.asarray(kpo)
+    nz = (K != 0) | (Kps != 0) | (Kpo != 0)
+    rows = np.nonzero(nz.any(axis=(0, 2)))[0]
+    cols = np.nonzero(nz.any(axis=(0, 1)))[0]
+    wy = int(np.max(np.abs(rows - (ny - 1)))) if rows.size else 0
+    wx = int(np.max(np.abs(cols - (nx - 1)))) if cols.size else 0
+    finite = np.isfinite(cutoff)
+    if mm.PBC and not (finite and 2 * wy + 1 <= ny and 2 * wx + 1 <= nx):
+        for arr in (K, Kps, Kpo):
+            for s in range(arr.shape[0]):
+                _fold(arr[s], nx, ny)
+        wy, wx, wrap = ny - 1, nx - 1, False
+    else:
+        wrap = bool(mm.PBC)
+        if not finite:
+            wy, wx = ny - 1, nx - 1
+    sl = np.s_[:, ny - 1 - wy:ny + wy, nx - 1 - wx:nx + wx]
+    scale = 1e-7  # mu0 / 4 pi
+    return KernelSet(K[sl] * scale, Kps[sl] * scale, Kpo[sl] * scale, sub_of, wx, wy, wrap,
+                     wy == ny - 1 and wx == nx - 1 and not wrap)

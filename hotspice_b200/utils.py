@@ -1,0 +1,50 @@
+"""Host-side helpers mirroring hotspice/utils.py (the parts the hot path needs)."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+
+def as_2D_array(value, shape) -> np.ndarray:
+    """Scalar -> constant array; array with prod(shape) values -> reshaped
+    (hotspice/utils.py:208-228). Always a float64 numpy array on the host."""
+    if isinstance(value, torch.Tensor):
+        value = value.detach().cpu().numpy()
+    if isinstance(value, list):
+        try:
+            value = np.asarray(value, dtype=float)
+        except ValueError:
+            raise ValueError("List of lists could not be converted to rectangular float64 array.")
+    if isinstance(value, np.ndarray) and value.size != 1:
+        if value.size != math.prod(shape):
+            raise ValueError(f"Incorrect shape: passed array of shape {value.shape} is not of desired shape {shape}.")
+        return np.asarray(value, dtype=float).reshape(shape)
+    return np.ones(shape, dtype=float) * float(np.asarray(value).reshape(-1)[0] if isinstance(value, np.ndarray) else value)
+
+
+def lower_than(x, y, rtol=1e-10):
+    """False if x is within rtol of y or larger (hotspice/utils.py:90-92)."""
+    return x < y and not (abs(x - y) <= rtol * abs(y))
+
+
+def check_repetition(arr, nx: int, ny: int) -> bool:
+    """True if ``arr`` is periodic with period nx along axis 1 and ny along axis 0
+    (the property of hotspice/utils.py:42-66)."""
+    arr = np.asarray(arr)
+    H, W = arr.shape[:2]
+    base = arr[:ny, :nx, ...]
+    reps = (math.ceil(H / ny), math.ceil(W / nx)) + (1,) * (arr.ndim - 2)
+    return bool(np.allclose(np.tile(base, reps)[:H, :W, ...], arr))
+
+
+def full_obj_name(obj) -> str:
+    cls = type(obj)
+    return f'{cls.__module__}.{cls.__qualname__}'
+
+
+def asnumpy(array) -> np.ndarray:
+    if isinstance(array, torch.Tensor):
+        return array.detach().cpu().numpy()
+    return np.asarray(array)

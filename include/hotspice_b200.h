@@ -1,0 +1,200 @@
+/*
+ * hotspice_b200.h — C ABI of the B200 (sm_100a) kinetic Monte Carlo engine.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers/sizes and an explicit CUDA
+ * stream (cudaStream_t passed as void*), returns an int status (HS_OK or a negative code,
+ * message via hs_last_error) and never allocates device memory: all buffers, including
+ * scratch, belong to the caller (the Python host layer allocates them as torch tensors).
+ * Launches are asynchronous; nothing here synchronises the stream.
+ *
+ * Reference interfaces each entry point replaces (paths inside the Hotspice project):
+ *   hs_dipolar_update        DipolarEnergy.update_single / update_multiple
+ *                            (hotspice/energies.py:310-329, 331-366)
+ *   hs_dipolar_full_direct   DipolarEnergy.update (hotspice/energies.py:290-308), direct sum
+ *   hs_dipolar_full_igemm    DipolarEnergy.update as a tensor-core implicit GEMM
+ *   hs_neel_step             Magnets._update_Néel + E_barrier + update_energy
+ *                            (hotspice/core.py:679-709, 625-656, 241-253)
+ *   hs_metropolis_step       Magnets._update_Metropolis + select/_select_grid/_select_single/
+ *                            _select_Poisson (hotspice/core.py:659-677, 456-570)
+ *   hs_wolff_step            Magnets._update_Wolff + _select_cluster_exchange
+ *                            (hotspice/core.py:711-718, 588-602)
+ *   hs_exchange_energy       ExchangeEnergy.update (hotspice/energies.py:771-781)
+ *   hs_philox_uniform        the variate stream that replaces numpy.random in the hot path
+ */
+#ifndef HOTSPICE_B200_H
+#define HOTSPICE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------ */
+#define HS_OK          0
+#define HS_EINVAL     -1   /* bad argument (size, pointer, unsupported combination)      */
+#define HS_ENOMEM     -2   /* caller-provided scratch too small                           */
+#define HS_ETIMEDOUT  -3   /* a bounded device loop gave up (flag in HsCounters.status)   */
+#define HS_ECUDA      -4   /* CUDA runtime error (launch failure etc.)                     */
+#define HS_ERANGE     -5   /* size beyond a compiled-in maximum                           */
+
+/* device-side status bits written to HsCounters.status */
+#define HS_ST_SELECT_RETRY   1   /* select() retried too often (no occupied sample)        */
+#define HS_ST_SWITCH_OVERFLOW 2  /* more switches than the switch list holds               */
+#define HS_ST_POISSON_OVERFLOW 4 /* Poisson-disc grid/queue capacity exceeded              */
+#define HS_ST_WOLFF_OVERFLOW 8   /* Wolff frontier capacity exceeded                       */
+
+/* update schemes / selection / barrier (SimParams values, hotspice/core.py:29-41) */
+#define HS_SCHEME_NEEL        0
+#define HS_SCHEME_METROPOLIS  1
+#define HS_SCHEME_WOLFF       2
+#define HS_SAMPLE_SINGLE      0
+#define HS_SAMPLE_GRID        1
+#define HS_SAMPLE_POISSON     2
+#define HS_BARRIER_SIMPLE     0
+#define HS_BARRIER_PARABOLIC  1
+
+/* update semantics of hs_dipolar_update */
+#define HS_UPDATE_SINGLE   0   /* add window, then negate E at the switch (update_single)   */
+#define HS_UPDATE_MULTIPLE 1   /* negate E at all switches, then add windows (update_multiple) */
+
+/*
+ * One lattice instance. All (ny, nx) fields are dense row-major device arrays.
+ * Pointers that a configuration does not use are NULL.
+ */
+typedef struct HsLattice {
+    /* -- 8-byte members ---------------------------------------------------------------- */
+    int8_t       *m;            /* spins -1/0/+1                                            */
+    const int8_t *occ;          /* occupation 0/1                                           */
+    float        *mm;           /* m * moment (dipolar source field)                        */
+    const float  *moment;       /* magnetic moment [A m^2]                                  */
+    const int32_t *nonzero;     /* (n_occ) flat indices of occupied cells, row-major         */
+    const int32_t *sub_of;      /* (uy*ux) unit-cell site -> kernel number, or -1           */
+    const float  *E_B;          /* anisotropy barrier [J]                                    */
+    const float  *beta;         /* 1/(kB T) [1/J]                                            */
+    const float  *K;            /* dipolar kernels (n_sub, 2wy+1, 2wx+1), prefactor excluded */
+    const float  *Kpo;          /* "perp-other" kernels, same shape, or NULL                 */
+    const float  *Kps;          /* "perp-self" kernels (full recompute only), or NULL        */
+    float        *E_dip;        /* dipolar energy [J]                                        */
+    float        *E_dip_perp;   /* dipolar perpendicular energy, or NULL                     */
+    const float  *zee;          /* Zeeman E_factor (E = m * zee), or NULL                    */
+    const float  *zee_perp;     /* Zeeman E_factor_perp, or NULL                             */
+    const float  *orient;       /* (ny, nx, 2) orientation, in-plane exchange only, or NULL */
+    const double *wolff_bond;   /* bond[c] = 1 - exp(-2 J / kBT * c), c = 0..24, uniform T, or NULL */
+    double        beta_uniform; /* 1/(kB T) when T is uniform, else 0                        */
+    double        J;            /* exchange coupling [J]                                     */
+    double        dip_pref;     /* DipolarEnergy.prefactor                                   */
+    double        m_perp_factor;
+    uint64_t      seed;         /* Philox key                                                */
+    /* -- 4-byte members ---------------------------------------------------------------- */
+    int32_t nx, ny;
+    int32_t ux, uy;             /* unit cell                                                 */
+    int32_t pbc;
+    int32_t in_plane;
+    int32_t use_perp;           /* USE_PERP_ENERGY                                           */
+    int32_t n_occ;
+    int32_t barrier_method;     /* HS_BARRIER_*                                              */
+    int32_t has_dipolar;
+    int32_t dip_wx, dip_wy;     /* kernel window half-widths                                 */
+    int32_t dip_wrap;           /* 1: PBC with a cropped (minimum-image) window              */
+    int32_t n_sub;
+    int32_t has_exchange;
+    int32_t nn_h, nn_w;         /* exchange nearest-neighbour mask size (odd, <= 5x5)        */
+    int32_t trunc_cutoff;       /* SIMULTANEOUS_SWITCHES_CONVOLUTION_OR_SUM_CUTOFF           */
+    int32_t trunc_size;         /* REDUCED_KERNEL_SIZE                                       */
+    int8_t  nn[28];             /* nearest-neighbour mask, row-major                         */
+} HsLattice;
+
+/* Device-resident per-instance counters (one struct in device memory). */
+typedef struct HsCounters {
+    double   t;            /* simulated time [s]                                            */
+    double   t0, mc0;      /* progress(): t and MCsteps at the start                         */
+    double   t_max, mc_max;/* progress(): limits (t_max also bounds a single Néel step)      */
+    int64_t  switches;
+    int64_t  attempted;
+    uint64_t rng_call;     /* next Philox call number                                        */
+    int32_t  status;       /* HS_ST_* bits                                                    */
+    int32_t  done;         /* progress(): stop condition reached                              */
+    int32_t  progress;     /* 1: evaluate the progress() stop rule before every step          */
+    int32_t  n_sw;         /* switches written by the last step                               */
+    int32_t  epoch;        /* Wolff cluster stamp                                             */
+    int32_t  steps;        /* steps executed                                                  */
+    double   bmin;         /* Néel: global minimum barrier of the last step                   */
+    double   last_time;    /* Néel: switching time drawn in the last step                     */
+    int64_t  near_threshold; /* decisions whose FP32 margin was below the stated tolerance   */
+    double   reserved[4];
+} HsCounters;
+
+/* Switch record list written by a step (device memory, capacity `cap`). */
+typedef struct HsSwitchList {
+    int32_t *y;
+    int32_t *x;
+    int32_t *mode;         /* 0: exact window, 1: truncated (REDUCED_KERNEL_SIZE) window      */
+    int32_t  cap;
+    int32_t  pad;
+} HsSwitchList;
+
+/* Metropolis selection plan, precomputed on the host from the geometry (hotspice/core.py:506-540). */
+typedef struct HsGridPlan {
+    const int32_t *phase_off;   /* (ux*uy + 1) offsets into phase_yx per supercell phase         */
+    const int32_t *phase_yx;    /* packed (oy << 16 | ox) occupied offsets inside one supercell   */
+    int32_t Rx, Ry;             /* supercell size in cells                                       */
+    int32_t snx, sny;           /* supercells per axis (every second one is sampled)             */
+    int32_t n_sc;               /* sampled supercells                                            */
+    int32_t sample_scheme;      /* HS_SAMPLE_*                                                   */
+    double  r_cells;            /* Poisson-disc radius in cell units                             */
+    int32_t poisson_k;          /* dart throws per active point                                  */
+    int32_t metropolis_time;    /* SimParams.METROPOLIS_TIME                                     */
+    double  attempt_freq;
+} HsGridPlan;
+
+/* ---- library ------------------------------------------------------------------------- */
+int hs_version(void);
+int hs_last_error(char *buf, int len);
+/* sizeof of the ABI structs, so bindings can check their mirrors */
+int hs_struct_sizes(int32_t *out, int n);
+
+/* n doubles u53 of Philox call `call` into out (device). */
+int hs_philox_uniform(uint64_t seed, uint64_t call, int32_t n, double *out, void *stream);
+
+/* ---- (a) incremental dipolar update --------------------------------------------------- */
+/* Applies the n switches listed in `sw` (device count *n_sw_dev, or n_host if n_sw_dev is
+ * NULL) to E_dip / E_dip_perp. m and mm must already hold the flipped spins. */
+int hs_dipolar_update(const HsLattice *L, const HsSwitchList *sw, const int32_t *n_sw_dev,
+                      int32_t n_host, int32_t semantics, const HsCounters *C, void *stream);
+
+/* ---- (b) full dipolar recompute ---------------------------------------------------------- */
+/* Direct sum over the kernel window. fp64 != 0 accumulates in double and writes double
+ * outputs E64/Ep64; otherwise FP32 into L->E_dip / L->E_dip_perp. */
+int hs_dipolar_full_direct(const HsLattice *L, int32_t fp64, double *E64, double *Ep64, void *stream);
+/* Tensor-core implicit GEMM (tcgen05, split-BF16 kernel, FP32 accumulation in TMEM).
+ * Writes L->E_dip (and E_dip_perp). `scratch` holds the split kernels; see hs_igemm_scratch_bytes. */
+int64_t hs_igemm_scratch_bytes(const HsLattice *L, int32_t nsplit);
+int hs_dipolar_full_igemm(const HsLattice *L, int32_t nsplit, void *scratch, int64_t scratch_bytes, void *stream);
+
+/* ---- (c) Néel-Arrhenius step ------------------------------------------------------------- */
+int64_t hs_neel_scratch_bytes(const HsLattice *L);
+int hs_neel_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, double attempt_freq,
+                 void *scratch, int64_t scratch_bytes, void *stream);
+
+/* ---- (d) Metropolis step (grid / single / Poisson-disc selection) ------------------------ */
+int64_t hs_metropolis_scratch_bytes(const HsLattice *L, const HsGridPlan *P);
+int hs_metropolis_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, const HsGridPlan *P,
+                       void *scratch, int64_t scratch_bytes, void *stream);
+
+/* ---- (e) Wolff cluster step (exchange-only lattices) ------------------------------------- */
+int64_t hs_wolff_scratch_bytes(const HsLattice *L);
+int hs_wolff_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw,
+                  void *scratch, int64_t scratch_bytes, void *stream);
+
+/* ---- helpers ------------------------------------------------------------------------------- */
+/* Exchange energy field E (and E_perp when use_perp) from the current spins. */
+int hs_exchange_energy(const HsLattice *L, float *E, float *E_perp, void *stream);
+/* Total switch energy dE = -2 E_total at every cell (NaN where unoccupied), for the API. */
+int hs_switch_energy(const HsLattice *L, float *dE, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HOTSPICE_B200_H */

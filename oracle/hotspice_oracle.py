@@ -719,3 +719,83 @@ def poisson_disc_cells(width, height, r, k, random):
     ox, oy = int(random() * width), int(random() * height)
     return [((p[0] + ox) % width, (p[1] + oy) % height) for p in pts
             if p[0] >= 0 and p[1] >= 0 and p[0] < lim_x and p[1] < lim_y]
+
+
+# ----------------------------------------------------------------------------------------
+# Lock-step helpers for parity tests: evaluate a step's decision without taking it, and
+# apply a decision made elsewhere (teacher forcing after a near-threshold disagreement).
+# ----------------------------------------------------------------------------------------
+def neel_decision(mm: OracleMagnets, attempt_freq=1e10):
+    """Log-domain keys of the next Néel step (same variates as _update_neel, call not
+    consumed): returns (keys, taus, bmin, attempt_freq_eff). keys is +inf where unoccupied."""
+    call = mm.rng.call
+    u = uniform_for(mm.rng.seed, call, mm.nx * mm.ny).reshape(mm.shape)
+    E1 = -np.log1p(-u)
+    with np.errstate(invalid='ignore', divide='ignore', over='ignore'):
+        if mm.USE_PERP_ENERGY:
+            b1, b2 = mm.E_barrier()
+            bmin = min(np.nanmin(b1), np.nanmin(b2))
+            a1, a2 = (b1 - bmin) * mm.beta, (b2 - bmin) * mm.beta
+            lo = np.minimum(a1, a2)
+            logscale = lo - np.log1p(np.exp(-np.abs(a1 - a2)))
+            af = attempt_freq / 2
+        else:
+            b = mm.E_barrier(min_only=True)
+            bmin = np.nanmin(b)
+            logscale = (b - bmin) * mm.beta
+            af = attempt_freq
+        keys = np.log(E1) + logscale
+    keys = np.where(mm.occupation.astype(bool), keys, np.inf)
+    return keys, np.exp(logscale) * E1, bmin, af
+
+
+def uniform_for(seed, call, n):
+    from .philox import uniform53
+    return uniform53(seed, call, n)
+
+
+def force_neel(mm: OracleMagnets, i, t_max=1.0, attempt_freq=1e10):
+    """Take the Néel step with switch index ``i`` (a (y, x) tuple, or None for 'no switch
+    within t_max'), consuming the step's call like _update_neel does."""
+    keys, taus, bmin, af = neel_decision(mm, attempt_freq)
+    mm.rng.call += 1
+    mm.attempted_switches += 1
+    if i is None:
+        mm.t += t_max
+        return None
+    time = taus[i] * np.exp(bmin * mm.beta[i]) / af
+    mm.m[i] *= -1
+    mm.switches += 1
+    mm.t += float(time)
+    mm.update_energy(np.asarray(i).reshape(2, -1))
+    return i
+
+
+def metropolis_decision(mm: OracleMagnets, Q=0.05, r=0, attempt_freq=1e10):
+    """Selection and acceptance inputs of the next Metropolis step: consumes the selection
+    calls (and the METROPOLIS_TIME call), returns (idx, p, u, dt) without consuming the
+    acceptance call or changing the state."""
+    idx = mm.select(r=mm.calc_r(Q) if r == 0 else r)
+    beta = mm.beta[idx[0], idx[1]]
+    with np.errstate(divide='ignore', over='ignore'):
+        p = np.clip(np.exp(-mm.switch_energy(idx) * beta), 1e-10, 1e10)
+        dt = 0.0
+        if mm.params['METROPOLIS_TIME']:
+            times = -np.log(mm.rng.random(size=idx.shape[1])) / attempt_freq / mm.n * \
+                np.exp(mm.E_barrier(idx, min_only=True) * beta)
+            dt = float(np.sum(times))
+    u = uniform_for(mm.rng.seed, mm.rng.call, idx.shape[1])
+    return idx, p, u, dt
+
+
+def force_metropolis(mm: OracleMagnets, idx, accepted_mask, dt):
+    """Apply a Metropolis step whose candidates were ``idx`` and accepted ``accepted_mask``."""
+    mm.rng.call += 1
+    mm.attempted_switches += idx.shape[1]
+    mm.t += dt
+    sw = idx[:, np.asarray(accepted_mask, dtype=bool)]
+    if sw.shape[1] > 0:
+        mm.m[sw[0], sw[1]] *= -1
+        mm.switches += sw.shape[1]
+        mm.update_energy(sw)
+    return sw

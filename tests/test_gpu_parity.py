@@ -1,0 +1,185 @@
+"""Parity of the CUDA path with the FP64 oracle (which is pinned to the reference).
+
+Tolerances (stated by the build's precision design):
+* energies: the device keeps E in FP32; max|E_gpu - E_oracle| / max|E_oracle| <= 2e-6 after the
+  run (<= 1e-6 right after a full recompute);
+* decisions: every Néel argmin / Metropolis acceptance / Wolff bond must equal the oracle's,
+  except where the decision margin is below the effect of a 1e-6 relative energy error
+  ("near-threshold"); those are counted, the oracle is then forced to the device's
+  decision so both continue in lock-step;
+* Wolff clusters are integer decisions against FP64 thresholds: exact, no exceptions.
+"""
+import numpy as np
+import pytest
+
+from cases import build_oracle, load_fixture, load_specs, rel_err
+from gpu_cases import build_product
+
+pytestmark = pytest.mark.gpu
+SPECS = load_specs()
+E_TOL = 1e-6
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+def _scheme(spec):
+    return spec.get('params', {}).get('UPDATE_SCHEME', 'Neel')
+
+
+def test_philox_device_matches_numpy():
+    import torch
+    from hotspice_b200 import _lib
+    from oracle.philox import uniform53
+    lib = _lib.load()
+    for seed, call, n in ((0, 0, 1000), (2 ** 64 - 1, 12345, 4097), (77, 2 ** 40 + 3, 33)):
+        out = torch.empty(n, dtype=torch.float64, device='cuda')
+        _lib.check(lib.hs_philox_uniform(seed, call, n, out.data_ptr(), torch.cuda.current_stream().cuda_stream))
+        assert np.array_equal(_np(out), uniform53(seed, call, n))
+
+
+@pytest.mark.parametrize('name', [n for n in SPECS if any(e['type'] == 'dipolar' for e in SPECS[n]['energies'])])
+def test_full_recompute_matches_oracle(name):
+    fx = load_fixture(name)
+    mp = build_product(name)
+    d = mp.get_energy('dipolar')
+    assert rel_err(_np(d.E), fx['E_dip_init']) < 1e-6
+    if mp.USE_PERP_ENERGY:
+        assert rel_err(_np(d.E_perp), fx['E_dip_perp_init']) < 1e-6
+    assert rel_err(_np(mp.E), fx['E_init']) < 1e-6
+    # single-precision accumulation of every (cell, kernel) product: cancellation between
+    # thousands of terms costs about one decimal digit
+    d.update(method='direct32')
+    assert rel_err(_np(d.E), fx['E_dip_init']) < 1e-5
+
+
+def _near_neel(mo, keys, i_dev, i_or, beta_max):
+    """Margin of choosing i_dev over the FP64 argmin i_or, against the effect of a 1e-6
+    relative energy error on two cells' barriers (each barrier moves by <= 2 dE)."""
+    Emax = np.max(np.abs(mo.E))
+    tol = 2 * 2 * 2 * E_TOL * Emax * beta_max + 1e-9
+    return keys[i_dev] - keys[i_or] <= tol
+
+
+@pytest.mark.parametrize('name', [n for n in SPECS if _scheme(SPECS[n]) in ('Neel',) and SPECS[n].get('steps')])
+def test_neel_lockstep(name):
+    from oracle.hotspice_oracle import force_neel, neel_decision
+    spec = SPECS[name]
+    mo = build_oracle(name)
+    mp = build_product(name)
+    near = 0
+    beta_max = float(np.max(mo.beta))
+    for s in range(spec['steps']):
+        keys, taus, bmin, af = neel_decision(mo)
+        flat = int(np.argmin(keys))
+        i_or = divmod(flat, mo.nx)
+        time = taus[i_or] * np.exp(bmin * mo.beta[i_or]) / af
+        sw_or = None if (time > 1 or np.isnan(time)) else i_or
+        sw_dev = mp.update()
+        if sw_dev != sw_or:
+            assert sw_dev is not None and sw_or is not None, f'step {s}: {sw_dev} vs {sw_or}'
+            assert _near_neel(mo, keys, sw_dev, i_or, beta_max), f'step {s}: {sw_dev} vs {sw_or} not near-threshold'
+            near += 1
+        force_neel(mo, sw_dev)
+    c = mp._read_counters()
+    assert int(c['rng_call']) == mo.rng.call
+    assert mp.attempted_switches == mo.attempted_switches
+    assert mp.switches == mo.switches
+    assert np.array_equal(_np(mp.m), mo.m)
+    assert rel_err(_np(mp.E), mo.E) < 2 * E_TOL
+    assert mp.t == pytest.approx(mo.t, rel=2e-2)
+    print(f'{name}: {spec["steps"]} steps, {near} near-threshold decisions')
+
+
+@pytest.mark.parametrize('name', [n for n in SPECS if _scheme(SPECS[n]) == 'Metropolis' and SPECS[n].get('steps')])
+def test_metropolis_lockstep(name):
+    from oracle.hotspice_oracle import force_metropolis, metropolis_decision
+    spec = SPECS[name]
+    kw = spec.get('update_kw', {})
+    mo = build_oracle(name)
+    mp = build_product(name)
+    near = 0
+    for s in range(spec['steps']):
+        idx, p, u, dt = metropolis_decision(mo, **kw)
+        acc_or = u < p
+        sw = mp.update(**kw)
+        got = {(int(a), int(b)) for a, b in zip(sw[0], sw[1])}
+        acc_dev = np.array([(int(a), int(b)) in got for a, b in zip(idx[0], idx[1])])
+        assert len(got) == int(acc_dev.sum()), f'step {s}: device switched a cell that was not a candidate'
+        diff = np.nonzero(acc_dev != acc_or)[0]
+        if diff.size:
+            Emax = np.max(np.abs(mo.E))
+            beta = mo.beta[idx[0], idx[1]]
+            band = p * beta * 2 * 2 * E_TOL * Emax * 1.01 + 1e-12
+            assert np.all(np.abs(u - p)[diff] <= band[diff]), f'step {s}: acceptance differs beyond tolerance'
+            near += diff.size
+        force_metropolis(mo, idx, acc_dev, dt)
+        assert mp._read_counters()['rng_call'] == mo.rng.call, f'step {s}: RNG call count diverged'
+    assert mp.attempted_switches == mo.attempted_switches
+    assert mp.switches == mo.switches
+    assert np.array_equal(_np(mp.m), mo.m)
+    assert rel_err(_np(mp.E), mo.E) < 2 * E_TOL
+    if spec.get('params', {}).get('METROPOLIS_TIME'):
+        assert mp.t == pytest.approx(mo.t, rel=2e-2)
+    print(f'{name}: {spec["steps"]} steps, {near} near-threshold acceptances')
+
+
+@pytest.mark.parametrize('name', [n for n in SPECS if _scheme(SPECS[n]) == 'Wolff'])
+def test_wolff_matches_reference_exactly(name):
+    """Integer cluster growth: identical clusters to the reference run, step by step."""
+    spec, fx = SPECS[name], load_fixture(name)
+    mp = build_product(name)
+    ys, xs = [], []
+    for s in range(spec['steps']):
+        c = mp.update()
+        ys += c[0].tolist(); xs += c[1].tolist()
+        assert mp.attempted_switches == fx['attempted'][s]
+        assert int(mp._read_counters()['rng_call']) == fx['calls'][s]
+    assert np.array_equal(ys, fx['sw_y']) and np.array_equal(xs, fx['sw_x'])
+    assert np.array_equal(_np(mp.m), fx['m_final'])
+    assert rel_err(_np(mp.E), fx['E_final']) < 1e-6
+
+
+@pytest.mark.parametrize('name', [n for n in SPECS if SPECS[n].get('progress')])
+def test_progress_matches_reference(name):
+    """progress() on the device (graph-replayed chunks, stop rule evaluated by the kernels)."""
+    spec, fx = SPECS[name], load_fixture(name)
+    mp = build_product(name)
+    dt, dmc = mp.progress(**spec['progress'])
+    assert dmc == pytest.approx(fx['progress'][1], rel=1e-12)
+    assert dt == pytest.approx(fx['progress'][0], rel=2e-2)
+    assert int(mp._read_counters()['rng_call']) == int(fx['progress_calls'])
+    assert np.array_equal(_np(mp.m), fx['m_final'])
+    assert rel_err(_np(mp.E), fx['E_final']) < 2 * E_TOL
+
+
+def test_progress_graph_equals_plain_launches():
+    """The graph-replayed device loop and plain per-step launches give identical states."""
+    import hotspice_b200 as hs
+    name = 'progress_pin16_metro'
+    spec = SPECS[name]
+    a = build_product(name, engine=hs.EngineConfig(use_graphs=True, graph_steps=8))
+    b = build_product(name, engine=hs.EngineConfig(use_graphs=False, graph_steps=8))
+    ra = a.progress(**spec['progress'])
+    rb = b.progress(**spec['progress'])
+    assert ra == rb
+    assert np.array_equal(_np(a.m), _np(b.m))
+    assert np.array_equal(_np(a.get_energy('dipolar')._E), _np(b.get_energy('dipolar')._E))
+
+
+def test_update_single_and_multiple_match_oracle():
+    """Energy plugin contract: update_single/update_multiple after flips in m."""
+    name = 'metro_oop32_trunc_pbc'
+    mo = build_oracle(name)
+    mp = build_product(name)
+    rng = np.random.default_rng(0)
+    for k in (1, 5, 25, 60):
+        flat = rng.choice(mo.nx * mo.ny, size=k, replace=False)
+        idx = np.asarray(np.unravel_index(np.sort(flat), mo.shape))
+        mo.m[idx[0], idx[1]] *= -1
+        m = mo.m.copy()
+        mp.m = m
+        mo.update_energy(idx)
+        mp.update_energy(idx)
+        assert rel_err(_np(mp.E), mo.E) < E_TOL, k
