@@ -426,6 +426,21 @@ class Magnets(ABC):
         for k, v in fields.items():
             rec[0][k] = v
         self._counters.copy_(torch.from_numpy(rec.view(np.uint8).copy()))
+        self._ctl = None
+
+    def _set_control(self, **fields):
+        """Asynchronously set counter fields (no host synchronisation): each value goes
+        through its own pinned staging buffer, ordered on the current stream."""
+        ctl = getattr(self, '_ctl', None) or {}
+        for k, v in fields.items():
+            if ctl.get(k) == v:
+                continue
+            dt = _lib.COUNTERS_DTYPE.fields[k][0]
+            off = _lib.COUNTERS_DTYPE.fields[k][1]
+            b = torch.from_numpy(np.array([v], dtype=dt).view(np.uint8)).pin_memory()
+            self._counters[off:off + b.numel()].copy_(b, non_blocking=True)
+            ctl[k] = v
+        self._ctl = ctl
 
     @property
     def t(self) -> float:
@@ -914,6 +929,21 @@ class Magnets(ABC):
             torch.cuda.current_stream(self.device).wait_stream(s)
             self._graphs[key] = g
         g.replay()
+
+    def run(self, steps: int, **kwargs):
+        """Engine extension (no reference counterpart): enqueue exactly ``steps`` update steps
+        of the current scheme on the device, without the progress() stop rule and without any
+        host synchronisation. Returns immediately; read counters / state to synchronise."""
+        if self._T_zero:
+            raise RuntimeError('run() with T=0 somewhere in the domain')
+        self._set_control(progress=0, done=0, t_max=float(kwargs.pop('t_max', math.inf)))
+        args_ = self._step_args(kwargs)
+        K = max(1, int(self.engine.graph_steps))
+        q, r = divmod(int(steps), K)
+        for _ in range(q):
+            self._run_chunk(args_, K)
+        if r:
+            self._run_chunk(args_, r)
 
     def _progress_stepwise(self, t_max: float = 1, MCsteps_max: float = 4., **kwargs):
         t_0, MCsteps_0 = self.t, self.MCsteps

@@ -162,6 +162,8 @@ HS_DEV void hs_barriers(const HsLattice &L, int y, int x, double &b1, double &b2
 
 // progress() stop rule of hotspice/core.py:753-760 with utils.lower_than (rtol 1e-10).
 HS_DEV bool hs_lower_than(double x, double y) {
+    // numpy.isclose treats an infinite y as close only to itself
+    if (isinf(y)) return x < y;
     return x < y && !(fabs(x - y) <= 1e-10 * fabs(y));
 }
 

@@ -26,6 +26,8 @@ def as_2D_array(value, shape) -> np.ndarray:
 
 def lower_than(x, y, rtol=1e-10):
     """False if x is within rtol of y or larger (hotspice/utils.py:90-92)."""
+    if math.isinf(y):  # numpy.isclose: an infinite y is close only to itself
+        return x < y
     return x < y and not (abs(x - y) <= rtol * abs(y))
 
 

@@ -131,7 +131,8 @@ def test_simparams_validation():
 def test_lower_than_matches_reference_rule():
     from hotspice_b200.utils import lower_than
     from oracle.hotspice_oracle import lower_than as ref
-    for x, y in [(1.0, 2.0), (1.0, 1.0 + 1e-11), (1 - 1e-12, 1.0), (2.0, 1.0), (0.0, 0.0), (-1.0, 0.0)]:
+    for x, y in [(1.0, 2.0), (1.0, 1.0 + 1e-11), (1 - 1e-12, 1.0), (2.0, 1.0), (0.0, 0.0), (-1.0, 0.0), (0.0, float('inf')),
+                 (float('inf'), float('inf')), (1.0, -float('inf'))]:
         assert lower_than(x, y) == ref(x, y)
 
 
