@@ -83,6 +83,8 @@ SIGNATURES = {
     'hs_metropolis_scratch_bytes': (C.c_int64, [C.POINTER(HsLattice), C.POINTER(HsGridPlan)]),
     'hs_metropolis_step': (C.c_int, [C.POINTER(HsLattice), P, C.POINTER(HsSwitchList), C.POINTER(HsGridPlan), P,
                                      C.c_int64, P]),
+    'hs_metropolis_step_noalloc': (C.c_int, [C.POINTER(HsLattice), P, C.POINTER(HsSwitchList),
+                                             C.POINTER(HsGridPlan), P]),
     'hs_wolff_scratch_bytes': (C.c_int64, [C.POINTER(HsLattice)]),
     'hs_wolff_step': (C.c_int, [C.POINTER(HsLattice), P, C.POINTER(HsSwitchList), P, C.c_int64, P]),
     'hs_exchange_energy': (C.c_int, [C.POINTER(HsLattice), P, P, P]),

@@ -183,6 +183,15 @@ int64_t hs_metropolis_scratch_bytes(const HsLattice *L, const HsGridPlan *P);
 int hs_metropolis_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, const HsGridPlan *P,
                        void *scratch, int64_t scratch_bytes, void *stream);
 
+/* Allocation-free variant of hs_metropolis_step (no counterpart in the reference). For callers
+ * that cannot allocate device memory: the working arrays live in a fixed 4 MiB device array
+ * inside the library, one per GPU, kept until the process exits. The first call on a device
+ * (with that device current) looks up the array's address; make it before any stream capture.
+ * Returns HS_ERANGE when the selection plan needs more than 4 MiB (hs_metropolis_scratch_bytes).
+ * All calls share the array: calls that overlap on the GPU race. */
+int hs_metropolis_step_noalloc(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, const HsGridPlan *P,
+                               void *stream);
+
 /* ---- (e) Wolff cluster step (exchange-only lattices) ------------------------------------- */
 int64_t hs_wolff_scratch_bytes(const HsLattice *L);
 int hs_wolff_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw,
