@@ -141,7 +141,7 @@ def measured_peaks():
 
 def profile_traffic():
     """Per-launch DRAM traffic of the update kernel from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, 'profiles', 'dip_update_kernel_pinwheel512.txt')
+    path = os.path.join(ROOT, 'profiles', 'engine_kernel_pinwheel512.txt')
     try:
         for line in open(path):
             if line.startswith('traffic_bytes_per_launch:'):
@@ -200,12 +200,15 @@ def run_product(args):
     dist, rank, ws, local = dist_setup()
     dev = torch.device('cuda', local)
     torch.cuda.set_device(dev)
-    from hotspice_b200 import _lib
+    from hotspice_b200.engine import Autotuner
+    mcs = args.mc_steps
     mm = build_product(dev, seed=SEED + rank)
     r = 20 * A
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     d = mm.get_energy('dipolar')
+    cs = Autotuner().tune(mm, steps=200, r=r) if not args.cluster_size else args.cluster_size
+    mm.engine.cluster_size = cs
 
     # pinned host copies of the start state for the end-to-end leg
     snap = {k: v.detach().clone() for k, v in (('m', mm._m_dev), ('mm', mm._mm_dev), ('E', d._E), ('Ep', d._Ep),
@@ -216,9 +219,9 @@ def run_product(args):
     h2d = sum(v.numel() * v.element_size() for v in host_in.values())
     d2h = host_out_m.numel() + host_out_c.numel()
 
-    # ---- device-resident throughput ------------------------------------------------------
+    # ---- device-resident throughput: one persistent launch per bench step ----------------
     for _ in range(args.warmup):
-        mm.run(STEPS_PER_BENCH_STEP, r=r)
+        mm.run(mcs, r=r)
     torch.cuda.synchronize(dev)
     c0 = mm._read_counters()
     if dist:
@@ -230,7 +233,7 @@ def run_product(args):
         for k in range(args.steps):
             flush.fill_(float(k))
             ev[k][0].record(stream)
-            mm.run(STEPS_PER_BENCH_STEP, r=r)
+            mm.run(mcs, r=r)
             ev[k][1].record(stream)
         torch.cuda.synchronize(dev)
     if dist:
@@ -241,41 +244,15 @@ def run_product(args):
     switches = int(c1['switches'] - c0['switches'])
     status = int(c1['status'])
 
-    # ---- representative update-kernel launch for the roofline -----------------------------
-    nsw = int(c1['n_sw'])
-    sw_t, sw_s = mm._sw
-    L = mm._lattice_struct()
-    lib = _lib.load()
-    reps = 200
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    E_save, Ep_save = d._E.clone(), d._Ep.clone()
-    # representative list: the mean switch count of the timed region, placed on the sampled
-    # supercell grid (every second 40-cell supercell), on occupied cells
-    k_rep = max(1, round(switches / (args.steps * STEPS_PER_BENCH_STEP)))
-    pos = [(40 + 80 * i, 41 + 80 * j) for i in range(6) for j in range(6)][:k_rep]
-    sw_t[0, :k_rep].copy_(torch.tensor([p[0] for p in pos], dtype=torch.int32))
-    sw_t[1, :k_rep].copy_(torch.tensor([p[1] for p in pos], dtype=torch.int32))
-    sw_t[2, :k_rep].zero_()
-    g = torch.cuda.CUDAGraph()
-    gs = torch.cuda.Stream(dev)
-    gs.wait_stream(stream)
-    with torch.cuda.graph(g, stream=gs):
-        for _ in range(reps):
-            lib.hs_dipolar_update(L, sw_s, None, k_rep, _lib.HS_UPDATE_MULTIPLE, None, gs.cuda_stream)
-    stream.wait_stream(gs)
-    g.replay()
-    flush.fill_(0.0)
-    e0.record(stream)
-    g.replay()
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    upd_ms = e0.elapsed_time(e1) / reps
-    d._E.copy_(E_save); d._Ep.copy_(Ep_save)
+    # ---- roofline of the fused engine kernel (the only kernel of a bench step) ------------
     ks = d.kernel_set
     W = (2 * ks.wx + 1) * (2 * ks.wy + 1)
-    alg_bytes = k_rep * W * (16 + 12)  # E f32 RMW + K + mm (16 B) and E_perp RMW + K_perp (12 B) per cell
+    # per switch: E f32 read+write, kernel, source m*mu (16 B) and E_perp read+write, perp kernel
+    # (12 B) for every window cell; per candidate: E, E_perp, Zeeman factor, beta-free E_B, spin
+    alg_bytes = (switches * W * 28 + attempts * 17) / args.steps
+    launch_ms = dev_ms / args.steps
     hbm, peak_kind = measured_peaks()
-    achieved = alg_bytes / (upd_ms * 1e-3) / 1e9
+    achieved = alg_bytes / (launch_ms * 1e-3) / 1e9
 
     # ---- end to end through the public API ------------------------------------------------
     mc_per_step = attempts / max(args.steps, 1) / mm.n
@@ -294,6 +271,7 @@ def run_product(args):
         d._E.copy_(host_in['E'], non_blocking=True)
         d._Ep.copy_(host_in['Ep'], non_blocking=True)
         mm._counters.copy_(host_in['C'], non_blocking=True)
+        mm._ctl = None
         dt_, dmc = mm.progress(t_max=math.inf, MCsteps_max=mc_per_step, r=r)
         e2e_att += int(round(dmc * mm.n))
         host_out_m.copy_(mm._m_dev, non_blocking=True)
@@ -316,23 +294,22 @@ def run_product(args):
         return
     value = attempts / (dev_ms * 1e-3)
     e2e_value = e2e_att / (e2e_ms * 1e-3)
-    launches = 2 * STEPS_PER_BENCH_STEP * args.steps
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded lattice, random start, lognormal E_B)",
         "config": {"workload": WORKLOAD, "lattice": "IP_Pinwheel", "nx": N, "ny": N, "magnets": mm.n,
-                   "steps_per_bench_step": STEPS_PER_BENCH_STEP, "l2": "flushed (256 MB write) between bench steps",
+                   "steps_per_bench_step": mcs, "l2": "flushed (256 MB write) between bench steps",
                    "parallelism": f"{ws} independent replicas" if ws > 1 else "single instance",
-                   "switches": switches, "device_status": status},
+                   "cluster_size": cs, "switches": switches, "attempts": attempts, "device_status": status},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": "Magnets.progress(t_max=inf, MCsteps_max=per-step share) with state restored from pinned host",
                 "wall_s": wall_e2e},
-        "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": "dip_update_kernel", "achieved": achieved, "peak": hbm,
+        "gpu_launches": launches_for(args.steps),
+        "roofline": {"bound": "hbm", "kernel": f"engine_kernel<{cs}>", "achieved": achieved, "peak": hbm,
                      "unit": "GB/s", "frac": achieved / hbm, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                     "traffic": profile_traffic(), "launch_us": upd_ms * 1e3, "switches_per_launch": k_rep,
-                     "algorithmic_bytes_per_launch": alg_bytes},
+                     "traffic": profile_traffic(), "launch_ms": launch_ms,
+                     "algorithmic_bytes_per_launch": alg_bytes, "window_cells": W},
         "clocks": sampler.summary(),
     }
     if not args.no_cpu_baseline:
@@ -345,6 +322,10 @@ def run_product(args):
         dist.destroy_process_group()
 
 
+def launches_for(steps):
+    return steps  # one persistent engine launch per bench step
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -354,6 +335,9 @@ def main():
     ap.add_argument('--ref-sample', type=int, default=40)
     ap.add_argument('--cpu-steps', type=int, default=400)
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--mc-steps', type=int, default=STEPS_PER_BENCH_STEP,
+                    help='Metropolis steps per bench step (the workload uses 1000)')
+    ap.add_argument('--cluster-size', type=int, default=0, help='CTAs per cluster (0: autotune)')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)

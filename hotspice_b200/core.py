@@ -72,7 +72,9 @@ class EngineConfig:
     resync_every: int = 0          # full dipolar recompute every N progress() steps (0: never)
     recompute: str = 'auto'        # 'auto' | 'direct64' | 'direct32' | 'igemm'
     direct_max_pairs: float = 4e11 # 'auto' uses the FP64 direct sum up to this many (cell, window) pairs
-    use_graphs: bool = True        # replay progress() chunks from captured CUDA graphs
+    persistent: bool = True        # run()/progress() as one persistent cluster launch (hs_engine_run)
+    cluster_size: int = 0          # CTAs per cluster for the persistent launch (0: cost model)
+    use_graphs: bool = True        # otherwise: replay progress() chunks from captured CUDA graphs
     graph_steps: int = 64          # steps per captured chunk
     igemm_splits: int = 3          # BF16 terms of the split kernel in the implicit GEMM
 
@@ -877,6 +879,10 @@ class Magnets(ABC):
             return self._progress_stepwise(t_max=t_max, MCsteps_max=MCsteps_max, **kwargs)
         if self._T_zero:
             raise RuntimeError('progress() with T=0 somewhere in the domain would never advance')
+        if self.engine.persistent:
+            from .engine import BatchEngine
+            return BatchEngine([self], cluster_size=self.engine.cluster_size or None).progress(
+                t_max=t_max, MCsteps_max=MCsteps_max, **kwargs)[0]
         c = self._read_counters()
         t0 = float(c['t'])
         mc0 = float(c['attempted']) / self.n
@@ -936,6 +942,9 @@ class Magnets(ABC):
         host synchronisation. Returns immediately; read counters / state to synchronise."""
         if self._T_zero:
             raise RuntimeError('run() with T=0 somewhere in the domain')
+        if self.engine.persistent:
+            self._engine_run(int(steps), kwargs)
+            return
         self._set_control(progress=0, done=0, t_max=float(kwargs.pop('t_max', math.inf)))
         args_ = self._step_args(kwargs)
         K = max(1, int(self.engine.graph_steps))
@@ -944,6 +953,37 @@ class Magnets(ABC):
             self._run_chunk(args_, K)
         if r:
             self._run_chunk(args_, r)
+
+    def _engine_run(self, steps, kwargs):
+        from .engine import BatchEngine
+        kw = dict(kwargs)
+        t_max = float(kw.pop('t_max', math.inf))
+        key = (steps, tuple(sorted((k, float(v)) for k, v in kw.items())), self._version, t_max,
+               self.engine.cluster_size)
+        cache = getattr(self, '_engine_cache', None)
+        if cache is None or cache[0] != key:
+            eng = BatchEngine([self], cluster_size=self.engine.cluster_size or None)
+            self._set_control(progress=0, done=0, t_max=t_max)
+            prepared = eng._prepare([steps], [kw])
+            self._engine_cache = cache = (key, eng, prepared)
+        else:
+            self._set_control(progress=0, done=0, t_max=t_max)
+        cache[1].launch(cache[2])
+
+    def _snapshot(self):
+        d = self._dipolar()
+        return {'m': self._m_dev.clone(), 'mm': self._mm_dev.clone(), 'C': self._counters.clone(),
+                'E': d._E.clone() if d is not None else None,
+                'Ep': d._Ep.clone() if d is not None and d._Ep is not None else None}
+
+    def _restore(self, snap):
+        d = self._dipolar()
+        self._m_dev.copy_(snap['m']); self._mm_dev.copy_(snap['mm']); self._counters.copy_(snap['C'])
+        if d is not None:
+            d._E.copy_(snap['E'])
+            if snap['Ep'] is not None:
+                d._Ep.copy_(snap['Ep'])
+        self._ctl = None
 
     def _progress_stepwise(self, t_max: float = 1, MCsteps_max: float = 4., **kwargs):
         t_0, MCsteps_0 = self.t, self.MCsteps

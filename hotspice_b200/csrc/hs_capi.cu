@@ -97,9 +97,9 @@ int hs_last_error(char *buf, int len) {
 }
 
 int hs_struct_sizes(int32_t *out, int n) {
-    const int32_t s[5] = {(int32_t)sizeof(HsLattice), (int32_t)sizeof(HsCounters), (int32_t)sizeof(HsSwitchList),
-                          (int32_t)sizeof(HsGridPlan), (int32_t)offsetof(HsLattice, nx)};
-    for (int i = 0; i < n && i < 5; ++i) out[i] = s[i];
+    const int32_t s[6] = {(int32_t)sizeof(HsLattice), (int32_t)sizeof(HsCounters), (int32_t)sizeof(HsSwitchList),
+                          (int32_t)sizeof(HsGridPlan), (int32_t)offsetof(HsLattice, nx), (int32_t)sizeof(HsInstance)};
+    for (int i = 0; i < n && i < 6; ++i) out[i] = s[i];
     return HS_OK;
 }
 
@@ -190,6 +190,15 @@ int hs_wolff_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, voi
     if (!C || !sw || !scratch) { hs_set_error("hs_wolff_step: null argument"); return HS_EINVAL; }
     return hs_launch_wolff(*L, C, *sw, scratch, scratch_bytes, (cudaStream_t)stream);
 }
+
+int hs_engine_run(const HsInstance *insts, int32_t n_inst, int32_t cluster_size, int32_t n_clusters, int32_t *work,
+                  void *stream) {
+    if (!insts || !work || n_inst < 0 || n_clusters <= 0) { hs_set_error("hs_engine_run: bad arguments"); return HS_EINVAL; }
+    if (n_inst == 0) return HS_OK;
+    return hs_launch_engine(insts, n_inst, cluster_size, n_clusters, work, (cudaStream_t)stream);
+}
+
+int hs_engine_max_clusters(int32_t cluster_size) { return hs_engine_max_clusters_impl(cluster_size); }
 
 int hs_exchange_energy(const HsLattice *L, float *E, float *E_perp, void *stream) {
     int rc = check_lattice(L, "hs_exchange_energy");

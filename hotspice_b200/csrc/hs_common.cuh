@@ -8,6 +8,7 @@
 #include "../../include/hotspice_b200.h"
 
 #define HS_DEV __device__ __forceinline__
+#define HS_HD __host__ __device__
 
 // ---------------------------------------------------------------------------------------
 // Philox4x32-10 (Salmon et al., SC'11). Counter = (element, call_lo, call_hi, 0),
@@ -86,9 +87,9 @@ HS_DEV void hs_exchange_at(const HsLattice &L, int y, int x, double &E, double &
                 int yy = y + ch - a, xx = x + cw - b;
                 if (L.pbc) { yy = hs_wrap(yy, L.ny); xx = hs_wrap(xx, L.nx); }
                 else if (yy < 0 || yy >= L.ny || xx < 0 || xx >= L.nx) continue;
-                s += w * (int)L.m[(int64_t)yy * L.nx + xx];
+                s += w * (int)__ldcg(L.m + (int64_t)yy * L.nx + xx);
             }
-        E = -L.J * ((double)s * (double)L.m[i]);
+        E = -L.J * ((double)s * (double)__ldcg(L.m + i));
     } else {
         double smx = 0.0, smy = 0.0;
         for (int a = 0; a < L.nn_h; ++a)
@@ -99,11 +100,11 @@ HS_DEV void hs_exchange_at(const HsLattice &L, int y, int x, double &E, double &
                 if (L.pbc) { yy = hs_wrap(yy, L.ny); xx = hs_wrap(xx, L.nx); }
                 else if (yy < 0 || yy >= L.ny || xx < 0 || xx >= L.nx) continue;
                 const int64_t j = (int64_t)yy * L.nx + xx;
-                const double mj = (double)L.m[j];
+                const double mj = (double)__ldcg(L.m + j);
                 smx += w * (double)L.orient[2 * j] * mj;
                 smy += w * (double)L.orient[2 * j + 1] * mj;
             }
-        const double mi = (double)L.m[i];
+        const double mi = (double)__ldcg(L.m + i);
         const double mx = (double)L.orient[2 * i] * mi, my = (double)L.orient[2 * i + 1] * mi;
         E = -L.J * (smx * mx + smy * my);
         Ep = -L.J * (smy * mx - smx * my);
@@ -115,11 +116,11 @@ HS_DEV void hs_energy_at(const HsLattice &L, int y, int x, double &E, double &Ep
     const int64_t i = (int64_t)y * L.nx + x;
     E = 0.0; Ep = 0.0;
     if (L.has_dipolar) {
-        E += (double)L.E_dip[i];
-        if (L.use_perp) Ep += (double)L.E_dip_perp[i];
+        E += (double)__ldcg(L.E_dip + i);
+        if (L.use_perp) Ep += (double)__ldcg(L.E_dip_perp + i);
     }
     if (L.zee) {
-        const double mi = (double)L.m[i];
+        const double mi = (double)__ldcg(L.m + i);
         E += mi * (double)L.zee[i];
         if (L.use_perp) Ep += mi * (double)L.zee_perp[i];
     }

@@ -14,63 +14,9 @@
 #include "hs_common.cuh"
 #include "hs_internal.h"
 
+#include "hs_steps.cuh"
+
 namespace {
-
-constexpr int HS_TY = 8;          // rows per tile (one warp per row)
-constexpr int HS_LOC = 512;       // switches staged in shared memory per pass
-
-struct SwInfo { int y, x, mode, sub; float mm; };
-
-// Does the window of switch (ys, mode) reach rows [t0, t0 + tn) (1-D test, axis length n)?
-HS_DEV bool hs_axis_overlap(int s, int half, int wrap, int n, int t0, int tn) {
-    if (wrap) {
-        if (2 * half + 1 >= n) return true;
-        const int ws = s - half;
-        return hs_wrap(t0 - ws, n) <= 2 * half || hs_wrap(ws - t0, n) < tn;
-    }
-    return !(s + half < t0 || s - half >= t0 + tn);
-}
-
-// Window half-width and wrap flag of a switch along one axis.
-HS_DEV void hs_window(const HsLattice &L, int mode, bool yaxis, int &half, int &wrap) {
-    const int n = yaxis ? L.ny : L.nx;
-    if (mode) {
-        half = L.trunc_size ? min(L.trunc_size, n - 1) : n - 1;
-        wrap = L.pbc;
-    } else {
-        half = yaxis ? L.dip_wy : L.dip_wx;
-        wrap = L.dip_wrap;
-    }
-}
-
-// Sum of kernel values that switch `w` contributes to target (y, x).
-HS_DEV void hs_contrib(const HsLattice &L, const SwInfo &w, int y, int x, float &acc, float &accp) {
-    if (!w.mode) {
-        const int dy = y - w.y, dx = x - w.x;
-        acc += w.mm * hs_kval(L, L.K, w.sub, dy, dx);
-        if (L.use_perp) accp += w.mm * hs_kval(L, L.Kpo, w.sub, dy, dx);
-        return;
-    }
-    const int ky = L.trunc_size ? min(L.trunc_size, L.ny - 1) : L.ny - 1;
-    const int kx = L.trunc_size ? min(L.trunc_size, L.nx - 1) : L.nx - 1;
-    int dys[2], dxs[2], ny_ = 0, nx_ = 0;
-    if (L.pbc) {
-        const int d0y = hs_wrap(y - w.y, L.ny), d0x = hs_wrap(x - w.x, L.nx);
-        if (d0y <= ky) dys[ny_++] = d0y;
-        if (d0y - L.ny >= -ky) dys[ny_++] = d0y - L.ny;
-        if (d0x <= kx) dxs[nx_++] = d0x;
-        if (d0x - L.nx >= -kx) dxs[nx_++] = d0x - L.nx;
-    } else {
-        const int dy = y - w.y, dx = x - w.x;
-        if (dy >= -ky && dy <= ky) dys[ny_++] = dy;
-        if (dx >= -kx && dx <= kx) dxs[nx_++] = dx;
-    }
-    for (int a = 0; a < ny_; ++a)
-        for (int b = 0; b < nx_; ++b) {
-            acc += w.mm * hs_kval(L, L.K, w.sub, dys[a], dxs[b]);
-            if (L.use_perp) accp += w.mm * hs_kval(L, L.Kpo, w.sub, dys[a], dxs[b]);
-        }
-}
 
 template <int VEC>
 __global__ void __launch_bounds__(32 * HS_TY)

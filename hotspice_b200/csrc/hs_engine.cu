@@ -1,0 +1,505 @@
+// Persistent cluster engine: many update steps of many lattice instances in one launch.
+//
+// Each thread-block cluster (CS CTAs, CS in {1, 2, 4, 8, 16}) repeatedly claims an instance
+// from a work counter and advances it by its step budget (or until the progress() stop
+// rule of hotspice/core.py:753-760 holds), with cluster barriers between the phases of a
+// step instead of kernel boundaries:
+//   Metropolis: [CTA 0] selection + acceptance + flips (metro_step_cta)  | barrier |
+//               [all]   dipolar update of the touched strips              | barrier |
+//   Néel:       [all]   barrier/log-time keys of a slice of the cells, CTA argmin -> CTA 0
+//                       through distributed shared memory                 | barrier |
+//               [CTA 0] final argmin, switching time, flip                | barrier |
+//               [all]   dipolar update                                    | barrier |
+//   Wolff:      [CTA 0] sparse cluster growth (wolff_step_cta)            | barrier |
+// Every branch that decides how many barriers are executed is taken on values every CTA of
+// the cluster reads after a barrier, so all CTAs always execute the same barrier sequence.
+//
+// The dipolar update distributes work items (switch k, window row, 32-column segment) over
+// all warps of the cluster. A strip (row, segment) is processed by the item of the first
+// switch whose window covers it, which accumulates the contributions of every covering
+// switch in list order: each strip is written once, deterministically, and the work is
+// proportional to the area the windows touch.
+#include <cooperative_groups.h>
+
+#include "hs_steps.cuh"
+#include "hs_internal.h"
+
+namespace cg = cooperative_groups;
+
+namespace {
+
+constexpr int ENG_NT = 512;     // threads per CTA
+constexpr int ENG_SWCAP = 512;  // switches staged per CTA in shared memory
+
+struct SwX {                    // staged switch with its window footprint
+    int y, x, mode, sub;
+    float mm;
+    int ylo, nrows;             // window rows: (ylo + i) mod ny, i < nrows
+    int sa0, sa1, sb0, sb1;     // covered 32-column segments: [sa0, sa1) and [sb0, sb1)
+    int items;                  // nrows * (segments)
+};
+
+HS_DEV void footprint(const HsLattice &L, SwX &w) {
+    int hy, wy, hx, wx;
+    hs_window(L, w.mode, true, hy, wy);
+    hs_window(L, w.mode, false, hx, wx);
+    const int nseg = (L.nx + 31) >> 5;
+    if (wy) {
+        if (2 * hy + 1 >= L.ny) { w.ylo = 0; w.nrows = L.ny; }
+        else { w.ylo = hs_wrap(w.y - hy, L.ny); w.nrows = 2 * hy + 1; }
+    } else {
+        const int lo = max(0, w.y - hy), hi = min(L.ny - 1, w.y + hy);
+        w.ylo = lo; w.nrows = hi - lo + 1;
+    }
+    w.sb0 = w.sb1 = 0;
+    if (wx && 2 * hx + 1 >= L.nx) { w.sa0 = 0; w.sa1 = nseg; }
+    else if (wx) {
+        const int lo = w.x - hx, hi = w.x + hx;
+        if (lo >= 0 && hi < L.nx) { w.sa0 = lo >> 5; w.sa1 = (hi >> 5) + 1; }
+        else if (lo < 0) { w.sa0 = 0; w.sa1 = (hi >> 5) + 1; w.sb0 = (lo + L.nx) >> 5; w.sb1 = nseg; }
+        else { w.sa0 = lo >> 5; w.sa1 = nseg; w.sb0 = 0; w.sb1 = ((hi - L.nx) >> 5) + 1; }
+        if (w.sb1 > w.sb0 && w.sb0 < w.sa1 && w.sa0 < w.sb1) {  // ranges touch: merge
+            w.sa0 = min(w.sa0, w.sb0); w.sa1 = max(w.sa1, w.sb1); w.sb0 = w.sb1 = 0;
+        }
+    } else {
+        const int lo = max(0, w.x - hx), hi = min(L.nx - 1, w.x + hx);
+        w.sa0 = lo >> 5; w.sa1 = (hi >> 5) + 1;
+    }
+    w.items = w.nrows * ((w.sa1 - w.sa0) + (w.sb1 - w.sb0));
+}
+
+HS_DEV bool covers(const HsLattice &L, const SwX &w, int row, int seg) {
+    int d = row - w.ylo;
+    if (d < 0) d += L.ny;
+    if (d >= w.nrows) return false;
+    return (seg >= w.sa0 && seg < w.sa1) || (seg >= w.sb0 && seg < w.sb1);
+}
+
+// item index -> (row, segment) of switch w
+HS_DEV void item_strip(const HsLattice &L, const SwX &w, int it, int &row, int &seg) {
+    const int na = w.sa1 - w.sa0, nb = w.sb1 - w.sb0, per = na + nb;
+    const int r = it / per, s = it % per;
+    row = w.ylo + r;
+    if (row >= L.ny) row -= L.ny;
+    seg = s < na ? w.sa0 + s : w.sb0 + (s - na);
+}
+
+// Stage the switch list into shared memory with footprints and an inclusive item prefix.
+HS_DEV int stage_switches(const HsLattice &L, const HsSwitchList &sw, int nsw, SwX *s_sw, int *s_pre) {
+    const int n = min(nsw, ENG_SWCAP);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        SwX w;
+        w.y = __ldcg(sw.y + k); w.x = __ldcg(sw.x + k); w.mode = sw.mode ? __ldcg(sw.mode + k) : 0;
+        w.sub = hs_sub(L, w.y, w.x);
+        w.mm = __ldcg(L.mm + (int64_t)w.y * L.nx + w.x);
+        footprint(L, w);
+        if (w.sub < 0) w.items = 0;
+        s_sw[k] = w;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int k = 0; k < n; ++k) { acc += s_sw[k].items; s_pre[k] = acc; }
+    }
+    __syncthreads();
+    return n;
+}
+
+// Contributions of staged switch w to the 4 cells x0..x0+3 of `row`.
+HS_DEV void contrib4(const HsLattice &L, const SwX &w, int row, int x0, float acc[4], float accp[4], bool neg[4]) {
+    if (!w.mode && !L.dip_wrap) {
+        // exact window without wrapping: one kernel row, consecutive columns
+        const int dy = row - w.y;
+        if (dy < -L.dip_wy || dy > L.dip_wy) return;
+        const int64_t W = 2 * L.dip_wx + 1, H = 2 * L.dip_wy + 1;
+        const int64_t base = (int64_t)w.sub * H * W + (int64_t)(dy + L.dip_wy) * W + (L.dip_wx - w.x);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int x = x0 + v, dx = x - w.x;
+            if (x < L.nx && dx >= -L.dip_wx && dx <= L.dip_wx) {
+                acc[v] += w.mm * __ldg(L.K + base + x);
+                if (L.use_perp) accp[v] += w.mm * __ldg(L.Kpo + base + x);
+            }
+            if (dy == 0 && dx == 0) neg[v] = true;
+        }
+        return;
+    }
+    SwInfo wi{w.y, w.x, w.mode, w.sub, w.mm};
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const int x = x0 + v;
+        if (x >= L.nx) continue;
+        hs_contrib(L, wi, row, x, acc[v], accp[v]);
+        if (w.y == row && w.x == x) neg[v] = true;
+    }
+}
+
+HS_DEV bool covers_seg(const HsLattice &L, const SwX &w, int row, int seg128) {
+    int d = row - w.ylo;
+    if (d < 0) d += L.ny;
+    if (d >= w.nrows) return false;
+    // 128-column segment seg128 spans 32-column segments [4 seg128, 4 seg128 + 4)
+    const int a0 = 4 * seg128, a1 = a0 + 4;
+    return (a0 < w.sa1 && w.sa0 < a1) || (a0 < w.sb1 && w.sb0 < a1);
+}
+
+// Dipolar update of the strips covered by the staged switches. Work item = (switch k, one
+// row of its window); warps gw = 0..nw-1 of the whole cluster take items gw, gw + nw, ...
+// Along the row the warp walks 128-column segments (4 cells per lane). A segment is written
+// by the item of the first switch covering it, which accumulates every covering switch in
+// list order.
+HS_DEV void update_items(const HsLattice &L, const SwX *s_sw, const int *s_pre, int n, int semantics, int gw, int nw,
+                         const HsSwitchList &sw, int nsw_total) {
+    if (n == 0) return;
+    const int lane = threadIdx.x & 31;
+    const float pref2 = (float)(2.0 * L.dip_pref);
+    const bool vec = (L.nx & 3) == 0;
+    int it0 = 0;
+    for (int k = 0; k < n; ++k) {
+        const SwX &wk = s_sw[k];
+        if (wk.sub < 0) continue;
+        const int nr = wk.nrows;
+        // first item index of this switch assigned to this warp
+        int r = gw - it0;
+        r %= nw; if (r < 0) r += nw;
+        for (; r < nr; r += nw) {
+            int row = wk.ylo + r;
+            if (row >= L.ny) row -= L.ny;
+            // 128-column segments this switch covers in this row
+            const int ranges[2][2] = {{wk.sa0 >> 2, (wk.sa1 + 3) >> 2}, {wk.sb0 >> 2, (wk.sb1 + 3) >> 2}};
+            for (int g = 0; g < 2; ++g) {
+                for (int seg = ranges[g][0]; seg < ranges[g][1]; ++seg) {
+                    if (g == 1 && seg >= ranges[0][0] && seg < ranges[0][1]) continue;  // already done in range 0
+                    bool owned = true;
+                    for (int q = 0; q < k; ++q)
+                        if (s_sw[q].sub >= 0 && covers_seg(L, s_sw[q], row, seg)) { owned = false; break; }
+                    if (!owned) continue;  // warp-uniform
+                    const int x0 = seg * 128 + lane * 4;
+                    float acc[4] = {0.f, 0.f, 0.f, 0.f}, accp[4] = {0.f, 0.f, 0.f, 0.f};
+                    bool neg[4] = {false, false, false, false};
+                    for (int q = k; q < n; ++q) {
+                        const SwX &w = s_sw[q];
+                        if (w.sub < 0 || !covers_seg(L, w, row, seg)) continue;
+                        contrib4(L, w, row, x0, acc, accp, neg);
+                    }
+                    for (int q = n; q < nsw_total; ++q) {  // beyond the staged ones: from global memory
+                        SwX w;
+                        w.y = __ldcg(sw.y + q); w.x = __ldcg(sw.x + q); w.mode = sw.mode ? __ldcg(sw.mode + q) : 0;
+                        w.sub = hs_sub(L, w.y, w.x);
+                        if (w.sub < 0) continue;
+                        w.mm = __ldcg(L.mm + (int64_t)w.y * L.nx + w.x);
+                        footprint(L, w);
+                        if (!covers_seg(L, w, row, seg)) continue;
+                        contrib4(L, w, row, x0, acc, accp, neg);
+                    }
+                    if (x0 >= L.nx) continue;
+                    const int64_t i = (int64_t)row * L.nx + x0;
+                    float mv[4], ev[4], pv[4];
+                    if (vec) {
+                        const float4 a = __ldcg(reinterpret_cast<const float4 *>(L.mm + i));
+                        const float4 e = __ldcg(reinterpret_cast<const float4 *>(L.E_dip + i));
+                        mv[0] = a.x; mv[1] = a.y; mv[2] = a.z; mv[3] = a.w;
+                        ev[0] = e.x; ev[1] = e.y; ev[2] = e.z; ev[3] = e.w;
+                        if (L.use_perp) {
+                            const float4 p = __ldcg(reinterpret_cast<const float4 *>(L.E_dip_perp + i));
+                            pv[0] = p.x; pv[1] = p.y; pv[2] = p.z; pv[3] = p.w;
+                        }
+                    } else {
+#pragma unroll
+                        for (int v = 0; v < 4; ++v) {
+                            const bool in = x0 + v < L.nx;
+                            mv[v] = in ? __ldcg(L.mm + i + v) : 0.f;
+                            ev[v] = in ? __ldcg(L.E_dip + i + v) : 0.f;
+                            pv[v] = (in && L.use_perp) ? __ldcg(L.E_dip_perp + i + v) : 0.f;
+                        }
+                    }
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) {
+                        if (semantics == HS_UPDATE_MULTIPLE) {
+                            if (neg[v]) { ev[v] = -ev[v]; pv[v] = -pv[v]; }
+                            ev[v] += pref2 * (mv[v] * acc[v]);
+                            pv[v] += pref2 * (mv[v] * accp[v]);
+                        } else {
+                            ev[v] += pref2 * (mv[v] * acc[v]);
+                            pv[v] += pref2 * (mv[v] * accp[v]);
+                            if (neg[v]) { ev[v] = -ev[v]; pv[v] = -pv[v]; }
+                        }
+                    }
+                    if (vec) {
+                        *reinterpret_cast<float4 *>(L.E_dip + i) = make_float4(ev[0], ev[1], ev[2], ev[3]);
+                        if (L.use_perp) *reinterpret_cast<float4 *>(L.E_dip_perp + i) = make_float4(pv[0], pv[1], pv[2], pv[3]);
+                    } else {
+                        for (int v = 0; v < 4 && x0 + v < L.nx; ++v) {
+                            L.E_dip[i + v] = ev[v];
+                            if (L.use_perp) L.E_dip_perp[i + v] = pv[v];
+                        }
+                    }
+                }
+            }
+        }
+        it0 += nr;
+    }
+}
+
+template <int CS>
+struct Sync {
+    HS_DEV static void all() {
+        if constexpr (CS == 1) __syncthreads();
+        else cg::this_cluster().sync();
+    }
+    HS_DEV static int rank() {
+        if constexpr (CS == 1) return 0;
+        else return (int)cg::this_cluster().block_rank();
+    }
+    template <typename T>
+    HS_DEV static void publish(T *local, T v) {  // rank 0 thread writes v into every CTA's copy
+        if constexpr (CS == 1) *local = v;
+        else {
+            cg::cluster_group c = cg::this_cluster();
+            for (int r = 0; r < CS; ++r) *c.map_shared_rank(local, r) = v;
+        }
+    }
+};
+
+HS_DEV HsKeyIdx eng_block_kmin(HsKeyIdx v, HsKeyIdx *sm) {
+    v = hs_warp_kmin(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) sm[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = (lane < (int)(blockDim.x >> 5)) ? sm[lane] : HsKeyIdx{0.0, -1};
+        v = hs_warp_kmin(v);
+    }
+    __syncthreads();
+    return v;
+}
+
+HS_DEV double eng_block_dmin(double v, double *sm) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) sm[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = (lane < (int)(blockDim.x >> 5)) ? sm[lane] : INFINITY;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    }
+    __syncthreads();
+    return v;
+}
+
+HS_DEV MetroScratch metro_scratch_of(const HsLattice &L, const HsGridPlan &P, void *base) {
+    int cap, gsz;
+    hs_metro_sizes(L, P, cap, gsz);
+    char *p = reinterpret_cast<char *>(base);
+    MetroScratch S;
+    S.cap = cap; S.gsz = gsz;
+    S.py = reinterpret_cast<int32_t *>(p); S.px = S.py + cap; p += hs_align_up_d(8LL * cap, 256);
+    S.grid = reinterpret_cast<int32_t *>(p); p += hs_align_up_d(4LL * gsz, 256);
+    S.ptx = reinterpret_cast<double *>(p); p += hs_align_up_d(8LL * gsz, 256);
+    S.pty = reinterpret_cast<double *>(p); p += hs_align_up_d(8LL * gsz, 256);
+    S.queue = reinterpret_cast<int32_t *>(p);
+    return S;
+}
+
+HS_DEV WolffScratch wolff_scratch_of(const HsLattice &L, void *base) {
+    const int64_t N = (int64_t)L.nx * L.ny;
+    char *p = reinterpret_cast<char *>(base);
+    WolffScratch S;
+    S.chk_ep = reinterpret_cast<int32_t *>(p); p += hs_align_up_d(4 * N, 256);
+    S.cl_ep = reinterpret_cast<int32_t *>(p); p += hs_align_up_d(4 * N, 256);
+    S.cl_layer = reinterpret_cast<int32_t *>(p); p += hs_align_up_d(4 * N, 256);
+    S.list = reinterpret_cast<int32_t *>(p); p += hs_align_up_d(4 * N, 256);
+    S.cand = reinterpret_cast<int32_t *>(p);
+    return S;
+}
+
+template <int CS>
+__global__ void __launch_bounds__(ENG_NT, 1) engine_kernel(const HsInstance *insts, int n_inst, int *work) {
+    __shared__ int s_inst, s_go;
+    __shared__ HsKeyIdx s_part[16];
+    __shared__ HsKeyIdx s_red[32];
+    __shared__ double s_dred[32];
+    __shared__ SwX s_sw[ENG_SWCAP];
+    __shared__ int s_pre[ENG_SWCAP];
+    __shared__ __align__(16) HsInstance s_I;
+    static_assert(sizeof(HsInstance) % 8 == 0, "HsInstance is copied in 8-byte words");
+    const int rank = Sync<CS>::rank();
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    for (;;) {
+        if (rank == 0 && threadIdx.x == 0) Sync<CS>::publish(&s_inst, atomicAdd(work, 1));
+        Sync<CS>::all();
+        const int ii = s_inst;
+        if (ii >= n_inst) break;
+        {   // stage the instance descriptor in shared memory (read through references below)
+            const unsigned long long *src = reinterpret_cast<const unsigned long long *>(insts + ii);
+            unsigned long long *dst = reinterpret_cast<unsigned long long *>(&s_I);
+            for (int k = threadIdx.x; k < (int)(sizeof(HsInstance) / 8); k += blockDim.x) dst[k] = __ldg(src + k);
+            __syncthreads();
+        }
+        const HsInstance &I = s_I;
+        const HsLattice &L = s_I.L;
+        const HsSwitchList &sw = s_I.sw;
+        const HsGridPlan &P = s_I.P;
+        HsCounters *C = s_I.C;
+        const int scheme = s_I.scheme;
+        for (int64_t st = 0;; ++st) {
+            if (rank == 0 && threadIdx.x == 0) {
+                int go;
+                if (C->done) go = 0;
+                else if (C->progress) { go = hs_progress_continue(C, L.n_occ); if (!go) { C->done = 1; C->n_sw = 0; } }
+                else go = st < I.steps;
+                Sync<CS>::publish(&s_go, go);
+            }
+            Sync<CS>::all();
+            if (!s_go) break;
+            if (scheme == HS_SCHEME_METROPOLIS) {
+                if (rank == 0) metro_step_cta(L, C, sw, P, metro_scratch_of(L, P, I.scratch));
+                Sync<CS>::all();
+                if (L.has_dipolar) {
+                    const int nsw = __ldcg(&C->n_sw);
+                    const int n = stage_switches(L, sw, nsw, s_sw, s_pre);
+                    update_items(L, s_sw, s_pre, n, HS_UPDATE_MULTIPLE, rank * nwarps + warp, CS * nwarps, sw, nsw);
+                }
+                Sync<CS>::all();
+            } else if (scheme == HS_SCHEME_NEEL) {
+                const uint64_t call = __ldcg(&C->rng_call);
+                const int64_t N = (int64_t)L.nx * L.ny;
+                const int64_t gt = (int64_t)rank * blockDim.x + threadIdx.x, gs = (int64_t)CS * blockDim.x;
+                const bool unif = L.beta_uniform > 0.0;
+                double bmin = 0.0;
+                if (!unif) {  // b_min pass (hotspice/core.py:688, 696)
+                    double v = INFINITY;
+                    for (int64_t i = gt; i < N; i += gs) {
+                        if (!L.occ[i]) continue;
+                        double b1, b2;
+                        hs_barriers(L, (int)(i / L.nx), (int)(i % L.nx), b1, b2);
+                        v = fmin(v, fmin(b1, b2));
+                    }
+                    v = eng_block_dmin(v, s_dred);
+                    if (threadIdx.x == 0) {
+                        HsKeyIdx p{v, rank};
+                        if constexpr (CS == 1) s_part[0] = p;
+                        else *cg::this_cluster().map_shared_rank(&s_part[rank], 0) = p;
+                    }
+                    Sync<CS>::all();
+                    if (rank == 0 && threadIdx.x == 0) {
+                        double b = INFINITY;
+                        for (int r = 0; r < CS; ++r) b = fmin(b, s_part[r].key);
+                        C->bmin = b;
+                        Sync<CS>::publish(&s_dred[0], b);
+                    }
+                    Sync<CS>::all();
+                    bmin = s_dred[0];
+                    Sync<CS>::all();
+                }
+                HsKeyIdx best{0.0, -1};
+                const bool two = L.use_perp != 0;
+                for (int64_t i = gt; i < N; i += gs) {
+                    if (!L.occ[i]) continue;
+                    double b1, b2;
+                    hs_barriers(L, (int)(i / L.nx), (int)(i % L.nx), b1, b2);
+                    const double beta = hs_beta(L, i);
+                    const double u = hs_u53(L.seed, call, (uint32_t)i);
+                    const double le1 = (double)hs_log_exp1_f32(u);
+                    double key;
+                    if (!two) key = le1 + (b1 - bmin) * beta;
+                    else {
+                        const double bm = fmin(b1, b2), dd = fabs(b1 - b2);
+                        key = le1 + (bm - bmin) * beta - (double)log1pf(expf((float)(-dd * beta)));
+                    }
+                    best = hs_kmin(best, HsKeyIdx{key, (int)i});
+                }
+                best = eng_block_kmin(best, s_red);
+                if (threadIdx.x == 0) {
+                    if constexpr (CS == 1) s_part[0] = best;
+                    else *cg::this_cluster().map_shared_rank(&s_part[rank], 0) = best;
+                }
+                Sync<CS>::all();
+                if (rank == 0 && threadIdx.x == 0) {
+                    HsKeyIdx w{0.0, -1};
+                    for (int r = 0; r < CS; ++r) w = hs_kmin(w, s_part[r]);
+                    neel_finalize(L, C, sw, w, call, bmin, unif, two, I.attempt_freq);
+                }
+                Sync<CS>::all();
+                if (L.has_dipolar) {
+                    const int nsw = __ldcg(&C->n_sw);
+                    const int n = stage_switches(L, sw, nsw, s_sw, s_pre);
+                    update_items(L, s_sw, s_pre, n, HS_UPDATE_SINGLE, rank * nwarps + warp, CS * nwarps, sw, nsw);
+                }
+                Sync<CS>::all();
+            } else {  // Wolff
+                if (rank == 0) wolff_step_cta(L, C, sw, wolff_scratch_of(L, I.scratch));
+                Sync<CS>::all();
+            }
+        }
+        Sync<CS>::all();
+    }
+}
+
+template <int CS>
+int launch_engine(const HsInstance *insts, int n_inst, int *work, int n_clusters, cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(n_clusters * CS, 1, 1);
+    cfg.blockDim = dim3(ENG_NT, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CS;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (CS > 8) {
+        cudaError_t e = cudaFuncSetAttribute(engine_kernel<CS>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) { hs_set_error("engine: cluster size %d not allowed: %s", CS, cudaGetErrorString(e)); return HS_ECUDA; }
+    }
+    cudaError_t e = cudaLaunchKernelEx(&cfg, engine_kernel<CS>, insts, n_inst, work);
+    if (e != cudaSuccess) { hs_set_error("engine launch (cluster %d x %d): %s", CS, n_clusters, cudaGetErrorString(e)); return HS_ECUDA; }
+    return hs_check_launch("engine_kernel");
+}
+
+}  // namespace
+
+int hs_launch_engine(const HsInstance *insts, int n_inst, int cluster_size, int n_clusters, int *work, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(work, 0, sizeof(int), st);
+    if (e != cudaSuccess) { hs_set_error("engine: work counter reset: %s", cudaGetErrorString(e)); return HS_ECUDA; }
+    switch (cluster_size) {
+        case 1: return launch_engine<1>(insts, n_inst, work, n_clusters, st);
+        case 2: return launch_engine<2>(insts, n_inst, work, n_clusters, st);
+        case 4: return launch_engine<4>(insts, n_inst, work, n_clusters, st);
+        case 8: return launch_engine<8>(insts, n_inst, work, n_clusters, st);
+        case 16: return launch_engine<16>(insts, n_inst, work, n_clusters, st);
+        default: hs_set_error("engine: cluster size must be 1, 2, 4, 8 or 16"); return HS_EINVAL;
+    }
+}
+
+int hs_engine_max_clusters_impl(int cluster_size) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cluster_size, 1, 1);
+    cfg.blockDim = dim3(ENG_NT, 1, 1);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster_size;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    cudaError_t e;
+    switch (cluster_size) {
+        case 1: e = cudaOccupancyMaxActiveClusters(&n, engine_kernel<1>, &cfg); break;
+        case 2: e = cudaOccupancyMaxActiveClusters(&n, engine_kernel<2>, &cfg); break;
+        case 4: e = cudaOccupancyMaxActiveClusters(&n, engine_kernel<4>, &cfg); break;
+        case 8: e = cudaOccupancyMaxActiveClusters(&n, engine_kernel<8>, &cfg); break;
+        case 16:
+            cudaFuncSetAttribute(engine_kernel<16>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            e = cudaOccupancyMaxActiveClusters(&n, engine_kernel<16>, &cfg); break;
+        default: hs_set_error("engine: bad cluster size"); return HS_EINVAL;
+    }
+    if (e != cudaSuccess) { hs_set_error("cudaOccupancyMaxActiveClusters: %s", cudaGetErrorString(e)); return HS_ECUDA; }
+    return n;
+}

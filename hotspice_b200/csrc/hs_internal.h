@@ -30,4 +30,8 @@ int hs_launch_philox(uint64_t seed, uint64_t call, int32_t n, double *out, cudaS
 int64_t hs_igemm_scratch(const HsLattice &L, int nsplit);
 int hs_launch_igemm(const HsLattice &L, int nsplit, void *scratch, int64_t scratch_bytes, cudaStream_t st);
 
+int hs_launch_engine(const HsInstance *insts, int n_inst, int cluster_size, int n_clusters, int *work,
+                     cudaStream_t st);
+int hs_engine_max_clusters_impl(int cluster_size);
+
 inline int64_t hs_align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }

@@ -9,7 +9,7 @@
 // otherwise a first pass finds b_min. Each CTA reduces (key, index) with warp shuffles (ties go
 // to the smaller index, like numpy.nanargmin); the last CTA to finish (atomic ticket) reduces
 // the per-CTA results, evaluates the switching time in FP64 and applies the switch.
-#include "hs_common.cuh"
+#include "hs_steps.cuh"
 #include "hs_internal.h"
 
 namespace {
@@ -135,47 +135,7 @@ neel_scan_kernel(HsLattice L, HsCounters *C, HsSwitchList sw, double attempt_fre
     w = block_kmin(w, sm);
     if (threadIdx.x != 0) return;
     S->ticket[0] = 0u;
-    C->rng_call = call + 1;
-    C->attempted += 1;
-    C->steps += 1;
-    const double t_eff = C->progress ? (C->t_max - (C->t - C->t0)) : C->t_max;
-    if (w.idx < 0) {  // no occupied cell: nanargmin would raise; record and stop
-        C->status |= HS_ST_SELECT_RETRY;
-        C->n_sw = 0;
-        C->t += t_eff;
-        return;
-    }
-    const int64_t i = w.idx;
-    const int y = (int)(i / L.nx), x = (int)(i % L.nx);
-    double b1, b2;
-    hs_barriers(L, y, x, b1, b2);
-    const double beta = hs_beta(L, i);
-    const double e1 = hs_exp1_f64(hs_u53(L.seed, call, (uint32_t)i));
-    double time;
-    if (!TWO) {
-        // time = E1 * exp((b - bmin) beta) * exp(bmin beta) / nu   (hotspice/core.py:698-700)
-        time = UNIF ? e1 * exp(b1 * beta) / attempt_freq
-                    : e1 * exp((b1 - bmin) * beta) * exp(bmin * beta) / attempt_freq;
-    } else {
-        const double bm = fmin(b1, b2), dd = fabs(b1 - b2);
-        // tau = E1 / (exp(-(b1-bmin) beta) + exp(-(b2-bmin) beta)); nu halves (core.py:691-693)
-        const double scale = exp((bm - bmin) * beta) / (1.0 + exp(-dd * beta));
-        time = e1 * scale * exp(bmin * beta) / (attempt_freq / 2.0);
-    }
-    C->last_time = time;
-    if (time > t_eff || isnan(time)) {
-        C->t += t_eff;
-        C->n_sw = 0;
-        return;
-    }
-    L.m[i] = (int8_t)(-L.m[i]);
-    L.mm[i] = -L.mm[i];
-    C->switches += 1;
-    C->t += time;
-    sw.y[0] = y;
-    sw.x[0] = x;
-    if (sw.mode) sw.mode[0] = 0;
-    C->n_sw = 1;
+    neel_finalize(L, C, sw, w, call, bmin, UNIF, TWO, attempt_freq);
 }
 
 }  // namespace

@@ -1,0 +1,686 @@
+// Step bodies shared by the standalone step kernels and the persistent cluster engine.
+#pragma once
+
+#include "hs_common.cuh"
+
+// ---- dipolar window helpers ----------------------------------------------------------
+
+constexpr int HS_TY = 8;          // rows per tile (one warp per row)
+constexpr int HS_LOC = 512;       // switches staged in shared memory per pass
+
+struct SwInfo { int y, x, mode, sub; float mm; };
+
+// Does the window of switch (ys, mode) reach rows [t0, t0 + tn) (1-D test, axis length n)?
+HS_DEV bool hs_axis_overlap(int s, int half, int wrap, int n, int t0, int tn) {
+    if (wrap) {
+        if (2 * half + 1 >= n) return true;
+        const int ws = s - half;
+        return hs_wrap(t0 - ws, n) <= 2 * half || hs_wrap(ws - t0, n) < tn;
+    }
+    return !(s + half < t0 || s - half >= t0 + tn);
+}
+
+// Window half-width and wrap flag of a switch along one axis.
+HS_DEV void hs_window(const HsLattice &L, int mode, bool yaxis, int &half, int &wrap) {
+    const int n = yaxis ? L.ny : L.nx;
+    if (mode) {
+        half = L.trunc_size ? min(L.trunc_size, n - 1) : n - 1;
+        wrap = L.pbc;
+    } else {
+        half = yaxis ? L.dip_wy : L.dip_wx;
+        wrap = L.dip_wrap;
+    }
+}
+
+// Sum of kernel values that switch `w` contributes to target (y, x).
+HS_DEV void hs_contrib(const HsLattice &L, const SwInfo &w, int y, int x, float &acc, float &accp) {
+    if (!w.mode) {
+        const int dy = y - w.y, dx = x - w.x;
+        acc += w.mm * hs_kval(L, L.K, w.sub, dy, dx);
+        if (L.use_perp) accp += w.mm * hs_kval(L, L.Kpo, w.sub, dy, dx);
+        return;
+    }
+    const int ky = L.trunc_size ? min(L.trunc_size, L.ny - 1) : L.ny - 1;
+    const int kx = L.trunc_size ? min(L.trunc_size, L.nx - 1) : L.nx - 1;
+    int dys[2], dxs[2], ny_ = 0, nx_ = 0;
+    if (L.pbc) {
+        const int d0y = hs_wrap(y - w.y, L.ny), d0x = hs_wrap(x - w.x, L.nx);
+        if (d0y <= ky) dys[ny_++] = d0y;
+        if (d0y - L.ny >= -ky) dys[ny_++] = d0y - L.ny;
+        if (d0x <= kx) dxs[nx_++] = d0x;
+        if (d0x - L.nx >= -kx) dxs[nx_++] = d0x - L.nx;
+    } else {
+        const int dy = y - w.y, dx = x - w.x;
+        if (dy >= -ky && dy <= ky) dys[ny_++] = dy;
+        if (dx >= -kx && dx <= kx) dxs[nx_++] = dx;
+    }
+    for (int a = 0; a < ny_; ++a)
+        for (int b = 0; b < nx_; ++b) {
+            acc += w.mm * hs_kval(L, L.K, w.sub, dys[a], dxs[b]);
+            if (L.use_perp) accp += w.mm * hs_kval(L, L.Kpo, w.sub, dys[a], dxs[b]);
+        }
+}
+
+
+// ---- Metropolis ------------------------------------------------------------------------
+
+constexpr int MT = 1024;              // threads of the step CTA
+constexpr int MAX_RETRY = 1 << 14;    // bound on select() retries before reporting
+
+struct MetroScratch {
+    int32_t *py, *px;                  // candidate positions (capacity cap)
+    int32_t *grid;                     // Poisson background grid (gsz)
+    double  *ptx, *pty;                // Poisson points (gsz)
+    int32_t *queue;                    // Poisson active list (gsz)
+    int32_t cap, gsz;
+};
+
+HS_DEV int block_excl_scan(int flag, int *warp_tot, int &total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned bal = __ballot_sync(0xffffffffu, flag);
+    if (lane == 0) warp_tot[warp] = __popc(bal);
+    __syncthreads();
+    if (warp == 0) {
+        int v = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
+        int incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) { int t = __shfl_up_sync(0xffffffffu, incl, o); if (lane >= o) incl += t; }
+        if (lane < (int)(blockDim.x >> 5)) warp_tot[lane] = incl - v;
+        if (lane == 31) warp_tot[32] = incl;
+    }
+    __syncthreads();
+    const int pre = warp_tot[warp] + __popc(bal & ((1u << lane) - 1u));
+    total = warp_tot[32];
+    __syncthreads();
+    return pre;
+}
+
+// Stable in-place compaction of (py, px)[0..n) keeping entries for which keep(y, x) holds.
+template <typename F>
+HS_DEV int block_compact(int32_t *py, int32_t *px, int n, F keep, int *warp_tot) {
+    int out = 0;
+    for (int base = 0; base < n; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        int y = 0, x = 0, f = 0;
+        if (i < n) { y = py[i]; x = px[i]; f = keep(y, x) ? 1 : 0; }
+        int tot;
+        const int pre = block_excl_scan(f, warp_tot, tot);
+        if (f) { py[out + pre] = y; px[out + pre] = x; }
+        out += tot;
+        __syncthreads();
+    }
+    return out;
+}
+
+HS_DEV int pymod(int a, int n) { int r = a % n; return r < 0 ? r + n : r; }
+
+// Poisson-disc dart throwing in cell units, executed by warp 0. Returns the number of points
+// written to (py, px) as nearest cell indices, and advances `call` by the variates consumed.
+HS_DEV int poisson_warp(const HsLattice &L, const HsGridPlan &P, const MetroScratch &S, uint64_t &call, int *status) {
+    const int lane = threadIdx.x & 31;
+    const double width = L.nx, height = L.ny;
+    const double r = P.r_cells + 1.0;
+    const double cs = r / sqrt(2.0);
+    const double rSq = r * r;
+    const int gw = (int)ceil(width / cs), gh = (int)ceil(height / cs);
+    const int gsz = gw * gh;
+    if (gsz > S.gsz) { if (lane == 0) *status |= HS_ST_POISSON_OVERFLOW; return 0; }
+    for (int g = lane; g < gsz; g += 32) S.grid[g] = -1;
+    __syncwarp();
+    auto rnd = [&]() { const double u = hs_u53(L.seed, call, 0u); call += 1; return u; };
+    const double p0x = (double)(int)(width * rnd());
+    const double p0y = (double)(int)(height * rnd());
+    int npts = 1, nq = 1;
+    if (lane == 0) { S.ptx[0] = p0x; S.pty[0] = p0y; S.queue[0] = 0; S.grid[(int)(p0x / cs) + (int)(p0y / cs) * gw] = 0; }
+    __syncwarp();
+    while (nq > 0) {
+        const int qi = (int)(rnd() * nq);
+        const int q = S.queue[qi];
+        // list.pop(qi): shift the tail left, preserving order
+        for (int j = qi + lane; j < nq - 1; j += 32) {
+            const int v = S.queue[j + 1];
+            __syncwarp(__activemask());
+            S.queue[j] = v;
+        }
+        __syncwarp();
+        nq -= 1;
+        const double qx = S.ptx[q], qy = S.pty[q];
+        for (int t = 0; t < P.poisson_k; ++t) {
+            const double alpha = 6.283185307179586 * rnd();
+            const double d = r * sqrt(3.0 * rnd() + 1.0);
+            const double px = qx + d * cos(alpha);
+            const double py = qy + d * sin(alpha);
+            if (!(0.0 <= px && px < width && 0.0 <= py && py < height)) continue;
+            const int gx = (int)(px / cs), gy = (int)(py / cs);
+            bool conflict = false;
+            if (lane < 25) {
+                const int xx = gx - 2 + lane / 5, yy = gy - 2 + lane % 5;
+                const int g = S.grid[pymod(xx + yy * gw, gsz)];
+                if (g >= 0) {
+                    double dx = fabs(px - S.ptx[g]), dy = fabs(py - S.pty[g]);
+                    if (dx > width * 0.5) dx -= width;
+                    if (dy > height * 0.5) dy -= height;
+                    conflict = (dx * dx + dy * dy) <= rSq;
+                }
+            }
+            if (__any_sync(0xffffffffu, conflict)) continue;
+            if (npts >= S.gsz) { if (lane == 0) *status |= HS_ST_POISSON_OVERFLOW; break; }
+            if (lane == 0) {
+                S.ptx[npts] = px; S.pty[npts] = py;
+                S.queue[nq] = npts;
+                S.grid[gx + gy * gw] = npts;
+            }
+            __syncwarp();
+            npts += 1; nq += 1;
+        }
+    }
+    __syncwarp();
+    // keep points with x < max(r, w - r), y < max(r, h - r) (PBC=True default), then offset
+    const double lx = fmax(r, width - r), ly = fmax(r, height - r);
+    const double ox = (double)(int)(rnd() * width), oy = (double)(int)(rnd() * height);
+    if (lane == 0) {
+        int k = 0;
+        for (int g = 0; g < gsz; ++g) {
+            const int p = S.grid[g];
+            if (p < 0) continue;
+            const double x = S.ptx[p], y = S.pty[p];
+            if (!(x >= 0.0 && y >= 0.0 && x < lx && y < ly)) continue;
+            const double fx = fmod(x + ox, width), fy = fmod(y + oy, height);
+            // nearest cell index, ties to the lower index
+            int ix = (int)floor(fx); if (fx - ix > 0.5) ix += 1; ix = min(max(ix, 0), L.nx - 1);
+            int iy = (int)floor(fy); if (fy - iy > 0.5) iy += 1; iy = min(max(iy, 0), L.ny - 1);
+            if (k < S.cap) { S.py[k] = iy; S.px[k] = ix; }
+            ++k;
+        }
+        if (k > S.cap) { *status |= HS_ST_POISSON_OVERFLOW; k = S.cap; }
+        S.grid[0] = k;  // hand the count back through memory
+    }
+    __syncwarp();
+    return S.grid[0];
+}
+
+// Block-wide exclusive scans of two flags at once (3 barriers in total).
+HS_DEV void block_excl_scan2(int f0, int f1, int *wt, int &pre0, int &pre1, int &tot0, int &tot1) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const unsigned b0 = __ballot_sync(0xffffffffu, f0), b1 = __ballot_sync(0xffffffffu, f1);
+    if (lane == 0) { wt[warp] = __popc(b0); wt[33 + warp] = __popc(b1); }
+    __syncthreads();
+    if (warp == 0) {
+        int v0 = lane < nw ? wt[lane] : 0, v1 = lane < nw ? wt[33 + lane] : 0;
+        int i0 = v0, i1 = v1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int a = __shfl_up_sync(0xffffffffu, i0, o), b = __shfl_up_sync(0xffffffffu, i1, o);
+            if (lane >= o) { i0 += a; i1 += b; }
+        }
+        if (lane < nw) { wt[lane] = i0 - v0; wt[33 + lane] = i1 - v1; }
+        if (lane == 31) { wt[32] = i0; wt[65] = i1; }
+    }
+    __syncthreads();
+    const unsigned below = (1u << lane) - 1u;
+    pre0 = wt[warp] + __popc(b0 & below);
+    pre1 = wt[33 + warp] + __popc(b1 & below);
+    tot0 = wt[32]; tot1 = wt[65];
+    __syncthreads();
+}
+
+// Grid-selection Metropolis step with one candidate per thread (n_sc <= blockDim.x), kept in
+// registers: the supercell filter, the offset and the occupation filter of
+// hotspice/core.py:534-553 and 484-487 become one pair of fused ballot scans. Returns false,
+// without side effects, when the step needs the rare branches (no candidate survives the
+// supercell filter -> _select_single, or none is occupied -> select() retries); the general
+// path then runs the step from the same RNG call.
+HS_DEV bool metro_grid_fast(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, const HsGridPlan &P,
+                            uint64_t call) {
+    __shared__ int wt[66];
+    __shared__ int s_bins[256];
+    __shared__ double s_tsum[32];
+    const int t = threadIdx.x;
+    int ox, oy;
+    if (L.pbc) {
+        ox = (int)floor(hs_u53(L.seed, call, 0u) * L.nx);
+        oy = (int)floor(hs_u53(L.seed, call + 1, 0u) * L.ny);
+    } else {
+        ox = -P.Rx + (int)floor(hs_u53(L.seed, call, 0u) * (2.0 * P.Rx));
+        oy = -P.Ry + (int)floor(hs_u53(L.seed, call + 1, 0u) * (2.0 * P.Ry));
+    }
+    if (P.Rx == L.nx) ox = 0;
+    if (P.Ry == L.ny) oy = 0;
+    const int phase = pymod(oy, L.uy) * L.ux + pymod(ox, L.ux);
+    const int off = P.phase_off[phase], len = P.phase_off[phase + 1] - off;
+    if (len <= 0) return false;
+    const int nscx = (min(P.snx, L.nx) + 1) / 2;
+    int ok = 0, valid = 0, x = 0, y = 0;
+    if (t < P.n_sc) {
+        const int pick = (int)floor(hs_u53(L.seed, call + 2, (uint32_t)t) * len);
+        const int yx = __ldg(P.phase_yx + off + pick);
+        x = 2 * (t % nscx) * P.Rx + (yx & 0xffff);
+        y = 2 * (t / nscx) * P.Ry + (yx >> 16);
+        if (L.pbc) {
+            ok = x < max(P.Rx, L.nx - P.Rx) && y < max(P.Ry, L.ny - P.Ry);
+            x = (x + ox) % L.nx; y = (y + oy) % L.ny;
+        } else {
+            x += ox; y += oy;
+            ok = x >= 0 && x < L.nx && y >= 0 && y < L.ny;
+        }
+        valid = ok && L.occ[(int64_t)y * L.nx + x] != 0;
+    }
+    int pre_ok, r, n_ok, k;
+    block_excl_scan2(ok, valid, wt, pre_ok, r, n_ok, k);
+    if (n_ok == 0 || k == 0) return false;  // block-uniform
+    const bool mtime = P.metropolis_time != 0;
+    const uint64_t call_time = call + 3;
+    const uint64_t call_acc = mtime ? call + 4 : call + 3;
+    if (t < 256) s_bins[t] = 0;
+    int acc = 0;
+    double tpart = 0.0;
+    long long near = 0;
+    if (valid) {
+        const int64_t i = (int64_t)y * L.nx + x;
+        double E, Ep;
+        hs_energy_at(L, y, x, E, Ep);
+        const double beta = hs_beta(L, i);
+        const double p = fmin(fmax(exp(2.0 * E * beta), 1e-10), 1e10);
+        if (mtime) {
+            double b1, b2;
+            hs_barriers(L, y, x, b1, b2);
+            const double u = hs_u53(L.seed, call_time, (uint32_t)r);
+            tpart = -log(u) / P.attempt_freq / (double)L.n_occ * exp(fmin(b1, b2) * beta);
+        }
+        const double u = hs_u53(L.seed, call_acc, (uint32_t)r);
+        acc = u < p;
+        if (fabs(u - p) <= p * beta * 2e-6 * fabs(E) && p < 1e10 && p > 1e-10) near = 1;
+    }
+    int pa, dummy, nacc, dtot;
+    block_excl_scan2(acc, 0, wt, pa, dummy, nacc, dtot);
+    const int bin = acc ? (x % L.ux) + (y % L.uy) * L.ux : 0;
+    if (acc) {
+        const int64_t i = (int64_t)y * L.nx + x;
+        L.m[i] = (int8_t)(-L.m[i]);
+        L.mm[i] = -L.mm[i];
+        if (pa < sw.cap) { sw.y[pa] = y; sw.x[pa] = x; }
+        atomicAdd(&s_bins[bin], 1);
+    }
+    if (mtime) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) tpart += __shfl_xor_sync(0xffffffffu, tpart, o);
+        if ((t & 31) == 0) s_tsum[t >> 5] = tpart;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) near += __shfl_xor_sync(0xffffffffu, near, o);
+    if ((t & 31) == 0 && near) atomicAdd((unsigned long long *)&C->near_threshold, (unsigned long long)near);
+    __syncthreads();
+    if (acc && sw.mode && pa < sw.cap) sw.mode[pa] = s_bins[bin] > L.trunc_cutoff ? 1 : 0;
+    if (t == 0) {
+        if (mtime) {
+            double ts = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) ts += s_tsum[w];
+            C->t += ts;
+        }
+        const int ncap = min(nacc, sw.cap);
+        C->attempted += k;
+        C->switches += ncap;
+        C->rng_call = call_acc + 1;
+        C->n_sw = ncap;
+        C->steps += 1;
+        if (nacc > sw.cap) C->status |= HS_ST_SWITCH_OVERFLOW;
+    }
+    __syncthreads();
+    return true;
+}
+
+// One Metropolis step executed by one CTA (selection, acceptance, flips, switch list).
+HS_DEV void metro_step_cta(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, const HsGridPlan &P,
+                           const MetroScratch &S) {
+    __shared__ int warp_tot[33];
+    __shared__ int s_k;
+    __shared__ uint64_t s_call;
+    __shared__ int s_status;
+    __shared__ int s_bins[256];
+    __shared__ double s_tsum[32];
+    if (C->done) return;
+    if (!hs_progress_continue(C, L.n_occ)) {
+        if (threadIdx.x == 0) { C->done = 1; C->n_sw = 0; }
+        return;
+    }
+    uint64_t call = C->rng_call;
+    if (P.sample_scheme == HS_SAMPLE_GRID && P.n_sc <= (int)blockDim.x && L.ux * L.uy <= 256 &&
+        metro_grid_fast(L, C, sw, P, call))
+        return;
+    if (threadIdx.x == 0) s_status = 0;
+    int k = 0;
+    int retry = 0;
+    for (; retry < MAX_RETRY; ++retry) {
+        // ---- selection -------------------------------------------------------------------
+        if (P.sample_scheme == HS_SAMPLE_GRID) {
+            int ox, oy;
+            if (L.pbc) {
+                ox = (int)floor(hs_u53(L.seed, call, 0u) * L.nx);
+                oy = (int)floor(hs_u53(L.seed, call + 1, 0u) * L.ny);
+            } else {
+                ox = -P.Rx + (int)floor(hs_u53(L.seed, call, 0u) * (2.0 * P.Rx));
+                oy = -P.Ry + (int)floor(hs_u53(L.seed, call + 1, 0u) * (2.0 * P.Ry));
+            }
+            if (P.Rx == L.nx) ox = 0;
+            if (P.Ry == L.ny) oy = 0;
+            const int phase = pymod(oy, L.uy) * L.ux + pymod(ox, L.ux);
+            const int off = P.phase_off[phase], len = P.phase_off[phase + 1] - off;
+            const int nscx = (min(P.snx, L.nx) + 1) / 2;
+            const int limx = max(P.Rx, L.nx - P.Rx), limy = max(P.Ry, L.ny - P.Ry);
+            // candidates, in the row-major supercell order of ixx[:sny:2, :snx:2].ravel()
+            for (int t = threadIdx.x; t < P.n_sc; t += blockDim.x) {
+                int ix = -1, iy = -1;
+                if (len > 0) {
+                    const int pick = (int)floor(hs_u53(L.seed, call + 2, (uint32_t)t) * len);
+                    const int yx = P.phase_yx[off + pick];
+                    ix = 2 * (t % nscx) * P.Rx + (yx & 0xffff);
+                    iy = 2 * (t / nscx) * P.Ry + (yx >> 16);
+                }
+                S.py[t] = iy; S.px[t] = ix;
+            }
+            if (len <= 0 && threadIdx.x == 0) s_status |= HS_ST_SELECT_RETRY;
+            __syncthreads();
+            const int nx = L.nx, ny = L.ny, pbc = L.pbc;
+            k = block_compact(S.py, S.px, P.n_sc, [&](int y, int x) {
+                if (x < 0) return false;
+                if (pbc) return x < limx && y < limy;
+                x += ox; y += oy;
+                return x >= 0 && x < nx && y >= 0 && y < ny;
+            }, warp_tot);
+            for (int t = threadIdx.x; t < k; t += blockDim.x) {
+                if (pbc) { S.px[t] = (S.px[t] + ox) % L.nx; S.py[t] = (S.py[t] + oy) % L.ny; }
+                else { S.px[t] += ox; S.py[t] += oy; }
+            }
+            call += 3;
+            __syncthreads();
+            if (k == 0) {  // no sample survived: _select_single (core.py:558)
+                const int i = (int)floor(hs_u53(L.seed, call, 0u) * L.n_occ);
+                if (threadIdx.x == 0) { const int f = L.nonzero[i]; S.py[0] = f / L.nx; S.px[0] = f % L.nx; }
+                call += 1;
+                k = 1;
+            }
+        } else if (P.sample_scheme == HS_SAMPLE_SINGLE) {
+            const int i = (int)floor(hs_u53(L.seed, call, 0u) * L.n_occ);
+            if (threadIdx.x == 0) { const int f = L.nonzero[i]; S.py[0] = f / L.nx; S.px[0] = f % L.nx; }
+            call += 1;
+            k = 1;
+        } else {  // Poisson
+            if (threadIdx.x < 32) {
+                uint64_t c = call;
+                int st = 0;
+                const int n = poisson_warp(L, P, S, c, &st);
+                if (threadIdx.x == 0) { s_k = n; s_call = c; s_status |= st; }
+            }
+            __syncthreads();
+            k = s_k;
+            call = s_call;
+        }
+        __syncthreads();
+        // ---- select(): drop unoccupied picks, retry if none is left (core.py:484-487) -------
+        const int8_t *occ = L.occ;
+        const int nx = L.nx;
+        k = block_compact(S.py, S.px, k, [&](int y, int x) { return occ[(int64_t)y * nx + x] != 0; }, warp_tot);
+        if (k > 0) break;
+    }
+    if (retry == MAX_RETRY) {
+        if (threadIdx.x == 0) { C->status |= HS_ST_SELECT_RETRY; C->rng_call = call; C->n_sw = 0; }
+        return;
+    }
+    // ---- acceptance --------------------------------------------------------------------------
+    const bool mtime = P.metropolis_time != 0;
+    const uint64_t call_time = call;
+    const uint64_t call_acc = mtime ? call + 1 : call;
+    if (threadIdx.x < 256) s_bins[threadIdx.x] = 0;
+    double tpart = 0.0;
+    long long near = 0;
+    int acc_base = 0;
+    __syncthreads();
+    for (int base = 0; base < k; base += blockDim.x) {
+        const int t = base + threadIdx.x;
+        int acc = 0, y = 0, x = 0;
+        if (t < k) {
+            y = S.py[t]; x = S.px[t];
+            const int64_t i = (int64_t)y * L.nx + x;
+            double E, Ep;
+            hs_energy_at(L, y, x, E, Ep);
+            const double dE = -2.0 * E;
+            const double beta = hs_beta(L, i);
+            const double p = fmin(fmax(exp(-dE * beta), 1e-10), 1e10);
+            if (mtime) {
+                double b1, b2;
+                hs_barriers(L, y, x, b1, b2);
+                const double u = hs_u53(L.seed, call_time, (uint32_t)t);
+                tpart += -log(u) / P.attempt_freq / (double)L.n_occ * exp(fmin(b1, b2) * beta);
+            }
+            const double u = hs_u53(L.seed, call_acc, (uint32_t)t);
+            acc = u < p;
+            // decision margin below a 1e-6 relative energy perturbation
+            if (fabs(u - p) <= p * beta * 2e-6 * fabs(E) && p < 1e10 && p > 1e-10) near += 1;
+        }
+        int tot;
+        const int pre = block_excl_scan(acc, warp_tot, tot);
+        if (acc) {
+            const int out = acc_base + pre;
+            if (out < sw.cap) { sw.y[out] = y; sw.x[out] = x; }
+        }
+        acc_base += tot;
+    }
+    const int nacc = acc_base;
+    // time sum (METROPOLIS_TIME)
+    if (mtime) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) tpart += __shfl_xor_sync(0xffffffffu, tpart, o);
+        if ((threadIdx.x & 31) == 0) s_tsum[threadIdx.x >> 5] = tpart;
+    }
+    // near-threshold count
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) near += __shfl_xor_sync(0xffffffffu, near, o);
+    if ((threadIdx.x & 31) == 0 && near) atomicAdd((unsigned long long *)&C->near_threshold, (unsigned long long)near);
+    __syncthreads();
+    const int ncap = min(nacc, sw.cap);
+    // flips and per-sublattice counts
+    for (int t = threadIdx.x; t < ncap; t += blockDim.x) {
+        const int y = sw.y[t], x = sw.x[t];
+        const int64_t i = (int64_t)y * L.nx + x;
+        L.m[i] = (int8_t)(-L.m[i]);
+        L.mm[i] = -L.mm[i];
+        const int bin = (x % L.ux) + (y % L.uy) * L.ux;
+        if (bin < 256) atomicAdd(&s_bins[bin], 1);
+    }
+    __syncthreads();
+    if (sw.mode)
+        for (int t = threadIdx.x; t < ncap; t += blockDim.x) {
+            const int y = sw.y[t], x = sw.x[t];
+            const int bin = (x % L.ux) + (y % L.uy) * L.ux;
+            sw.mode[t] = (bin < 256 && s_bins[bin] > L.trunc_cutoff) ? 1 : 0;
+        }
+    if (threadIdx.x == 0) {
+        if (mtime) {
+            double ts = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) ts += s_tsum[w];
+            C->t += ts;
+        }
+        C->attempted += k;
+        C->switches += ncap;
+        C->rng_call = call_acc + 1;
+        C->n_sw = ncap;
+        C->steps += 1;
+        C->status |= s_status;
+        if (nacc > sw.cap) C->status |= HS_ST_SWITCH_OVERFLOW;
+    }
+}
+
+// ---- Wolff -------------------------------------------------------------------------------
+
+constexpr int WT = 1024;
+
+struct WolffScratch {
+    int32_t *chk_ep;   // epoch in which the cell was checked (seed or frontier)
+    int32_t *cl_ep;    // epoch in which the cell joined the cluster
+    int32_t *cl_layer; // layer in which it joined
+    int32_t *list;     // cluster cells in BFS order (capacity N)
+    int32_t *cand;     // frontier of the current layer (capacity N)
+};
+
+// One Wolff cluster step executed by one CTA.
+HS_DEV void wolff_step_cta(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, const WolffScratch &S) {
+    __shared__ int s_ncand, s_nacc, s_epoch;
+    if (C->done) return;
+    if (!hs_progress_continue(C, L.n_occ)) {
+        if (threadIdx.x == 0) { C->done = 1; C->n_sw = 0; }
+        return;
+    }
+    const int nx = L.nx, ny = L.ny;
+    const int64_t N = (int64_t)nx * ny;
+    uint64_t call = C->rng_call;
+    if (threadIdx.x == 0) { s_epoch = C->epoch + 1; C->epoch = s_epoch; }
+    // seed: _select_single (np.random.randint(n) -> nonzero index)
+    const int seed = L.nonzero[(int)floor(hs_u53(L.seed, call, 0u) * L.n_occ)];
+    call += 1;
+    __syncthreads();
+    const int epoch = s_epoch;
+    const int8_t ms = L.m[seed];
+    if (threadIdx.x == 0) {
+        S.chk_ep[seed] = epoch;
+        S.cl_ep[seed] = epoch;
+        S.cl_layer[seed] = 0;
+        S.list[0] = seed;
+    }
+    int lstart = 0, lend = 1;
+    const int ch = L.nn_h / 2, cw = L.nn_w / 2;
+    const double m2J = -2.0 * L.J;
+    int layer = 1;
+    for (; layer <= (int)N + 1; ++layer) {
+        if (threadIdx.x == 0) { s_ncand = 0; s_nacc = 0; }
+        __syncthreads();
+        // frontier: unchecked same-spin cells j with q = j + c - b for a new cell q, mask[b] != 0
+        for (int t = lstart + threadIdx.x; t < lend; t += blockDim.x) {
+            const int q = S.list[t];
+            const int qy = q / nx, qx = q % nx;
+            for (int a = 0; a < L.nn_h; ++a)
+                for (int b = 0; b < L.nn_w; ++b) {
+                    if (!L.nn[a * L.nn_w + b]) continue;
+                    int jy = qy - ch + a, jx = qx - cw + b;
+                    if (L.pbc) { jy = hs_wrap(jy, ny); jx = hs_wrap(jx, nx); }
+                    else if (jy < 0 || jy >= ny || jx < 0 || jx >= nx) continue;
+                    const int j = jy * nx + jx;
+                    if (L.m[j] != ms) continue;
+                    if (atomicExch(&S.chk_ep[j], epoch) == epoch) continue;
+                    S.cand[atomicAdd(&s_ncand, 1)] = j;
+                }
+        }
+        __syncthreads();
+        const int ncand = s_ncand;
+        if (ncand == 0) break;  // empty frontier: the reference's while-loop ends, no draw
+        for (int t = threadIdx.x; t < ncand; t += blockDim.x) {
+            const int j = S.cand[t];
+            const int jy = j / nx, jx = j % nx;
+            int count = 0;
+            for (int a = 0; a < L.nn_h; ++a)
+                for (int b = 0; b < L.nn_w; ++b) {
+                    const int w = L.nn[a * L.nn_w + b];
+                    if (!w) continue;
+                    int yy = jy + ch - a, xx = jx + cw - b;
+                    if (L.pbc) { yy = hs_wrap(yy, ny); xx = hs_wrap(xx, nx); }
+                    else if (yy < 0 || yy >= ny || xx < 0 || xx >= nx) continue;
+                    const int k = yy * nx + xx;
+                    if (S.cl_ep[k] == epoch && S.cl_layer[k] < layer) count += w;
+                }
+            // bond = 1 - exp(-2 J / kBT * count), kBT = 1/beta (hotspice/core.py:599)
+            double bond;
+            if (L.wolff_bond && count <= 24) {
+                bond = L.wolff_bond[count];
+            } else {
+                const double kBT = 1.0 / hs_beta(L, j);
+                bond = 1.0 - exp(m2J / kBT * (double)count);
+            }
+            const double u = hs_u53(L.seed, call, (uint32_t)j);
+            if (!(u > bond)) {
+                S.cl_ep[j] = epoch;
+                S.cl_layer[j] = layer;
+                S.list[lend + atomicAdd(&s_nacc, 1)] = j;
+            }
+        }
+        call += 1;
+        __syncthreads();
+        lstart = lend;
+        lend += s_nacc;
+    }
+    if (layer > (int)N + 1 && threadIdx.x == 0) C->status |= HS_ST_WOLFF_OVERFLOW;
+    // flip the cluster; counters as in core.py:714-716
+    for (int t = threadIdx.x; t < lend; t += blockDim.x) {
+        const int j = S.list[t];
+        L.m[j] = (int8_t)(-L.m[j]);
+        L.mm[j] = -L.mm[j];
+        if (t < sw.cap) { sw.y[t] = j / nx; sw.x[t] = j % nx; if (sw.mode) sw.mode[t] = 0; }
+    }
+    if (threadIdx.x == 0) {
+        C->attempted += lend;
+        C->switches += lend;
+        C->rng_call = call;
+        C->n_sw = min(lend, sw.cap);
+        C->steps += 1;
+        if (lend > sw.cap) C->status |= HS_ST_SWITCH_OVERFLOW;
+    }
+}
+
+// ---- Néel -------------------------------------------------------------------------------
+// Final stage of a Néel step once the global argmin `w` of the log-domain keys is known:
+// switching time in FP64, flip, counters and the one-entry switch list
+// (hotspice/core.py:699-709). Executed by a single thread.
+HS_DEV void neel_finalize(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, HsKeyIdx w, uint64_t call,
+                          double bmin, bool unif, bool two, double attempt_freq) {
+    C->rng_call = call + 1;
+    C->attempted += 1;
+    C->steps += 1;
+    const double t_eff = C->progress ? (C->t_max - (C->t - C->t0)) : C->t_max;
+    if (w.idx < 0) {  // no occupied cell: nanargmin would raise; record and stop
+        C->status |= HS_ST_SELECT_RETRY;
+        C->n_sw = 0;
+        C->t += t_eff;
+        return;
+    }
+    const int64_t i = w.idx;
+    const int y = (int)(i / L.nx), x = (int)(i % L.nx);
+    double b1, b2;
+    hs_barriers(L, y, x, b1, b2);
+    const double beta = hs_beta(L, i);
+    const double e1 = hs_exp1_f64(hs_u53(L.seed, call, (uint32_t)i));
+    double time;
+    if (!two) {
+        // time = E1 * exp((b - bmin) beta) * exp(bmin beta) / nu   (hotspice/core.py:698-700)
+        time = unif ? e1 * exp(b1 * beta) / attempt_freq
+                    : e1 * exp((b1 - bmin) * beta) * exp(bmin * beta) / attempt_freq;
+    } else {
+        const double bm = fmin(b1, b2), dd = fabs(b1 - b2);
+        // tau = E1 / (exp(-(b1-bmin) beta) + exp(-(b2-bmin) beta)); nu halves (core.py:691-693)
+        const double scale = exp((bm - bmin) * beta) / (1.0 + exp(-dd * beta));
+        time = e1 * scale * exp(bmin * beta) / (attempt_freq / 2.0);
+    }
+    C->last_time = time;
+    if (time > t_eff || isnan(time)) {
+        C->t += t_eff;
+        C->n_sw = 0;
+        return;
+    }
+    L.m[i] = (int8_t)(-L.m[i]);
+    L.mm[i] = -L.mm[i];
+    C->switches += 1;
+    C->t += time;
+    sw.y[0] = y;
+    sw.x[0] = x;
+    if (sw.mode) sw.mode[0] = 0;
+    C->n_sw = 1;
+}
+
+// Scratch layout of the Metropolis step (shared by the host launcher and the engine).
+HS_HD inline int64_t hs_align_up_d(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
+HS_HD inline void hs_metro_sizes(const HsLattice &L, const HsGridPlan &P, int &cap, int &gsz) {
+    cap = P.n_sc > 1 ? P.n_sc : 1;
+    gsz = 0;
+    if (P.sample_scheme == HS_SAMPLE_POISSON) {
+        const double r = P.r_cells + 1.0, cs = r / sqrt(2.0);
+        gsz = (int)(ceil(L.nx / cs) * ceil(L.ny / cs));
+        cap = cap > gsz ? cap : gsz;
+    }
+}

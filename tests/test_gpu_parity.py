@@ -159,8 +159,8 @@ def test_progress_graph_equals_plain_launches():
     import hotspice_b200 as hs
     name = 'progress_pin16_metro'
     spec = SPECS[name]
-    a = build_product(name, engine=hs.EngineConfig(use_graphs=True, graph_steps=8))
-    b = build_product(name, engine=hs.EngineConfig(use_graphs=False, graph_steps=8))
+    a = build_product(name, engine=hs.EngineConfig(persistent=False, use_graphs=True, graph_steps=8))
+    b = build_product(name, engine=hs.EngineConfig(persistent=False, use_graphs=False, graph_steps=8))
     ra = a.progress(**spec['progress'])
     rb = b.progress(**spec['progress'])
     assert ra == rb
