@@ -1,23 +1,30 @@
 """Benchmark of the kinetic Monte Carlo hot path on B200.
 
-Workload (one bench step): the in-plane pinwheel lattice of 512 x 512 cells (131,072
-magnets, a = 300 nm, moment 1e-15 A m^2, E_B lognormal with mean 6e-20 J and 5 % sigma,
-T = 300 K), dipolar interaction cut off at 20a plus a 1 mT Zeeman field at 22.5 degrees,
-advanced by 1,000 Metropolis multisample steps with the grid selection at spacing r = 20a,
-FP32 incremental energy updates. Seeded synthetic inputs (no dataset is involved).
+Headline workload ("batched", the configuration the metric's batched-vs-plain comparison is
+quoted on): 256 independent lattice instances, lattice drawn uniformly from {OOP square
+(a = 200 nm, moment 1.1e-15), IP pinwheel (a = 300 nm, moment 1e-15), kagome (a = 500 nm,
+moment 1e-15)}, grid n uniform in [32, 256], T uniform in [200, 400] K, Zeeman 0-5 mT at a
+random angle, E_B lognormal (mean 5.5e-20 J, 5 % sigma), dipolar cutoff 16a, Néel-Arrhenius
+for even and Metropolis (grid selection, default r = calc_r(0.05)) for odd instances, FP32
+energies. Seeded synthetic inputs; no dataset is involved. One bench step advances every
+instance by 200 update steps in one persistent engine launch (the full workload is 20,000
+steps each, i.e. 100 bench steps).
 
-  value : switch-attempts/s with the state resident in HBM (steps replayed from captured
-          CUDA graphs, no host synchronisation inside a bench step), L2 flushed between
-          bench steps.
-  e2e   : the same metric through the public API (Magnets.progress) with the start state
-          copied in from pinned host memory and the final spins and counters copied out,
-          every bench step.
+  value : switch-attempts/s of the whole batch, state resident in HBM, L2 flushed (256 MB
+          write) between bench steps.
+  e2e   : the same through the public API (BatchEngine.run) with every instance's start state
+          copied in from pinned host memory and the spins and counters copied out per step.
+  plain : the plain single-instance GPU form (Magnets.update() once per step, one instance
+          at a time) on a sample of the same instances.
+  single_instance: the 512 x 512 pinwheel lattice (131,072 magnets, cutoff 20a + 1 mT Zeeman,
+          Metropolis grid r = 20a, 1000 steps per bench step) with the best single-instance
+          path (autotuned).
 
-Multi-GPU: one independent lattice per rank (the work shards into independent instances,
-no data-path collective); value = all ranks' attempts / max-over-ranks device time.
+Multi-GPU: one independent batch per rank (independent instances, no data-path collective);
+value = all ranks' attempts / max-over-ranks device time.
 
 `--impl reference` times the reference algorithm's NumPy restatement (the oracle) on the host
-cores on a bounded sample of the same workload.
+on a bounded sample of the same instances.
 """
 from __future__ import annotations
 
@@ -37,42 +44,78 @@ sys.path.insert(0, ROOT)
 
 METRIC = "switch-attempts/sec/GPU batched-served vs plain at 1e-6 rel-E err; p50/p99 latency"
 UNIT = "switch-attempts/s"
-A = 300e-9
-N = 512
-STEPS_PER_BENCH_STEP = 1000
 SEED = 20261203
-WORKLOAD = ("IP_Pinwheel 512x512 (131072 magnets), a=300nm, moment=1e-15, E_B lognormal(6e-20, 5%), T=300K, "
-            "dipolar cutoff 20a + Zeeman 1mT@22.5deg, Metropolis grid r=20a, 1000 multisample steps per bench step, FP32")
+N_INST = 256
+STEPS_PER_BENCH_STEP = 200
+LATTICES = (('OOP_Square', 200e-9, 1.1e-15), ('IP_Pinwheel', 300e-9, 1e-15), ('IP_Kagome', 500e-9, 1e-15))
+WORKLOAD = ("batched: 256 instances, lattice uniform in {OOP_Square a=200nm, IP_Pinwheel a=300nm, IP_Kagome a=500nm}, "
+            "n uniform in [32,256], T uniform in [200,400]K, Zeeman 0-5mT random angle, E_B lognormal(5.5e-20, 5%), "
+            "dipolar cutoff 16a, Neel (even) / Metropolis grid (odd), 200 steps per instance per bench step, FP32")
 
 
-def workload_inputs(seed=SEED):
+def instance_specs(n_inst=N_INST, seed=SEED):
     g = np.random.Generator(np.random.PCG64(seed))
-    m0 = g.integers(0, 2, size=(N, N)) * 2 - 1
-    EB = 6e-20 * g.lognormal(-0.05 ** 2 / 2, 0.05, size=(N, N))
+    specs = []
+    for i in range(n_inst):
+        kind = int(g.integers(0, 3))
+        n = int(g.integers(32, 257))
+        specs.append(dict(i=i, lattice=LATTICES[kind][0], a=LATTICES[kind][1], moment=LATTICES[kind][2], n=n,
+                          T=float(g.uniform(200, 400)), B=float(g.uniform(0, 5e-3)), angle=float(g.uniform(0, 2 * math.pi)),
+                          scheme='Neel' if i % 2 == 0 else 'Metropolis', seed=seed * 1000 + i))
+    return specs
+
+
+def _geometry_shape(spec):
+    n = spec['n']
+    if spec['lattice'] == 'IP_Kagome':
+        return int(n / math.sqrt(3)) // 4 * 4 - 1, n
+    return n, n
+
+
+def instance_inputs(spec):
+    ny, nx = _geometry_shape(spec)
+    g = np.random.Generator(np.random.PCG64(spec['seed']))
+    m0 = g.integers(0, 2, size=(ny, nx)) * 2 - 1
+    EB = 5.5e-20 * g.lognormal(-0.05 ** 2 / 2, 0.05, size=(ny, nx))
     return m0, EB
 
 
-def build_product(device, seed=SEED):
+def build_instance(spec, device):
     import hotspice_b200 as hs
-    m0, EB = workload_inputs(seed)
-    mm = hs.ASI.IP_Pinwheel(A, N, T=300.0, E_B=EB, moment=1e-15, pattern=m0,
-                            energies=[hs.DipolarEnergy(cutoff_range=20 * A),
-                                      hs.ZeemanEnergy(1e-3, math.radians(22.5))],
-                            params=hs.SimParams(UPDATE_SCHEME='Metropolis', MULTISAMPLING_SCHEME='grid'),
-                            seed=seed, device=device,
-                            engine=hs.EngineConfig(graph_steps=100))
-    return mm
+    m0, EB = instance_inputs(spec)
+    cls = getattr(hs.ASI, spec['lattice'])
+    return cls(spec['a'], spec['n'], T=spec['T'], E_B=EB, moment=spec['moment'], pattern=m0,
+               energies=[hs.DipolarEnergy(cutoff_range=16 * spec['a']), hs.ZeemanEnergy(spec['B'], spec['angle'])],
+               params=hs.SimParams(UPDATE_SCHEME=spec['scheme']), seed=spec['seed'], device=device)
 
 
-def build_oracle(seed=SEED):
-    from oracle.geometry import ip_pinwheel
+def build_oracle_instance(spec):
+    from oracle import geometry as G
     from oracle.hotspice_oracle import OracleDipolar, OracleMagnets, OracleZeeman
-    m0, EB = workload_inputs(seed)
-    return OracleMagnets(ip_pinwheel(A, N), m0, T=300.0, E_B=EB, moment=1e-15,
-                         energies=[OracleDipolar(cutoff_range=20 * A), OracleZeeman(1e-3, math.radians(22.5))],
-                         params=dict(UPDATE_SCHEME='Metropolis'), seed=seed)
+    m0, EB = instance_inputs(spec)
+    geo = {'OOP_Square': G.oop_square, 'IP_Pinwheel': G.ip_pinwheel, 'IP_Kagome': G.ip_kagome}[spec['lattice']]
+    return OracleMagnets(geo(spec['a'], spec['n']), m0, T=spec['T'], E_B=EB, moment=spec['moment'],
+                         energies=[OracleDipolar(cutoff_range=16 * spec['a']), OracleZeeman(spec['B'], spec['angle'])],
+                         params=dict(UPDATE_SCHEME=spec['scheme']), seed=spec['seed'])
 
 
+# ---------------------------------------------------------------------------- single instance
+A1, N1 = 300e-9, 512
+WORKLOAD1 = ("IP_Pinwheel 512x512 (131072 magnets), a=300nm, moment=1e-15, E_B lognormal(6e-20, 5%), T=300K, "
+             "dipolar cutoff 20a + Zeeman 1mT@22.5deg, Metropolis grid r=20a, 1000 steps per bench step")
+
+
+def build_single(device, seed=SEED):
+    import hotspice_b200 as hs
+    g = np.random.Generator(np.random.PCG64(seed))
+    m0 = g.integers(0, 2, size=(N1, N1)) * 2 - 1
+    EB = 6e-20 * g.lognormal(-0.05 ** 2 / 2, 0.05, size=(N1, N1))
+    return hs.ASI.IP_Pinwheel(A1, N1, T=300.0, E_B=EB, moment=1e-15, pattern=m0,
+                              energies=[hs.DipolarEnergy(cutoff_range=20 * A1), hs.ZeemanEnergy(1e-3, math.radians(22.5))],
+                              params=hs.SimParams(UPDATE_SCHEME='Metropolis'), seed=seed, device=device)
+
+
+# ---------------------------------------------------------------------------- plumbing
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
     Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,'
@@ -122,10 +165,9 @@ class ClockSampler:
 def dist_setup():
     ws = int(os.environ.get('WORLD_SIZE', '1'))
     if ws > 1:
-        import torch.distributed as dist
         import datetime
-        backend = 'nccl'
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        import torch.distributed as dist
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
         return dist, dist.get_rank(), ws, int(os.environ.get('LOCAL_RANK', '0'))
     return None, 0, 1, 0
 
@@ -140,8 +182,8 @@ def measured_peaks():
 
 
 def profile_traffic():
-    """Per-launch DRAM traffic of the update kernel from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, 'profiles', 'engine_kernel_pinwheel512.txt')
+    """Per-launch DRAM traffic of the engine kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, 'profiles', 'engine_kernel_batched256.txt')
     try:
         for line in open(path):
             if line.startswith('traffic_bytes_per_launch:'):
@@ -151,135 +193,171 @@ def profile_traffic():
     return None
 
 
-def cpu_baseline_sample(steps=60):
-    """The oracle (NumPy restatement of the reference) on a bounded sample of the workload."""
-    mo = build_oracle()
-    r = 20 * A
-    for _ in range(3):
-        mo.update(r=r)
-    a0 = mo.attempted_switches
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        mo.update(r=r)
-    dt = time.perf_counter() - t0
-    return (mo.attempted_switches - a0) / dt, dt, steps
+def algorithmic_bytes(mm, dattempts, dswitches, steps):
+    """Bytes a step must move, from the run's own counters: a Néel step reads every occupied
+    cell's FP64 energy, spin, Zeeman factor and E_B (17 B; +12 B of E_perp and its Zeeman
+    factor in-plane); a Metropolis step reads those for its candidates; every switch
+    read-modify-writes the FP64 energy and reads the FP32 kernel and source field over its
+    window (24 B per window cell; +20 B for E_perp and its kernel in-plane)."""
+    d = mm._dipolar()
+    W = (2 * d.kernel_set.wx + 1) * (2 * d.kernel_set.wy + 1)
+    per_cell = 17 + (12 if mm.USE_PERP_ENERGY else 0)
+    upd = W * (24 + (20 if mm.USE_PERP_ENERGY else 0))
+    if mm.params.UPDATE_SCHEME.name == 'NEEL':
+        return steps * mm.n * per_cell + dswitches * upd
+    return dattempts * per_cell + dswitches * upd
+
+
+# ---------------------------------------------------------------------------- reference arm
+def oracle_sample(specs, seconds_per_instance=2.5, max_steps=400):
+    """Time the NumPy oracle on a few instances of the batch (two per scheme)."""
+    picks = [s for s in specs if s['scheme'] == 'Neel'][:2] + [s for s in specs if s['scheme'] == 'Metropolis'][:2]
+    att, secs, steps_done = 0, 0.0, 0
+    for spec in picks:
+        mo = build_oracle_instance(spec)
+        mo.update()
+        a0, t0, k = mo.attempted_switches, time.perf_counter(), 0
+        while k < max_steps and time.perf_counter() - t0 < seconds_per_instance:
+            mo.update()
+            k += 1
+        secs += time.perf_counter() - t0
+        att += mo.attempted_switches - a0
+        steps_done += k
+    return att / secs, secs, steps_done, len(picks)
 
 
 def run_reference(args):
     rank, ws = int(os.environ.get('RANK', '0')), int(os.environ.get('WORLD_SIZE', '1'))
     if rank != 0:
         return
-    mo = build_oracle()
-    r = 20 * A
-    sample = args.ref_sample
+    specs = instance_specs()
     for _ in range(args.warmup):
-        for _ in range(sample):
-            mo.update(r=r)
-    att, secs = 0, 0.0
+        oracle_sample(specs, seconds_per_instance=0.3, max_steps=20)
+    vals, secs_all = [], 0.0
     for _ in range(args.steps):
-        a0 = mo.attempted_switches
-        t0 = time.perf_counter()
-        for _ in range(sample):
-            mo.update(r=r)
-        secs += time.perf_counter() - t0
-        att += mo.attempted_switches - a0
-    v = att / secs
+        v, secs, st, ni = oracle_sample(specs, seconds_per_instance=args.ref_seconds)
+        vals.append(v)
+        secs_all += secs
+    v = float(np.mean(vals))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1e3 * secs_all / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sample_steps_per_bench_step": sample},
+            "config": {"workload": WORKLOAD, "sample": "2 Néel + 2 Metropolis instances of the batch per bench step"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-                             "sample": f"{sample} Metropolis steps per bench step of the 512x512 workload "
-                                       f"(NumPy oracle restating the reference, single process)"},
+                             "sample": f"4 instances of the batch, up to {args.ref_seconds}s each per bench step, NumPy "
+                                       f"oracle restating the reference (single process)"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
+# ---------------------------------------------------------------------------- product arm
 def run_product(args):
     import torch
+    from hotspice_b200.engine import BatchEngine
     dist, rank, ws, local = dist_setup()
     dev = torch.device('cuda', local)
     torch.cuda.set_device(dev)
-    from hotspice_b200.engine import Autotuner
-    mcs = args.mc_steps
-    mm = build_product(dev, seed=SEED + rank)
-    r = 20 * A
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    d = mm.get_energy('dipolar')
-    cs = Autotuner().tune(mm, steps=200, r=r) if not args.cluster_size else args.cluster_size
-    mm.engine.cluster_size = cs
-
-    # pinned host copies of the start state for the end-to-end leg
-    snap = {k: v.detach().clone() for k, v in (('m', mm._m_dev), ('mm', mm._mm_dev), ('E', d._E), ('Ep', d._Ep),
-                                               ('C', mm._counters))}
-    host_in = {k: v.cpu().pin_memory() for k, v in snap.items()}
-    host_out_m = torch.empty_like(mm._m_dev, device='cpu').pin_memory()
-    host_out_c = torch.empty_like(mm._counters, device='cpu').pin_memory()
-    h2d = sum(v.numel() * v.element_size() for v in host_in.values())
-    d2h = host_out_m.numel() + host_out_c.numel()
+    specs = instance_specs(args.instances, seed=SEED + 7919 * rank)
+    t_setup = time.perf_counter()
+    mms = [build_instance(s, dev) for s in specs]
+    setup_s = time.perf_counter() - t_setup
+    eng = BatchEngine(mms)
+    S = args.mc_steps
 
     # ---- device-resident throughput: one persistent launch per bench step ----------------
     for _ in range(args.warmup):
-        mm.run(mcs, r=r)
+        eng.run(S)
     torch.cuda.synchronize(dev)
-    c0 = mm._read_counters()
+    c0 = [mm._read_counters() for mm in mms]
     if dist:
         dist.barrier()
-    torch.cuda.synchronize(dev)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     sampler = ClockSampler(local)
     with sampler:
         for k in range(args.steps):
             flush.fill_(float(k))
             ev[k][0].record(stream)
-            mm.run(mcs, r=r)
+            eng.run(S)
             ev[k][1].record(stream)
         torch.cuda.synchronize(dev)
     if dist:
         dist.barrier()
     dev_ms = sum(a.elapsed_time(b) for a, b in ev)
-    c1 = mm._read_counters()
-    attempts = int(c1['attempted'] - c0['attempted'])
-    switches = int(c1['switches'] - c0['switches'])
-    status = int(c1['status'])
-
-    # ---- roofline of the fused engine kernel (the only kernel of a bench step) ------------
-    ks = d.kernel_set
-    W = (2 * ks.wx + 1) * (2 * ks.wy + 1)
-    # per switch: E f32 read+write, kernel, source m*mu (16 B) and E_perp read+write, perp kernel
-    # (12 B) for every window cell; per candidate: E, E_perp, Zeeman factor, beta-free E_B, spin
-    alg_bytes = (switches * W * 28 + attempts * 17) / args.steps
+    c1 = [mm._read_counters() for mm in mms]
+    attempts = sum(int(b['attempted'] - a['attempted']) for a, b in zip(c0, c1))
+    switches = sum(int(b['switches'] - a['switches']) for a, b in zip(c0, c1))
+    status = [int(b['status']) for b in c1]
+    alg = sum(algorithmic_bytes(mm, int(b['attempted'] - a['attempted']), int(b['switches'] - a['switches']),
+                                S * args.steps) for mm, a, b in zip(mms, c0, c1)) / args.steps
     launch_ms = dev_ms / args.steps
     hbm, peak_kind = measured_peaks()
-    achieved = alg_bytes / (launch_ms * 1e-3) / 1e9
+    achieved = alg / (launch_ms * 1e-3) / 1e9
+    cluster_sizes = sorted({p.cs for p in eng._prepare([1] * len(mms), [{}] * len(mms))})
 
-    # ---- end to end through the public API ------------------------------------------------
-    mc_per_step = attempts / max(args.steps, 1) / mm.n
-    for _ in range(max(1, args.warmup // 2)):
-        mm.progress(t_max=math.inf, MCsteps_max=mc_per_step, r=r)
+    # ---- energy error of the batch against an FP64 recompute ------------------------------
+    # Only instances whose kernel is symmetric: with a pair of magnets exactly at the cutoff
+    # radius the reference's kernel keeps the pair one way and drops it the other (distances
+    # are cumulative sums), so its incremental energies drift from any full recompute by
+    # construction (the FP64 reference algorithm drifts identically).
+    errs = []
+    sym = [mm for mm in mms if mm._dipolar().kernel_set.asymmetry < 1e-12]
+    n_asym = len(mms) - len(sym)
+    for mm in sym[:: max(1, len(sym) // 16)]:
+        d = mm._dipolar()
+        E32 = d._E.double().clone()
+        d.update(method='direct64')
+        E64 = d._E.double()
+        errs.append(float((E32 - E64).abs().max() / E64.abs().max()))
+        d._E.copy_(E32)
+
+    # ---- end to end through the public API (start states in, spins + counters out) ---------
+    snaps = [mm._snapshot() for mm in mms]
+    host_in = [{k: (v.cpu().pin_memory() if v is not None else None) for k, v in s.items()} for s in snaps]
+    host_out = [(torch.empty_like(mm._m_dev, device='cpu').pin_memory(),
+                 torch.empty_like(mm._counters, device='cpu').pin_memory()) for mm in mms]
+    h2d = sum(sum(v.numel() * v.element_size() for v in h.values() if v is not None) for h in host_in)
+    d2h = sum(a.numel() + b.numel() for a, b in host_out)
+    cdt = _counters_dtype()
+    att_in = [int(np.frombuffer(h['C'].numpy().tobytes(), dtype=cdt)[0]['attempted']) for h in host_in]
     torch.cuda.synchronize(dev)
-    if dist:
-        dist.barrier()
-    e2e_att = 0
-    t_e2e = time.perf_counter()
     ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_att = 0
     ee0.record(stream)
     for k in range(args.steps):
-        mm._m_dev.copy_(host_in['m'], non_blocking=True)
-        mm._mm_dev.copy_(host_in['mm'], non_blocking=True)
-        d._E.copy_(host_in['E'], non_blocking=True)
-        d._Ep.copy_(host_in['Ep'], non_blocking=True)
-        mm._counters.copy_(host_in['C'], non_blocking=True)
-        mm._ctl = None
-        dt_, dmc = mm.progress(t_max=math.inf, MCsteps_max=mc_per_step, r=r)
-        e2e_att += int(round(dmc * mm.n))
-        host_out_m.copy_(mm._m_dev, non_blocking=True)
-        host_out_c.copy_(mm._counters, non_blocking=True)
+        for mm, h in zip(mms, host_in):
+            d = mm._dipolar()
+            mm._m_dev.copy_(h['m'], non_blocking=True)
+            mm._mm_dev.copy_(h['mm'], non_blocking=True)
+            mm._counters.copy_(h['C'], non_blocking=True)
+            d._E.copy_(h['E'], non_blocking=True)
+            if h['Ep'] is not None:
+                d._Ep.copy_(h['Ep'], non_blocking=True)
+            mm._ctl = None
+        eng.run(S)
+        for mm, (hm, hc) in zip(mms, host_out):
+            hm.copy_(mm._m_dev, non_blocking=True)
+            hc.copy_(mm._counters, non_blocking=True)
+        torch.cuda.synchronize(dev)
+        e2e_att += sum(int(np.frombuffer(hc.numpy().tobytes(), dtype=cdt)[0]['attempted']) - a
+                       for (hm, hc), a in zip(host_out, att_in))
     ee1.record(stream)
     torch.cuda.synchronize(dev)
     e2e_ms = ee0.elapsed_time(ee1)
-    wall_e2e = time.perf_counter() - t_e2e
+
+    # ---- plain single-instance GPU form on a sample of the same instances ----------------
+    plain_att, plain_s, plain_n = 0, 0.0, 0
+    for mm in mms[:: max(1, len(mms) // args.plain_sample)]:
+        a0 = mm.attempted_switches
+        t0 = time.perf_counter()
+        for _ in range(args.plain_steps):
+            mm.update()
+        torch.cuda.synchronize(dev)
+        plain_s += time.perf_counter() - t0
+        plain_att += mm.attempted_switches - a0
+        plain_n += 1
+    plain_value = plain_att / plain_s
 
     # ---- reductions over ranks -------------------------------------------------------------
     vals = torch.tensor([dev_ms, e2e_ms, float(attempts), float(e2e_att)], dtype=torch.float64, device=dev)
@@ -288,42 +366,77 @@ def run_product(args):
         sm = vals.clone(); dist.all_reduce(sm, op=dist.ReduceOp.SUM)
         dev_ms, e2e_ms = float(mx[0]), float(mx[1])
         attempts, e2e_att = int(sm[2]), int(sm[3])
+    single = None
+    if rank == 0 and not args.no_single:
+        single = run_single(dev, stream)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
     value = attempts / (dev_ms * 1e-3)
-    e2e_value = e2e_att / (e2e_ms * 1e-3)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (seeded lattice, random start, lognormal E_B)",
-        "config": {"workload": WORKLOAD, "lattice": "IP_Pinwheel", "nx": N, "ny": N, "magnets": mm.n,
-                   "steps_per_bench_step": mcs, "l2": "flushed (256 MB write) between bench steps",
-                   "parallelism": f"{ws} independent replicas" if ws > 1 else "single instance",
-                   "cluster_size": cs, "switches": switches, "attempts": attempts, "device_status": status},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "api": "Magnets.progress(t_max=inf, MCsteps_max=per-step share) with state restored from pinned host",
-                "wall_s": wall_e2e},
-        "gpu_launches": launches_for(args.steps),
-        "roofline": {"bound": "hbm", "kernel": f"engine_kernel<{cs}>", "achieved": achieved, "peak": hbm,
-                     "unit": "GB/s", "frac": achieved / hbm, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                     "traffic": profile_traffic(), "launch_ms": launch_ms,
-                     "algorithmic_bytes_per_launch": alg_bytes, "window_cells": W},
+        "dtype": "f32", "data": "synthetic (seeded lattices, random starts, lognormal E_B)",
+        "config": {"workload": WORKLOAD, "instances": len(mms), "steps_per_instance_per_bench_step": S,
+                   "l2": "flushed (256 MB write) between bench steps",
+                   "parallelism": f"{ws} independent batches (one per GPU)" if ws > 1 else "one batch, one GPU",
+                   "cluster_sizes": cluster_sizes, "switches": switches, "attempts": attempts,
+                   "device_status_nonzero": sum(1 for s in status if s),
+                   "max_rel_energy_error_vs_fp64": max(errs),
+                   "energy_error_note": f"FP32 incremental vs FP64 full recompute over {len(errs)} instances with "
+                                        f"symmetric kernels; {n_asym} of {len(mms)} instances have a cutoff-boundary "
+                                        f"asymmetric kernel whose incremental energies drift from a full recompute in "
+                                        f"the reference algorithm itself",
+                   "setup_s": setup_s},
+        "e2e": {"value": e2e_att / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "api": "BatchEngine.run with every start state from pinned host"},
+        "plain": {"value": plain_value, "unit": UNIT, "instances": plain_n, "steps_each": args.plain_steps,
+                  "form": "Magnets.update() per step, one instance at a time", "batched_over_plain": value / plain_value},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "kernel": "engine_kernel<1>", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "traffic": profile_traffic(), "launch_ms": launch_ms, "algorithmic_bytes_per_launch": alg},
         "clocks": sampler.summary(),
     }
+    if single is not None:
+        line["single_instance"] = single
     if not args.no_cpu_baseline:
-        v, secs, st = cpu_baseline_sample(args.cpu_steps)
+        v, secs, st, ni = oracle_sample(specs, seconds_per_instance=args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-                                "sample": f"{st} Metropolis steps of the same 512x512 workload ({secs:.1f} s) with the "
-                                          f"NumPy oracle restating the reference"}
+                                "sample": f"{ni} instances of the batch ({st} steps, {secs:.1f} s) with the NumPy oracle "
+                                          f"restating the reference"}
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
 
 
-def launches_for(steps):
-    return steps  # one persistent engine launch per bench step
+def _counters_dtype():
+    from hotspice_b200 import _lib
+    return _lib.COUNTERS_DTYPE
+
+
+def run_single(dev, stream):
+    """The 512 x 512 pinwheel instance, best single-instance path chosen by measurement."""
+    import torch
+    from hotspice_b200.engine import Autotuner
+    mm = build_single(dev)
+    r = 20 * A1
+    choice = Autotuner().tune(mm, steps=200, r=r, include_step_kernels=True)
+    for _ in range(2):
+        mm.run(1000, r=r)
+    torch.cuda.synchronize(dev)
+    a0 = mm.attempted_switches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(3):
+        mm.run(1000, r=r)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    att = mm.attempted_switches - a0
+    return {"workload": WORKLOAD1, "value": att / (ms * 1e-3), "unit": UNIT, "us_per_mc_step": ms * 1e3 / 3000,
+            "path": "per-step kernels (CUDA graphs)" if choice == 0 else f"engine cluster {choice}"}
 
 
 def main():
@@ -332,12 +445,14 @@ def main():
     ap.add_argument('--steps', type=int, default=10)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='product', choices=['product', 'reference'])
-    ap.add_argument('--ref-sample', type=int, default=40)
-    ap.add_argument('--cpu-steps', type=int, default=400)
+    ap.add_argument('--instances', type=int, default=N_INST)
+    ap.add_argument('--mc-steps', type=int, default=STEPS_PER_BENCH_STEP, help='update steps per instance per bench step')
+    ap.add_argument('--plain-sample', type=int, default=8)
+    ap.add_argument('--plain-steps', type=int, default=100)
+    ap.add_argument('--ref-seconds', type=float, default=2.5)
+    ap.add_argument('--cpu-seconds', type=float, default=2.5)
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--mc-steps', type=int, default=STEPS_PER_BENCH_STEP,
-                    help='Metropolis steps per bench step (the workload uses 1000)')
-    ap.add_argument('--cluster-size', type=int, default=0, help='CTAs per cluster (0: autotune)')
+    ap.add_argument('--no-single', action='store_true')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)

@@ -720,13 +720,9 @@ class Magnets(ABC):
         if method == 'auto':
             method = 'direct64' if N * W <= self.engine.direct_max_pairs else 'igemm'
         if method == 'direct64':
-            E64 = torch.empty((self.ny, self.nx), device=self.device, dtype=torch.float64)
-            Ep64 = torch.empty_like(E64) if self.USE_PERP_ENERGY else None
-            _lib.check(self._lib.hs_dipolar_full_direct(L, 1, E64.data_ptr(), _ptr(Ep64), self._stream()),
-                       'hs_dipolar_full_direct')
-            d._E.copy_(E64)
-            if Ep64 is not None:
-                d._Ep.copy_(Ep64)
+            _lib.check(self._lib.hs_dipolar_full_direct(L, 1, d._E.data_ptr(),
+                                                        _ptr(d._Ep) if self.USE_PERP_ENERGY else None,
+                                                        self._stream()), 'hs_dipolar_full_direct')
         elif method == 'direct32':
             _lib.check(self._lib.hs_dipolar_full_direct(L, 0, None, None, self._stream()), 'hs_dipolar_full_direct')
         elif method == 'igemm':

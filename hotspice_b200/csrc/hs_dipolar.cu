@@ -102,33 +102,37 @@ dip_update_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev, int n_h
         if (!any) return;
         const float4 mm4 = *reinterpret_cast<const float4 *>(L.mm + row + x0);
         const float mmv[4] = {mm4.x, mm4.y, mm4.z, mm4.w};
-        float4 e4 = *reinterpret_cast<float4 *>(L.E_dip + row + x0);
-        float ev[4] = {e4.x, e4.y, e4.z, e4.w};
+        const double2 e01 = *reinterpret_cast<const double2 *>(L.E_dip + row + x0);
+        const double2 e23 = *reinterpret_cast<const double2 *>(L.E_dip + row + x0 + 2);
+        double ev[4] = {e01.x, e01.y, e23.x, e23.y};
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
             if (semantics == HS_UPDATE_MULTIPLE) {
                 if (negate[v]) ev[v] = -ev[v];
-                ev[v] += pref2 * (mmv[v] * acc[v]);
+                ev[v] += (double)(pref2 * (mmv[v] * acc[v]));
             } else {
-                ev[v] += pref2 * (mmv[v] * acc[v]);
+                ev[v] += (double)(pref2 * (mmv[v] * acc[v]));
                 if (negate[v]) ev[v] = -ev[v];
             }
         }
-        *reinterpret_cast<float4 *>(L.E_dip + row + x0) = make_float4(ev[0], ev[1], ev[2], ev[3]);
+        *reinterpret_cast<double2 *>(L.E_dip + row + x0) = make_double2(ev[0], ev[1]);
+        *reinterpret_cast<double2 *>(L.E_dip + row + x0 + 2) = make_double2(ev[2], ev[3]);
         if (L.use_perp) {
-            float4 p4 = *reinterpret_cast<float4 *>(L.E_dip_perp + row + x0);
-            float pv[4] = {p4.x, p4.y, p4.z, p4.w};
+            const double2 p01 = *reinterpret_cast<const double2 *>(L.E_dip_perp + row + x0);
+            const double2 p23 = *reinterpret_cast<const double2 *>(L.E_dip_perp + row + x0 + 2);
+            double pv[4] = {p01.x, p01.y, p23.x, p23.y};
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
                 if (semantics == HS_UPDATE_MULTIPLE) {
                     if (negate[v]) pv[v] = -pv[v];
-                    pv[v] += pref2 * (mmv[v] * accp[v]);
+                    pv[v] += (double)(pref2 * (mmv[v] * accp[v]));
                 } else {
-                    pv[v] += pref2 * (mmv[v] * accp[v]);
+                    pv[v] += (double)(pref2 * (mmv[v] * accp[v]));
                     if (negate[v]) pv[v] = -pv[v];
                 }
             }
-            *reinterpret_cast<float4 *>(L.E_dip_perp + row + x0) = make_float4(pv[0], pv[1], pv[2], pv[3]);
+            *reinterpret_cast<double2 *>(L.E_dip_perp + row + x0) = make_double2(pv[0], pv[1]);
+            *reinterpret_cast<double2 *>(L.E_dip_perp + row + x0 + 2) = make_double2(pv[2], pv[3]);
         }
         return;
     }
@@ -137,14 +141,14 @@ dip_update_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev, int n_h
         const int x = x0 + v;
         if (x >= L.nx || !touched[v]) continue;
         const float mmv = L.mm[row + x];
-        float e = L.E_dip[row + x];
-        if (semantics == HS_UPDATE_MULTIPLE) { if (negate[v]) e = -e; e += pref2 * (mmv * acc[v]); }
-        else { e += pref2 * (mmv * acc[v]); if (negate[v]) e = -e; }
+        double e = L.E_dip[row + x];
+        if (semantics == HS_UPDATE_MULTIPLE) { if (negate[v]) e = -e; e += (double)(pref2 * (mmv * acc[v])); }
+        else { e += (double)(pref2 * (mmv * acc[v])); if (negate[v]) e = -e; }
         L.E_dip[row + x] = e;
         if (L.use_perp) {
-            float p = L.E_dip_perp[row + x];
-            if (semantics == HS_UPDATE_MULTIPLE) { if (negate[v]) p = -p; p += pref2 * (mmv * accp[v]); }
-            else { p += pref2 * (mmv * accp[v]); if (negate[v]) p = -p; }
+            double p = L.E_dip_perp[row + x];
+            if (semantics == HS_UPDATE_MULTIPLE) { if (negate[v]) p = -p; p += (double)(pref2 * (mmv * accp[v])); }
+            else { p += (double)(pref2 * (mmv * accp[v])); if (negate[v]) p = -p; }
             L.E_dip_perp[row + x] = p;
         }
     }
@@ -193,13 +197,9 @@ __global__ void dip_full_direct_kernel(HsLattice L, int fp64, double *E64, doubl
             }
         }
         const Acc scale = (Acc)L.dip_pref * (Acc)L.moment[i] * (Acc)mi;
-        if (fp64) {
-            E64[i] = (double)(scale * acc);
-            if (L.use_perp && Ep64) Ep64[i] = (double)(scale * accp);
-        } else {
-            L.E_dip[i] = (float)(scale * acc);
-            if (L.use_perp) L.E_dip_perp[i] = (float)(scale * accp);
-        }
+        double *Eo = E64 ? E64 : L.E_dip, *Epo = Ep64 ? Ep64 : L.E_dip_perp;
+        Eo[i] = (double)(scale * acc);
+        if (L.use_perp && Epo) Epo[i] = (double)(scale * accp);
     }
 }
 
@@ -224,8 +224,8 @@ int hs_launch_dipolar_full_direct(const HsLattice &L, int fp64, double *E64, dou
         if (full) dip_full_direct_kernel<double, true><<<blocks, threads, 0, st>>>(L, 1, E64, Ep64);
         else dip_full_direct_kernel<double, false><<<blocks, threads, 0, st>>>(L, 1, E64, Ep64);
     } else {
-        if (full) dip_full_direct_kernel<float, true><<<blocks, threads, 0, st>>>(L, 0, nullptr, nullptr);
-        else dip_full_direct_kernel<float, false><<<blocks, threads, 0, st>>>(L, 0, nullptr, nullptr);
+        if (full) dip_full_direct_kernel<float, true><<<blocks, threads, 0, st>>>(L, 0, E64, Ep64);
+        else dip_full_direct_kernel<float, false><<<blocks, threads, 0, st>>>(L, 0, E64, Ep64);
     }
     return hs_check_launch("dip_full_direct_kernel");
 }

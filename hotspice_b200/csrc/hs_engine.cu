@@ -194,40 +194,47 @@ HS_DEV void update_items(const HsLattice &L, const SwX *s_sw, const int *s_pre, 
                     }
                     if (x0 >= L.nx) continue;
                     const int64_t i = (int64_t)row * L.nx + x0;
-                    float mv[4], ev[4], pv[4];
+                    float mv[4];
+                    double ev[4], pv[4];
                     if (vec) {
                         const float4 a = __ldcg(reinterpret_cast<const float4 *>(L.mm + i));
-                        const float4 e = __ldcg(reinterpret_cast<const float4 *>(L.E_dip + i));
+                        const double2 e0 = __ldcg(reinterpret_cast<const double2 *>(L.E_dip + i));
+                        const double2 e1 = __ldcg(reinterpret_cast<const double2 *>(L.E_dip + i + 2));
                         mv[0] = a.x; mv[1] = a.y; mv[2] = a.z; mv[3] = a.w;
-                        ev[0] = e.x; ev[1] = e.y; ev[2] = e.z; ev[3] = e.w;
+                        ev[0] = e0.x; ev[1] = e0.y; ev[2] = e1.x; ev[3] = e1.y;
                         if (L.use_perp) {
-                            const float4 p = __ldcg(reinterpret_cast<const float4 *>(L.E_dip_perp + i));
-                            pv[0] = p.x; pv[1] = p.y; pv[2] = p.z; pv[3] = p.w;
+                            const double2 p0 = __ldcg(reinterpret_cast<const double2 *>(L.E_dip_perp + i));
+                            const double2 p1 = __ldcg(reinterpret_cast<const double2 *>(L.E_dip_perp + i + 2));
+                            pv[0] = p0.x; pv[1] = p0.y; pv[2] = p1.x; pv[3] = p1.y;
                         }
                     } else {
 #pragma unroll
                         for (int v = 0; v < 4; ++v) {
                             const bool in = x0 + v < L.nx;
                             mv[v] = in ? __ldcg(L.mm + i + v) : 0.f;
-                            ev[v] = in ? __ldcg(L.E_dip + i + v) : 0.f;
-                            pv[v] = (in && L.use_perp) ? __ldcg(L.E_dip_perp + i + v) : 0.f;
+                            ev[v] = in ? __ldcg(L.E_dip + i + v) : 0.0;
+                            pv[v] = (in && L.use_perp) ? __ldcg(L.E_dip_perp + i + v) : 0.0;
                         }
                     }
 #pragma unroll
                     for (int v = 0; v < 4; ++v) {
                         if (semantics == HS_UPDATE_MULTIPLE) {
                             if (neg[v]) { ev[v] = -ev[v]; pv[v] = -pv[v]; }
-                            ev[v] += pref2 * (mv[v] * acc[v]);
-                            pv[v] += pref2 * (mv[v] * accp[v]);
+                            ev[v] += (double)(pref2 * (mv[v] * acc[v]));
+                            pv[v] += (double)(pref2 * (mv[v] * accp[v]));
                         } else {
-                            ev[v] += pref2 * (mv[v] * acc[v]);
-                            pv[v] += pref2 * (mv[v] * accp[v]);
+                            ev[v] += (double)(pref2 * (mv[v] * acc[v]));
+                            pv[v] += (double)(pref2 * (mv[v] * accp[v]));
                             if (neg[v]) { ev[v] = -ev[v]; pv[v] = -pv[v]; }
                         }
                     }
                     if (vec) {
-                        *reinterpret_cast<float4 *>(L.E_dip + i) = make_float4(ev[0], ev[1], ev[2], ev[3]);
-                        if (L.use_perp) *reinterpret_cast<float4 *>(L.E_dip_perp + i) = make_float4(pv[0], pv[1], pv[2], pv[3]);
+                        *reinterpret_cast<double2 *>(L.E_dip + i) = make_double2(ev[0], ev[1]);
+                        *reinterpret_cast<double2 *>(L.E_dip + i + 2) = make_double2(ev[2], ev[3]);
+                        if (L.use_perp) {
+                            *reinterpret_cast<double2 *>(L.E_dip_perp + i) = make_double2(pv[0], pv[1]);
+                            *reinterpret_cast<double2 *>(L.E_dip_perp + i + 2) = make_double2(pv[2], pv[3]);
+                        }
                     } else {
                         for (int v = 0; v < 4 && x0 + v < L.nx; ++v) {
                             L.E_dip[i + v] = ev[v];
@@ -395,23 +402,8 @@ __global__ void __launch_bounds__(ENG_NT, 1) engine_kernel(const HsInstance *ins
                     bmin = s_dred[0];
                     Sync<CS>::all();
                 }
-                HsKeyIdx best{0.0, -1};
                 const bool two = L.use_perp != 0;
-                for (int64_t i = gt; i < N; i += gs) {
-                    if (!L.occ[i]) continue;
-                    double b1, b2;
-                    hs_barriers(L, (int)(i / L.nx), (int)(i % L.nx), b1, b2);
-                    const double beta = hs_beta(L, i);
-                    const double u = hs_u53(L.seed, call, (uint32_t)i);
-                    const double le1 = (double)hs_log_exp1_f32(u);
-                    double key;
-                    if (!two) key = le1 + (b1 - bmin) * beta;
-                    else {
-                        const double bm = fmin(b1, b2), dd = fabs(b1 - b2);
-                        key = le1 + (bm - bmin) * beta - (double)log1pf(expf((float)(-dd * beta)));
-                    }
-                    best = hs_kmin(best, HsKeyIdx{key, (int)i});
-                }
+                HsKeyIdx best = neel_scan_range(L, gt, gs, N, call, bmin, HsKeyIdx{0.0, -1});
                 best = eng_block_kmin(best, s_red);
                 if (threadIdx.x == 0) {
                     if constexpr (CS == 1) s_part[0] = best;

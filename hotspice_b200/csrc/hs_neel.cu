@@ -98,23 +98,8 @@ neel_scan_kernel(HsLattice L, HsCounters *C, HsSwitchList sw, double attempt_fre
     const int64_t N = (int64_t)L.nx * L.ny;
     const uint64_t call = C->rng_call;
     const double bmin = UNIF ? 0.0 : C->bmin;
-    HsKeyIdx best{0.0, -1};
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
-        if (!L.occ[i]) continue;
-        double b1, b2;
-        hs_barriers(L, (int)(i / L.nx), (int)(i % L.nx), b1, b2);
-        const double beta = hs_beta(L, i);
-        const double u = hs_u53(L.seed, call, (uint32_t)i);
-        const double le1 = (double)hs_log_exp1_f32(u);
-        double key;
-        if (!TWO) {
-            key = le1 + (b1 - bmin) * beta;
-        } else {
-            const double bm = fmin(b1, b2), dd = fabs(b1 - b2);
-            key = le1 + (bm - bmin) * beta - (double)log1pf(expf((float)(-dd * beta)));
-        }
-        best = hs_kmin(best, HsKeyIdx{key, (int)i});
-    }
+    HsKeyIdx best = neel_scan_range(L, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x,
+                                    N, call, bmin, HsKeyIdx{0.0, -1});
     best = block_kmin(best, sm);
     if (threadIdx.x == 0) {
         S->part[blockIdx.x] = best;

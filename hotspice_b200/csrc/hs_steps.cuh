@@ -684,3 +684,78 @@ HS_HD inline void hs_metro_sizes(const HsLattice &L, const HsGridPlan &P, int &c
         cap = cap > gsz ? cap : gsz;
     }
 }
+
+// Barriers of hotspice/core.py:625-656 from an already-loaded total energy E, perpendicular
+// energy Ep (before m_perp_factor) and E_B.
+HS_DEV void hs_barriers_from(const HsLattice &L, double E, double Ep, double EB, double &b1, double &b2) {
+    const double dE = -2.0 * E;
+    const double Ecur = -dE / 2.0;
+    if (!L.use_perp) {
+        double b;
+        if (L.barrier_method == HS_BARRIER_SIMPLE) {
+            b = fmax(dE, EB - Ecur);
+        } else {
+            const double inv4 = 0.25 / EB;
+            const double q = dE * inv4 + 1.0;
+            b = (dE > 4.0 * EB) ? dE : fmin(EB * q * q, dE + 4.0 * EB);
+        }
+        b1 = b2 = b;
+    } else {
+        const double Ept = L.m_perp_factor * Ep;
+        b1 = fmax(dE, (EB + Ept) - Ecur);
+        b2 = fmax(dE, (EB - Ept) - Ecur);
+    }
+}
+
+// Néel log-domain keys (see hs_neel.cu) of cells start, start + stride, ... < N, folded into
+// `best`. The loads of NEEL_UNR cells are issued before any of them is used, so that one
+// thread keeps several L2 round trips in flight; the (key, index) minimum does not depend on
+// the visiting order.
+constexpr int NEEL_UNR = 4;
+HS_DEV HsKeyIdx neel_scan_range(const HsLattice &L, int64_t start, int64_t stride, int64_t N, uint64_t call,
+                                double bmin, HsKeyIdx best) {
+    const bool two = L.use_perp != 0;
+    for (int64_t base = start; base < N; base += stride * NEEL_UNR) {
+        int8_t oc[NEEL_UNR], mv[NEEL_UNR];
+        double ed[NEEL_UNR], edp[NEEL_UNR];
+        float zf[NEEL_UNR], zfp[NEEL_UNR], eb[NEEL_UNR], bt[NEEL_UNR];
+#pragma unroll
+        for (int k = 0; k < NEEL_UNR; ++k) {
+            const int64_t i = base + k * stride;
+            const bool v = i < N;
+            oc[k] = v ? L.occ[i] : (int8_t)0;
+            mv[k] = v ? __ldcg(L.m + i) : (int8_t)0;
+            ed[k] = (v && L.has_dipolar) ? __ldcg(L.E_dip + i) : 0.0;
+            edp[k] = (v && L.has_dipolar && two) ? __ldcg(L.E_dip_perp + i) : 0.0;
+            zf[k] = (v && L.zee) ? __ldg(L.zee + i) : 0.f;
+            zfp[k] = (v && L.zee && two) ? __ldg(L.zee_perp + i) : 0.f;
+            eb[k] = v ? __ldg(L.E_B + i) : 0.f;
+            bt[k] = (v && L.beta_uniform <= 0.0) ? __ldg(L.beta + i) : 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k < NEEL_UNR; ++k) {
+            if (!oc[k]) continue;
+            const int64_t i = base + k * stride;
+            double E = ed[k], Ep = edp[k];
+            if (L.zee) { E += (double)mv[k] * (double)zf[k]; if (two) Ep += (double)mv[k] * (double)zfp[k]; }
+            if (L.has_exchange) {
+                double e, ep;
+                hs_exchange_at(L, (int)(i / L.nx), (int)(i % L.nx), e, ep);
+                E += e;
+                if (two) Ep += ep;
+            }
+            double b1, b2;
+            hs_barriers_from(L, E, Ep, (double)eb[k], b1, b2);
+            const double beta = L.beta_uniform > 0.0 ? L.beta_uniform : (double)bt[k];
+            const double le1 = (double)hs_log_exp1_f32(hs_u53(L.seed, call, (uint32_t)i));
+            double key;
+            if (!two) key = le1 + (b1 - bmin) * beta;
+            else {
+                const double bm = fmin(b1, b2), dd = fabs(b1 - b2);
+                key = le1 + (bm - bmin) * beta - (double)log1pf(expf((float)(-dd * beta)));
+            }
+            best = hs_kmin(best, HsKeyIdx{key, (int)i});
+        }
+    }
+    return best;
+}

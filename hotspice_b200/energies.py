@@ -182,7 +182,8 @@ class DipolarEnergy(Energy):
         self._Kps = torch.as_tensor(ks.Kps, device=dev, dtype=torch.float32).contiguous() if mm.in_plane else None
         self._sub_of = torch.as_tensor(ks.sub_of.reshape(-1), device=dev, dtype=torch.int32)
         self.kernel_unitcell_indices = ks.sub_of
-        self._E = torch.zeros((mm.ny, mm.nx), device=dev, dtype=torch.float32)
+        # FP64 accumulators of the FP32 per-switch increments (see hs_dipolar.cu)
+        self._E = torch.zeros((mm.ny, mm.nx), device=dev, dtype=torch.float64)
         self._Ep = torch.zeros_like(self._E) if mm.in_plane else None
         mm._state_changed()
 
@@ -204,7 +205,7 @@ class DipolarEnergy(Energy):
 
     @property
     def E(self):
-        return self._E.double()
+        return self._E.clone()
 
     @E.setter
     def E(self, value):
@@ -214,11 +215,11 @@ class DipolarEnergy(Energy):
     def E_perp(self):
         if self._Ep is None or not self.mm.USE_PERP_ENERGY:
             return torch.zeros_like(self._E, dtype=torch.float64)
-        return self._Ep.double()
+        return self._Ep.clone()
 
     @property
     def E_tot(self):
-        return float(torch.sum(self._E.double())) / 2
+        return float(torch.sum(self._E)) / 2
 
     def get_NN_interaction(self):
         """Largest nearest-neighbour kernel magnitude times prefactor * <moment>^2

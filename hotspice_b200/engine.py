@@ -73,6 +73,17 @@ def cluster_size_for(mm: Magnets) -> int:
     return 16
 
 
+def step_cost(mm: Magnets) -> float:
+    """Relative cost of one update step (cells scanned or window cells updated)."""
+    d = mm._dipolar()
+    win = (2 * d.kernel_set.wx + 1) * (2 * d.kernel_set.wy + 1) if d is not None else 9
+    if mm.params.UPDATE_SCHEME == Scheme.NEEL:
+        return mm.nx * mm.ny + win
+    if mm.params.UPDATE_SCHEME == Scheme.WOLFF:
+        return mm.nx * mm.ny
+    return 2048 + 2 * win
+
+
 @dataclass
 class _Prepared:
     inst: torch.Tensor
@@ -85,7 +96,9 @@ class BatchEngine:
     """Advance several Magnets at once: ``run(steps)`` (fixed step budgets) or
     ``progress(t_max, MCsteps_max)`` (the reference's stop rule, per instance)."""
 
-    def __init__(self, magnets, cluster_size: int | None = None, device=None):
+    def __init__(self, magnets, cluster_size: int | None = None, device=None, throughput: bool | None = None):
+        """``throughput``: give every instance a single-CTA cluster (best aggregate throughput when
+        there are at least as many instances as SMs); default: on when len(magnets) >= SM count."""
         self.magnets = list(magnets)
         if not self.magnets:
             raise ValueError('BatchEngine needs at least one Magnets instance')
@@ -94,6 +107,11 @@ class BatchEngine:
             if mm.device != self.device:
                 raise ValueError('all instances of a BatchEngine must live on the same device')
         self.cluster_size = cluster_size
+        if throughput is None:
+            throughput = len(self.magnets) >= torch.cuda.get_device_properties(self.device).multi_processor_count
+        self.throughput = throughput
+        self._cache = None
+        self._streams = []
         self.lib = _bind()
         self._work = torch.zeros(1, device=self.device, dtype=torch.int32)
         self._max_clusters = {}
@@ -125,13 +143,30 @@ class BatchEngine:
             I.attempt_freq = 1e10
         return I, [buf, s]
 
+    def _throughput_sizes(self, steps):
+        """Cluster sizes for throughput mode: an instance whose step budget costs more than an
+        even share of the GPU (total cost / SM count) gets enough CTAs to finish in about that
+        share, so one large lattice does not leave the rest of the GPU idle at the end."""
+        n_sm = torch.cuda.get_device_properties(self.device).multi_processor_count
+        costs = [max(1, st) * step_cost(mm) for mm, st in zip(self.magnets, steps)]
+        share = sum(costs) / n_sm
+        out = []
+        for c in costs:
+            cs = 1
+            while cs < 16 and c / cs > share:
+                cs *= 2
+            out.append(cs)
+        return out
+
     def _prepare(self, steps, kws):
         groups = {}
         keep = []
-        for mm, st, kw in zip(self.magnets, steps, kws):
+        tsizes = self._throughput_sizes(steps) if (self.throughput and not self.cluster_size) else None
+        for j, (mm, st, kw) in enumerate(zip(self.magnets, steps, kws)):
             if mm._T_zero:
                 raise RuntimeError('an instance has T=0 somewhere in its domain')
-            cs = self.cluster_size or getattr(mm, '_cluster_size', None) or cluster_size_for(mm)
+            cs = self.cluster_size or (tsizes[j] if tsizes else None) or getattr(mm, '_cluster_size', None) \
+                or cluster_size_for(mm)
             I, k = self._describe(mm, st, kw)
             keep += k
             groups.setdefault(cs, []).append(I)
@@ -144,12 +179,27 @@ class BatchEngine:
         return out
 
     def launch(self, prepared, stream=None):
-        st = stream if stream is not None else torch.cuda.current_stream(self.device).cuda_stream
-        for p in prepared:
-            n_clusters = min(p.n, self._max(p.cs))
-            work = self._work
-            _lib.check(self.lib.hs_engine_run(p.inst.data_ptr(), p.n, p.cs, n_clusters, work.data_ptr(), st),
-                       'hs_engine_run')
+        """One engine launch per cluster-size group; several groups run concurrently on side
+        streams that join the caller's stream again."""
+        main = torch.cuda.current_stream(self.device) if stream is None else stream
+        if len(prepared) == 1:
+            self._launch_one(prepared[0], 0, main.cuda_stream)
+            return
+        if len(self._streams) < len(prepared):
+            self._streams += [torch.cuda.Stream(self.device) for _ in range(len(prepared) - len(self._streams))]
+        while self._work.numel() < len(prepared):
+            self._work = torch.zeros(len(prepared), device=self.device, dtype=torch.int32)
+        for g, p in enumerate(prepared):
+            s = self._streams[g]
+            s.wait_stream(main)
+            self._launch_one(p, g, s.cuda_stream)
+        for g in range(len(prepared)):
+            main.wait_stream(self._streams[g])
+
+    def _launch_one(self, p, g, st):
+        n_clusters = min(p.n, self._max(p.cs))
+        _lib.check(self.lib.hs_engine_run(p.inst.data_ptr(), p.n, p.cs, n_clusters, self._work[g:].data_ptr(), st),
+                   'hs_engine_run')
 
     def run(self, steps, **kwargs):
         """Enqueue ``steps`` (an int or one int per instance) update steps of every instance
@@ -158,7 +208,11 @@ class BatchEngine:
         kws = [dict(kwargs) for _ in self.magnets]
         for mm, kw in zip(self.magnets, kws):
             mm._set_control(progress=0, done=0, t_max=float(kw.pop('t_max', math.inf)))
-        prepared = self._prepare(steps, kws)
+        key = (tuple(steps), tuple(sorted((k, float(v)) for k, v in kwargs.items() if k != 't_max')),
+               tuple(mm._version for mm in self.magnets), self.cluster_size, self.throughput)
+        if self._cache is None or self._cache[0] != key:
+            self._cache = (key, self._prepare(steps, kws))
+        prepared = self._cache[1]
         self.launch(prepared)
         return prepared
 
@@ -196,26 +250,35 @@ class Autotuner:
         win = (d.kernel_set.wx, d.kernel_set.wy) if d is not None else (0, 0)
         return (type(mm).__name__, mm.nx, mm.ny, mm.params.UPDATE_SCHEME, mm.params.MULTISAMPLING_SCHEME, win)
 
-    def tune(self, mm: Magnets, steps=200, candidates=CLUSTER_SIZES, **kw) -> int:
+    def tune(self, mm: Magnets, steps=200, candidates=CLUSTER_SIZES, include_step_kernels=False, **kw) -> int:
+        """Returns the chosen cluster size, or 0 for the per-step kernels (CUDA-graph replays),
+        and configures ``mm.engine`` accordingly."""
         k = self.key(mm)
-        if k in self.cache:
-            mm._cluster_size = self.cache[k]
-            return self.cache[k]
-        snap = mm._snapshot()
-        best, best_t = None, math.inf
-        for cs in candidates:
-            eng = BatchEngine([mm], cluster_size=cs)
-            eng.run(max(steps // 10, 5), **kw)  # warm-up
-            torch.cuda.synchronize(mm.device)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            eng.run(steps, **kw)
-            e1.record()
-            torch.cuda.synchronize(mm.device)
-            t = e0.elapsed_time(e1)
-            mm._restore(snap)
-            if t < best_t:
-                best, best_t = cs, t
-        self.cache[k] = best
-        mm._cluster_size = best
+        if k not in self.cache:
+            snap = mm._snapshot()
+            persistent, cs0 = mm.engine.persistent, mm.engine.cluster_size
+            best, best_t = None, math.inf
+            cands = ([0] if include_step_kernels else []) + list(candidates)
+            for cs in cands:
+                mm.engine.persistent = cs != 0
+                mm.engine.cluster_size = cs
+                mm._engine_cache = None
+                mm.run(max(steps // 10, 5), **kw)  # warm-up (captures graphs / prepares descriptors)
+                torch.cuda.synchronize(mm.device)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                mm.run(steps, **kw)
+                e1.record()
+                torch.cuda.synchronize(mm.device)
+                t = e0.elapsed_time(e1)
+                mm._restore(snap)
+                if t < best_t:
+                    best, best_t = cs, t
+            mm.engine.persistent, mm.engine.cluster_size = persistent, cs0
+            self.cache[k] = best
+        best = self.cache[k]
+        mm.engine.persistent = best != 0
+        mm.engine.cluster_size = best
+        mm._cluster_size = best or None
+        mm._engine_cache = None
         return best

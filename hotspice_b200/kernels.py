@@ -29,6 +29,7 @@ class KernelSet:
     wy: int
     wrap: bool
     full: bool               # window spans every offset of the lattice
+    asymmetry: float = 0.0   # see kernel_asymmetry()
 
 
 def _site_kernels(nx, ny, ux, uy, y, x, dx_cell, dy_cell, ori, occ, in_plane, cutoff, decay, I):
@@ -103,6 +104,7 @@ def build_kernels(mm, cutoff=np.inf, decay_exponent=-3) -> KernelSet:
     if not ks:
         raise ValueError('no occupied unit-cell site: nothing to build a dipolar kernel for')
     K, Kps, Kpo = np.asarray(ks), np.asarray(kps), np.asarray(kpo)
+    asym = kernel_asymmetry(K, sub_of, nx, ny)
     nz = (K != 0) | (Kps != 0) | (Kpo != 0)
     rows = np.nonzero(nz.any(axis=(0, 2)))[0]
     cols = np.nonzero(nz.any(axis=(0, 1)))[0]
@@ -121,4 +123,32 @@ def build_kernels(mm, cutoff=np.inf, decay_exponent=-3) -> KernelSet:
     sl = np.s_[:, ny - 1 - wy:ny + wy, nx - 1 - wx:nx + wx]
     scale = 1e-7  # mu0 / 4 pi
     return KernelSet(K[sl] * scale, Kps[sl] * scale, Kpo[sl] * scale, sub_of, wx, wy, wrap,
-                     wy == ny - 1 and wx == nx - 1 and not wrap)
+                     wy == ny - 1 and wx == nx - 1 and not wrap, asym)
+
+
+def kernel_asymmetry(K, sub_of, nx, ny):
+    """max |K_s(d) - K_s'(-d)| / max |K| over all sites s and offsets d, s' the site at d.
+
+    The interaction of two magnets must not depend on which one is the kernel's centre, and
+    it does not, except through rounding: distances come from cumulative sums of the cell
+    spacings (as in the reference), so r(d) and r(-d) can differ in the last bit, and a pair
+    at exactly the cutoff radius can be kept one way and dropped the other. Incremental
+    updates use the switched magnet's kernel while a full recompute uses the target's, so a
+    non-zero value means the incremental energies drift from a full recompute by design (the
+    reference drifts identically)."""
+    uy, ux = sub_of.shape
+    H, W = 2 * ny - 1, 2 * nx - 1
+    flip = K[:, ::-1, ::-1]
+    worst = 0.0
+    for ys in range(uy):
+        for xs in range(ux):
+            s = sub_of[ys, xs]
+            if s < 0:
+                continue
+            rows = (ys - (ny - 1) + np.arange(H)) % uy
+            cols = (xs - (nx - 1) + np.arange(W)) % ux
+            tgt = sub_of[rows[:, None], cols[None, :]]
+            other = np.where(tgt >= 0, flip[np.clip(tgt, 0, None), np.arange(H)[:, None], np.arange(W)[None, :]], 0.0)
+            worst = max(worst, float(np.max(np.abs(K[s] - other))))
+    den = float(np.max(np.abs(K)))
+    return worst / den if den > 0 else 0.0

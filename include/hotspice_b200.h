@@ -76,8 +76,8 @@ typedef struct HsLattice {
     const float  *K;            /* dipolar kernels (n_sub, 2wy+1, 2wx+1), prefactor excluded */
     const float  *Kpo;          /* "perp-other" kernels, same shape, or NULL                 */
     const float  *Kps;          /* "perp-self" kernels (full recompute only), or NULL        */
-    float        *E_dip;        /* dipolar energy [J]                                        */
-    float        *E_dip_perp;   /* dipolar perpendicular energy, or NULL                     */
+    double       *E_dip;        /* dipolar energy [J] (FP64 accumulator of FP32 increments)  */
+    double       *E_dip_perp;   /* dipolar perpendicular energy, or NULL                     */
     const float  *zee;          /* Zeeman E_factor (E = m * zee), or NULL                    */
     const float  *zee_perp;     /* Zeeman E_factor_perp, or NULL                             */
     const float  *orient;       /* (ny, nx, 2) orientation, in-plane exchange only, or NULL */
@@ -179,8 +179,8 @@ int hs_dipolar_update(const HsLattice *L, const HsSwitchList *sw, const int32_t 
                       int32_t n_host, int32_t semantics, const HsCounters *C, void *stream);
 
 /* ---- (b) full dipolar recompute ---------------------------------------------------------- */
-/* Direct sum over the kernel window. fp64 != 0 accumulates in double and writes double
- * outputs E64/Ep64; otherwise FP32 into L->E_dip / L->E_dip_perp. */
+/* Direct sum over the kernel window. fp64 != 0 accumulates in double, otherwise in float.
+ * Writes E64/Ep64 when given, else L->E_dip / L->E_dip_perp. */
 int hs_dipolar_full_direct(const HsLattice *L, int32_t fp64, double *E64, double *Ep64, void *stream);
 /* Tensor-core implicit GEMM (tcgen05, split-BF16 kernel, FP32 accumulation in TMEM).
  * Writes L->E_dip (and E_dip_perp). `scratch` holds the split kernels; see hs_igemm_scratch_bytes. */
