@@ -33,7 +33,7 @@ def build(verbose: bool = False, force: bool = False, extra=()):
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(d) for d in deps):
         return LIB
     cmd = [nvcc(), *ARCH, '-lineinfo', '-O3', '-std=c++17', '-DHS_BUILD',
-           '-Xcompiler', '-fPIC', '-shared', '-o', LIB + '.tmp', *srcs, '-lcuda', *extra]
+           '-Xcompiler', '-fPIC', '-shared', '-o', LIB + '.tmp', *srcs, *extra]
     if verbose:
         print(' '.join(cmd))
     r = subprocess.run(cmd, capture_output=True, text=True)

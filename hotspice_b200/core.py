@@ -718,7 +718,9 @@ class Magnets(ABC):
         N = self.nx * self.ny
         W = N if ks.full else (2 * ks.wx + 1) * (2 * ks.wy + 1)
         if method == 'auto':
-            method = 'direct64' if N * W <= self.engine.direct_max_pairs else 'igemm'
+            method = 'direct64' if N * W <= self.engine.direct_max_pairs or not self._igemm_ok(d) else 'igemm'
+        elif method == 'igemm' and not self._igemm_ok(d):
+            raise ValueError('igemm recompute needs the full uncropped kernel and a uniform moment')
         if method == 'direct64':
             _lib.check(self._lib.hs_dipolar_full_direct(L, 1, d._E.data_ptr(),
                                                         _ptr(d._Ep) if self.USE_PERP_ENERGY else None,
@@ -730,8 +732,19 @@ class Magnets(ABC):
             buf = self._get_scratch('igemm', max(nbytes, 1))
             _lib.check(self._lib.hs_dipolar_full_igemm(L, self.engine.igemm_splits, buf.data_ptr(), buf.numel(),
                                                         self._stream()), 'hs_dipolar_full_igemm')
+            st = int(buf[nbytes - 256:nbytes - 252].view(torch.int32).item())  # status word (synchronises)
+            if st:
+                raise RuntimeError(f'hs_dipolar_full_igemm reported status {st} (1: wait timed out, 2: moment not uniform)')
         else:
             raise ValueError(f"unknown recompute method '{method}'")
+
+    def _igemm_ok(self, d) -> bool:
+        """The implicit GEMM covers the full uncropped kernel and a uniform moment."""
+        ks = d.kernel_set
+        if not (ks.wx == self.nx - 1 and ks.wy == self.ny - 1 and not ks.wrap):
+            return False
+        mom = self._moment_np[self.occupation.astype(bool)]
+        return mom.size == 0 or bool(np.all(mom == mom.flat[0]))
 
     def _dipolar_apply(self, d, indices2D, semantics):
         idx = np.asarray(indices2D, dtype=np.int64).reshape(2, -1)

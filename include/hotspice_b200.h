@@ -182,8 +182,13 @@ int hs_dipolar_update(const HsLattice *L, const HsSwitchList *sw, const int32_t 
 /* Direct sum over the kernel window. fp64 != 0 accumulates in double, otherwise in float.
  * Writes E64/Ep64 when given, else L->E_dip / L->E_dip_perp. */
 int hs_dipolar_full_direct(const HsLattice *L, int32_t fp64, double *E64, double *Ep64, void *stream);
-/* Tensor-core implicit GEMM (tcgen05, split-BF16 kernel, FP32 accumulation in TMEM).
- * Writes L->E_dip (and E_dip_perp). `scratch` holds the split kernels; see hs_igemm_scratch_bytes. */
+/* Tensor-core implicit GEMM (tcgen05, split-BF16 kernel, FP32 accumulation in TMEM), the
+ * counterpart of DipolarEnergy.update (hotspice/energies.py:290-308) for the full, uncropped
+ * kernel (dip_wx = nx-1, dip_wy = ny-1, no wrap) and a uniform moment over the occupied cells.
+ * nsplit (1..3) BF16 terms of the FP32 kernel. Writes L->E_dip (and E_dip_perp).
+ * `scratch` holds the split kernels and BF16 spins (hs_igemm_scratch_bytes); its last 256 bytes
+ * start with an int32 status word, valid once the stream has reached the end of the call:
+ * 0 = ok, bit 0 = a pipeline wait timed out, bit 1 = the moment is not uniform (E is wrong). */
 int64_t hs_igemm_scratch_bytes(const HsLattice *L, int32_t nsplit);
 int hs_dipolar_full_igemm(const HsLattice *L, int32_t nsplit, void *scratch, int64_t scratch_bytes, void *stream);
 
