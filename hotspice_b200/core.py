@@ -76,7 +76,7 @@ class EngineConfig:
     cluster_size: int = 0          # CTAs per cluster for the persistent launch (0: cost model)
     use_graphs: bool = True        # otherwise: replay progress() chunks from captured CUDA graphs
     graph_steps: int = 64          # steps per captured chunk
-    igemm_splits: int = 3          # BF16 terms of the split kernel in the implicit GEMM
+    igemm_splits: int = 3          # BF16 terms of the split kernel in the implicit GEMM (2: faster, ~1e-6 rel)
 
 
 @dataclass(slots=True)

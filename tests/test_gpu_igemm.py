@@ -13,7 +13,8 @@ import torch
 
 pytestmark = pytest.mark.gpu
 
-TOL_SPLIT3 = 2e-6    # FP32 accumulation of a 24-bit split kernel
+TOL = {3: 1e-6,      # 3 BF16 splits (the default): FP64 near field, FP32 chunks of the far field
+       2: 2e-6}      # 2 splits: 16-bit kernel terms in the far field
 TOL_SPLIT1 = 1e-2    # plain BF16 kernel (8-bit significand)
 
 
@@ -54,12 +55,13 @@ def _compare(mm, nsplit=3):
     ('kag', 36, None, False),      # empty cells, several sublattices
     ('sq', 150, None, True),       # in-plane, periodic, two column tiles
 ])
-def test_igemm_matches_fp64(kind, n, ny, PBC):
+@pytest.mark.parametrize('nsplit', [2, 3])
+def test_igemm_matches_fp64(kind, n, ny, PBC, nsplit):
     mm = _make(kind, n, ny, PBC)
-    err, errp = _compare(mm, 3)
-    print(f'{kind} {mm.nx}x{mm.ny} PBC={PBC}: rel err {err:.2e} perp {errp:.2e}')
-    assert err <= TOL_SPLIT3
-    assert errp <= TOL_SPLIT3
+    err, errp = _compare(mm, nsplit)
+    print(f'{kind} {mm.nx}x{mm.ny} PBC={PBC} nsplit={nsplit}: rel err {err:.2e} perp {errp:.2e}')
+    assert err <= TOL[nsplit]
+    assert errp <= TOL[nsplit]
 
 
 def test_igemm_split_levels():
@@ -67,9 +69,11 @@ def test_igemm_split_levels():
     e1, _ = _compare(mm, 1)
     e2, _ = _compare(mm, 2)
     e3, _ = _compare(mm, 3)
+    # with two or more splits the kernel is carried to 16+ bits and the FP32 accumulation
+    # of the far field dominates, so splits 2 and 3 agree to within that error
     assert e1 <= TOL_SPLIT1
-    assert e3 <= e2 <= e1
-    assert e3 <= TOL_SPLIT3
+    assert max(e2, e3) < e1
+    assert e2 <= TOL[2] and e3 <= TOL[3]
 
 
 def test_igemm_energy_total():
