@@ -369,6 +369,12 @@ def run_product(args):
     single = None
     if rank == 0 and not args.no_single:
         single = run_single(dev, stream)
+    served = None
+    if args.served > 0:
+        served = run_served(dev, args, dist, rank, ws)
+    recompute = None
+    if rank == 0 and args.recompute_n > 0:
+        recompute = run_recompute(dev, n=args.recompute_n)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -401,6 +407,10 @@ def run_product(args):
     }
     if single is not None:
         line["single_instance"] = single
+    if served is not None:
+        line["served"] = served
+    if recompute is not None:
+        line["full_recompute"] = recompute
     if not args.no_cpu_baseline:
         v, secs, st, ni = oracle_sample(specs, seconds_per_instance=args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
@@ -409,6 +419,159 @@ def run_product(args):
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
+
+
+def measured_tensor_peak():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
+            p = json.load(f)
+        return float(p['bf16_tflops_sustained']), float(p['bf16_tflops']), 'measured'
+    except Exception:
+        return 1400.0, 1590.0, 'fallback'
+
+
+def igemm_mma_flops(nx, ny, nsplit, BM=128, BN=256, BK=64):
+    """FLOPs the implicit GEMM issues on the tensor cores for one full recompute (tiles of
+    128 columns x 256 rows, every kernel row that reaches the tile, 64-column K-blocks)."""
+    P = -(-nx // BM) * BM
+    C = P // BK
+    tot = 0
+    for yt in range(-(-ny // BN)):
+        y0 = yt * BN
+        dlo, dhi = max(-(ny - 1), -(y0 + BN - 1)), ny - 1 - y0
+        tot += (dhi - dlo + 1) * C * (P // BM)
+    return tot * nsplit * 2 * BM * BN * BK
+
+
+def run_recompute(dev, n=2048, n_check=512, reps=3):
+    """Full dipolar recompute of an OOP square lattice with the full (uncut) kernel: the
+    tensor-core implicit GEMM timed at n x n, its error against the FP64 direct sum at n_check."""
+    import torch
+    import hotspice_b200 as hs
+
+    def build(k):
+        g = np.random.Generator(np.random.PCG64(SEED + k))
+        m0 = g.integers(0, 2, size=(k, k)) * 2 - 1
+        return hs.ASI.OOP_Square(200e-9, k, T=300.0, E_B=5e-20, moment=1.1e-15, pattern=m0,
+                                 energies=[hs.DipolarEnergy()], engine=hs.EngineConfig(recompute='direct64'),
+                                 seed=SEED + k, device=dev)
+    out = {}
+    mm = build(n_check)
+    d = mm._dipolar()
+    d.update(method='direct64')
+    E64 = d.E
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    d.update(method='direct64')
+    e1.record()
+    torch.cuda.synchronize(dev)
+    t_direct = e0.elapsed_time(e1)
+    d.update(method='igemm')
+    err = float((d.E - E64).abs().max() / E64.abs().max())
+    etot = abs(d.E_tot - float(E64.sum()) / 2) / abs(float(E64.sum()) / 2)
+    e0.record()
+    d.update(method='igemm')
+    e1.record()
+    torch.cuda.synchronize(dev)
+    t_ig_check = e0.elapsed_time(e1)
+    del mm, d, E64
+    torch.cuda.empty_cache()
+    mm = build(n)
+    d = mm._dipolar()
+    nsplit = mm.engine.igemm_splits
+    d.update(method='igemm')
+    torch.cuda.synchronize(dev)
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        d.update(method='igemm')
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ts.append(e0.elapsed_time(e1))
+    ms = float(np.median(ts))
+    fl = igemm_mma_flops(n, n, nsplit)
+    sus, burst, kind = measured_tensor_peak()
+    cells = n * n
+    out.update({
+        "workload": f"OOP_Square {n}x{n} ({cells} magnets), full uncut dipolar kernel ({2*n-1}x{2*n-1}), random +-1 spins; "
+                    f"one full E_dipolar recompute (hs_dipolar_full_igemm, {nsplit} BF16 kernel splits, FP32 TMEM "
+                    f"accumulation in chunks flushed to FP64, near field summed in FP64)",
+        "ms": ms, "pairs_per_s": cells * cells / (ms * 1e-3),
+        "roofline": {"bound": "tensor", "kernel": "igemm_kernel", "achieved": fl / (ms * 1e-3) / 1e12,
+                     "peak": sus, "unit": "TFLOP/s", "frac": fl / (ms * 1e-3) / 1e12 / sus,
+                     "peak_kind": f"{kind} bf16_tflops_sustained (burst {burst})",
+                     "flops": "MMA FLOPs issued per recompute (padded tiles, all splits); the whole call is timed, "
+                              "its split/spin preparation and FP64 finalize included"},
+        "check": {"n": n_check, "max_rel_err_vs_fp64_direct": err, "rel_err_E_tot": etot,
+                  "igemm_ms": t_ig_check, "fp64_direct_ms": t_direct, "speedup": t_direct / t_ig_check},
+    })
+    del mm, d
+    torch.cuda.empty_cache()
+    return out
+
+
+SERVED_WORKLOAD = ("served: the first {k} requests of a seeded Poisson arrival stream (mean 200/s); lattice uniform over "
+                   "{{OOP_Square a=200nm, IP_Pinwheel a=300nm, IP_Kagome a=500nm, exchange-only square Ising J=1e-21 J "
+                   "(Wolff)}}, n log-uniform in [64,1024], steps log-uniform in [1e3,1e5], T uniform in [200,400]K, Zeeman "
+                   "0-5mT random angle, E_B lognormal(5.5e-20, 5%), dipolar cutoff 16a, Neel / Metropolis alternating")
+
+
+def run_served(dev, args, dist, rank, ws):
+    """Continuous batching against one-request-at-a-time solves on the same arrival stream."""
+    import torch
+    from hotspice_b200 import serving as SV
+    reqs = SV.request_stream(args.served, rate=200.0, seed=SEED)
+    mine = SV.shard_requests(reqs, ws, rank) if ws > 1 else reqs
+    srv = SV.Server(device=dev)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    res = srv.serve(mine, realtime=True)
+    torch.cuda.synchronize(dev)
+    # one-at-a-time solves: per-step time of each request alone (a 200-step sample through
+    # Magnets.run, the single-instance persistent launch), scaled to its step budget
+    svc = []
+    for r in mine:
+        mm = SV.build_magnets(r.spec, device=dev)
+        k = min(r.steps, 200)
+        mm.run(k)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        mm.run(k)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        svc.append(e0.elapsed_time(e1) * 1e-3 / k * r.steps)
+        del mm
+    seq_lat = SV.fifo_latencies([r.arrival for r in mine], svc)
+    seq_end = max(a + l for a, l in zip([r.arrival for r in mine], seq_lat))
+    mine_stats = dict(lat=[x.latency for x in res], att=sum(x.attempts for x in res), makespan=srv.stats.makespan,
+                      seq_lat=list(seq_lat), seq_end=seq_end, rounds=srv.stats.rounds, max_active=srv.stats.max_active,
+                      peak=srv.stats.admitted_bytes_peak, budget=srv.hbm_budget)
+    allst = [mine_stats]
+    if dist:
+        allst = [None] * ws
+        dist.all_gather_object(allst, mine_stats)
+    if rank != 0:
+        return None
+    lat = np.concatenate([np.asarray(a['lat']) for a in allst])
+    seq = np.concatenate([np.asarray(a['seq_lat']) for a in allst])
+    att = sum(a['att'] for a in allst)
+    makespan = max(a['makespan'] for a in allst)
+    seq_end = max(a['seq_end'] for a in allst)
+    return {"workload": SERVED_WORKLOAD.format(k=args.served), "requests": int(lat.size),
+            "value": att / makespan, "unit": UNIT, "makespan_s": makespan, "attempts": att,
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_s": float(lat.mean()), "rounds": sum(a['rounds'] for a in allst),
+            "max_resident": max(a['max_active'] for a in allst),
+            "hbm_budget_bytes": allst[0]['budget'], "peak_admitted_bytes": max(a['peak'] for a in allst),
+            "sequential": {"p50_s": float(np.percentile(seq, 50)), "p99_s": float(np.percentile(seq, 99)),
+                           "makespan_s": seq_end, "value": att / seq_end,
+                           "form": "one request at a time, FIFO over the same arrivals; service time = steps x the "
+                                   "request's per-step time alone (200-step sample through Magnets.run)"},
+            "served_over_sequential": seq_end / makespan,
+            "latency_clock": "host wall clock from each request's arrival to its result on the host"}
 
 
 def _counters_dtype():
@@ -453,9 +616,17 @@ def main():
     ap.add_argument('--cpu-seconds', type=float, default=2.5)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-single', action='store_true')
+    ap.add_argument('--served', type=int, default=64, help='requests of the served arrival stream (0: skip)')
+    ap.add_argument('--recompute-n', type=int, default=2048, help='lattice side of the full-recompute timing (0: skip)')
+    ap.add_argument('--only-recompute', action='store_true', help='run only the full-recompute timing and print it')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)
+    elif args.only_recompute:
+        import torch
+        dev = torch.device('cuda', 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({"full_recompute": run_recompute(dev, n=args.recompute_n)}))
     else:
         run_product(args)
 

@@ -113,8 +113,20 @@ class BatchEngine:
         self._cache = None
         self._streams = []
         self.lib = _bind()
-        self._work = torch.zeros(1, device=self.device, dtype=torch.int32)
+        # one work counter per cluster-size group, never reallocated (launches in flight use them)
+        self._work = torch.zeros(len(CLUSTER_SIZES), device=self.device, dtype=torch.int32)
         self._max_clusters = {}
+        self._desc = {}     # id(mm) -> (version, kw key, HsInstance, buffers it points into)
+
+    def set_magnets(self, magnets):
+        """Replace the instance list (a serving loop changes it between launches); descriptors
+        of instances that stay are reused."""
+        self.magnets = list(magnets)
+        if not self.magnets:
+            raise ValueError('BatchEngine needs at least one Magnets instance')
+        live = {id(mm) for mm in self.magnets}
+        self._desc = {k: v for k, v in self._desc.items() if k in live}
+        self._cache = None
 
     def _max(self, cs):
         if cs not in self._max_clusters:
@@ -123,6 +135,16 @@ class BatchEngine:
                 raise RuntimeError(_lib.last_error())
             self._max_clusters[cs] = max(1, n)
         return self._max_clusters[cs]
+
+    def _describe_cached(self, mm: Magnets, steps: int, kw) -> tuple[HsInstance, list]:
+        key = (mm._version, tuple(sorted((k, float(v)) for k, v in kw.items())))
+        hit = self._desc.get(id(mm))
+        if hit is None or hit[0] is not mm or hit[1] != key:
+            I, keep = self._describe(mm, steps, kw)
+            self._desc[id(mm)] = hit = (mm, key, I, keep)
+        I = HsInstance.from_buffer_copy(hit[2])
+        I.steps = int(steps)
+        return I, hit[3]
 
     def _describe(self, mm: Magnets, steps: int, kw) -> tuple[HsInstance, list]:
         kind, L, s, extra, buf = mm._step_args(kw)
@@ -158,23 +180,26 @@ class BatchEngine:
             out.append(cs)
         return out
 
-    def _prepare(self, steps, kws):
+    def _prepare(self, steps, kws, sizes=None):
         groups = {}
         keep = []
-        tsizes = self._throughput_sizes(steps) if (self.throughput and not self.cluster_size) else None
+        tsizes = self._throughput_sizes(steps) if (self.throughput and not self.cluster_size and not sizes) else None
         for j, (mm, st, kw) in enumerate(zip(self.magnets, steps, kws)):
             if mm._T_zero:
                 raise RuntimeError('an instance has T=0 somewhere in its domain')
-            cs = self.cluster_size or (tsizes[j] if tsizes else None) or getattr(mm, '_cluster_size', None) \
-                or cluster_size_for(mm)
-            I, k = self._describe(mm, st, kw)
+            cs = (sizes[j] if sizes else None) or self.cluster_size or (tsizes[j] if tsizes else None) \
+                or getattr(mm, '_cluster_size', None) or cluster_size_for(mm)
+            if cs not in CLUSTER_SIZES:
+                raise ValueError(f'cluster size {cs} not in {CLUSTER_SIZES}')
+            I, k = self._describe_cached(mm, st, kw)
             keep += k
             groups.setdefault(cs, []).append(I)
         out = []
         for cs, lst in sorted(groups.items()):
             arr = (HsInstance * len(lst))(*lst)
             raw = np.frombuffer(bytes(arr), dtype=np.uint8)
-            t = torch.from_numpy(raw.copy()).to(self.device)
+            # pinned staging + asynchronous copy on the current stream: no host synchronisation
+            t = torch.from_numpy(raw.copy()).pin_memory().to(self.device, non_blocking=True)
             out.append(_Prepared(t, len(lst), cs, keep))
         return out
 
@@ -187,8 +212,6 @@ class BatchEngine:
             return
         if len(self._streams) < len(prepared):
             self._streams += [torch.cuda.Stream(self.device) for _ in range(len(prepared) - len(self._streams))]
-        while self._work.numel() < len(prepared):
-            self._work = torch.zeros(len(prepared), device=self.device, dtype=torch.int32)
         for g, p in enumerate(prepared):
             s = self._streams[g]
             s.wait_stream(main)
@@ -201,17 +224,18 @@ class BatchEngine:
         _lib.check(self.lib.hs_engine_run(p.inst.data_ptr(), p.n, p.cs, n_clusters, self._work[g:].data_ptr(), st),
                    'hs_engine_run')
 
-    def run(self, steps, **kwargs):
+    def run(self, steps, sizes=None, **kwargs):
         """Enqueue ``steps`` (an int or one int per instance) update steps of every instance
-        without the stop rule; asynchronous."""
+        without the stop rule; asynchronous. ``sizes``: optional cluster size per instance."""
         steps = [int(steps)] * len(self.magnets) if np.isscalar(steps) else [int(s) for s in steps]
         kws = [dict(kwargs) for _ in self.magnets]
         for mm, kw in zip(self.magnets, kws):
             mm._set_control(progress=0, done=0, t_max=float(kw.pop('t_max', math.inf)))
         key = (tuple(steps), tuple(sorted((k, float(v)) for k, v in kwargs.items() if k != 't_max')),
-               tuple(mm._version for mm in self.magnets), self.cluster_size, self.throughput)
+               tuple(mm._version for mm in self.magnets), tuple(id(mm) for mm in self.magnets),
+               tuple(sizes) if sizes else None, self.cluster_size, self.throughput)
         if self._cache is None or self._cache[0] != key:
-            self._cache = (key, self._prepare(steps, kws))
+            self._cache = (key, self._prepare(steps, kws, sizes))
         prepared = self._cache[1]
         self.launch(prepared)
         return prepared

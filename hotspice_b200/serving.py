@@ -1,0 +1,414 @@
+"""Serving: a request loop for parameter-sweep simulations with continuous batching.
+
+Requests (one lattice, its parameters and a step budget each) arrive over time. The
+:class:`Server` admits them while device memory (an HBM budget, from each request's footprint
+estimate) and instance slots allow, keeps every admitted Magnets state resident on the GPU,
+and advances all admitted instances together in *rounds*: one persistent engine launch
+(``hs_engine_run``, hotspice_b200/csrc/hs_engine.cu) per round, in which every instance runs a
+quantum of steps sized so that each gets about the same device time (processor sharing
+between the requests on the GPU). Requests that arrive while a round runs are built on the
+host and admitted into the next round, which is queued on the device behind the running one,
+so their work overlaps with the requests already there. A request retires when its step
+budget is done; its result and completion latency are recorded at that round's end.
+
+Results do not depend on the mix: each instance draws its variates from its own Philox stream
+(keyed by its seed and its own step counters on the device), and the engine runs the same
+per-instance step sequence however the steps are cut into rounds and whichever cluster size
+runs them, so a request gives the same final state alone and in any mix.
+
+The scheduling policy (:class:`AdmissionQueue`, :func:`plan_quanta`, :func:`shard_requests`)
+is plain host code; the reference has no serving layer (its experiments call
+``Magnets.progress`` in a loop, hotspice/core.py:736-760, one simulation at a time).
+"""
+from __future__ import annotations
+
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .engine import step_cost
+
+LATTICE_GEOMETRY = {
+    # lattice: (a, moment) of the sweep's instances
+    'OOP_Square': (200e-9, 1.1e-15),
+    'IP_Pinwheel': (300e-9, 1e-15),
+    'IP_Kagome': (500e-9, 1e-15),
+    'Ising_Square': (200e-9, 1.1e-15),   # exchange-only OOP square lattice, Wolff updates
+}
+
+
+@dataclass
+class SimRequest:
+    """One simulation: ``spec`` describes the lattice and its parameters (see
+    :func:`build_magnets`), ``steps`` the update steps to run, ``arrival`` the time (s) after
+    the start of the stream at which it arrives."""
+    rid: int
+    spec: dict
+    steps: int
+    arrival: float = 0.0
+
+
+@dataclass
+class SimResult:
+    rid: int
+    steps: int
+    arrival: float
+    admitted: float
+    finished: float
+    switches: int
+    attempts: int
+    t: float
+    E_tot: float
+    m_avg: float
+    state: np.ndarray | None = None    # final spins (int8), when the server keeps them
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+def geometry_shape(spec) -> tuple[int, int]:
+    """(ny, nx) of the lattice a spec builds (IP_Kagome derives ny from nx, hotspice/ASI.py)."""
+    n = int(spec['n'])
+    if spec['lattice'] == 'IP_Kagome':
+        return int(n / math.sqrt(3)) // 4 * 4 - 1, n
+    return n, n
+
+
+def footprint_bytes(spec) -> int:
+    """Device bytes a request holds while resident (estimate made before it is built): per
+    cell the spins, moments, FP64 energies (and perpendicular energies), E_B, temperature and
+    Zeeman factors, scratch; plus the kernel windows of the dipolar cutoff."""
+    ny, nx = geometry_shape(spec)
+    cells = nx * ny
+    per_cell = 96 if spec['lattice'] in ('IP_Pinwheel', 'IP_Kagome') else 64
+    kern = 0
+    if spec['lattice'] != 'Ising_Square':
+        w = int(spec.get('cutoff_cells', 16)) * 4 + 1
+        kern = 6 * 3 * w * w * 4
+    return cells * per_cell + kern + (1 << 20)
+
+
+def instance_inputs(spec):
+    """Seeded start state (iid +-1) and lognormal E_B field of a spec."""
+    ny, nx = geometry_shape(spec)
+    g = np.random.Generator(np.random.PCG64(int(spec['seed'])))
+    m0 = g.integers(0, 2, size=(ny, nx)) * 2 - 1
+    EB = float(spec.get('E_B', 5.5e-20)) * g.lognormal(-0.05 ** 2 / 2, 0.05, size=(ny, nx))
+    return m0, EB
+
+
+def build_magnets(spec, device=None):
+    """The Magnets instance of a request spec: ``lattice`` in LATTICE_GEOMETRY, ``n`` (grid
+    side), ``T``, Zeeman ``B`` (T) at ``angle``, ``scheme`` ('Neel' / 'Metropolis'; Ising
+    lattices use Wolff with exchange ``J``), ``seed``; dipolar cutoff of ``cutoff_cells``
+    lattice constants (default 16)."""
+    import hotspice_b200 as hs
+    lat = spec['lattice']
+    a, moment = LATTICE_GEOMETRY[lat]
+    m0, EB = instance_inputs(spec)
+    if lat == 'Ising_Square':
+        return hs.ASI.OOP_Square(a, int(spec['n']), T=spec['T'], E_B=0.0, moment=moment, pattern=m0, PBC=True,
+                                 energies=[hs.ExchangeEnergy(J=float(spec.get('J', 1e-21)))],
+                                 params=hs.SimParams(UPDATE_SCHEME='Wolff', MULTISAMPLING_SCHEME='cluster'),
+                                 seed=int(spec['seed']), device=device)
+    cls = getattr(hs.ASI, lat)
+    cut = float(spec.get('cutoff_cells', 16)) * a
+    return cls(a, int(spec['n']), T=spec['T'], E_B=EB, moment=moment, pattern=m0,
+               energies=[hs.DipolarEnergy(cutoff_range=cut), hs.ZeemanEnergy(spec.get('B', 0.0), spec.get('angle', 0.0))],
+               params=hs.SimParams(UPDATE_SCHEME=spec.get('scheme', 'Neel')), seed=int(spec['seed']), device=device)
+
+
+def request_stream(n_requests, rate=200.0, n_range=(64, 1024), steps_range=(1000, 100000), seed=7,
+                   lattices=('OOP_Square', 'IP_Pinwheel', 'IP_Kagome', 'Ising_Square')):
+    """Seeded Poisson arrival stream of sweep requests: exponential inter-arrival times of
+    mean 1/rate, lattice uniform over ``lattices``, n and steps log-uniform over their ranges,
+    T uniform in [200, 400] K, Zeeman 0-5 mT at a random angle; dipolar lattices alternate
+    Néel / Metropolis."""
+    g = np.random.Generator(np.random.PCG64(seed))
+    t = 0.0
+    out = []
+    for i in range(n_requests):
+        t += float(g.exponential(1.0 / rate))
+        lat = lattices[int(g.integers(0, len(lattices)))]
+        n = int(round(math.exp(g.uniform(math.log(n_range[0]), math.log(n_range[1])))))
+        steps = int(round(math.exp(g.uniform(math.log(steps_range[0]), math.log(steps_range[1])))))
+        spec = dict(lattice=lat, n=n, T=float(g.uniform(200, 400)), B=float(g.uniform(0, 5e-3)),
+                    angle=float(g.uniform(0, 2 * math.pi)), scheme='Neel' if i % 2 == 0 else 'Metropolis',
+                    seed=seed * 1_000_003 + i)
+        out.append(SimRequest(i, spec, steps, t))
+    return out
+
+
+class AdmissionQueue:
+    """Arrived requests wait here in arrival order; :meth:`admit` hands out those that fit
+    the free device bytes and slots, first come first admitted. A request that does not fit
+    yet lets later ones that do fit pass it, until it has been passed over ``max_skip`` times;
+    from then on nothing behind it is admitted before it (so a large request cannot starve)."""
+
+    def __init__(self, footprint=footprint_bytes, max_skip=64):
+        self.waiting: deque[SimRequest] = deque()
+        self.footprint = footprint
+        self.max_skip = max_skip
+        self._skipped = {}
+
+    def push(self, req: SimRequest):
+        self.waiting.append(req)
+
+    def __len__(self):
+        return len(self.waiting)
+
+    def admit(self, free_bytes: int, free_slots: int) -> list[SimRequest]:
+        out, keep = [], deque()
+        blocked = False
+        while self.waiting:
+            r = self.waiting.popleft()
+            need = self.footprint(r.spec)
+            if not blocked and free_slots > 0 and need <= free_bytes:
+                out.append(r)
+                free_bytes -= need
+                free_slots -= 1
+                self._skipped.pop(r.rid, None)
+                continue
+            keep.append(r)
+            if not blocked:
+                s = self._skipped.get(r.rid, 0) + 1
+                self._skipped[r.rid] = s
+                if s > self.max_skip:
+                    blocked = True   # the head has been bypassed long enough: admit nothing behind it
+        self.waiting = keep
+        return out
+
+
+def plan_cluster_sizes(remaining_costs, n_sm, sizes=(1, 2, 4, 8, 16)):
+    """CTAs per instance for the next round: an instance whose remaining work exceeds an even
+    share of the GPU (total remaining work / SM count) gets enough CTAs (a power of two, at
+    most 16) to finish in about that share, so large requests do not hold the tail."""
+    share = max(sum(remaining_costs) / max(n_sm, 1), 1.0)
+    out = []
+    for c in remaining_costs:
+        cs = sizes[0]
+        for s in sizes:
+            cs = s
+            if c / s <= share:
+                break
+        out.append(cs)
+    return out
+
+
+def plan_quanta(costs, remaining, quantum_cost, sizes=None):
+    """Steps each active instance runs in the next round: about ``quantum_cost`` cost units
+    per CTA of its cluster (the per-step cost of :func:`hotspice_b200.engine.step_cost`), at
+    least one step, at most what remains of its budget."""
+    sizes = sizes or [1] * len(costs)
+    out = []
+    for c, r, cs in zip(costs, remaining, sizes):
+        q = max(1, int(quantum_cost * cs // max(c, 1)))
+        out.append(int(min(q, r)))
+    return out
+
+
+def shard_requests(requests, world_size, rank):
+    """The requests one rank serves: greedy least-loaded assignment of the stream (in arrival
+    order) by estimated work (steps x per-step cost), the same on every rank, so no
+    collective is needed to agree on it."""
+    load = [0.0] * world_size
+    mine = []
+    for r in requests:
+        ny, nx = geometry_shape(r.spec)
+        w = r.steps * float(nx * ny + 1089)
+        k = min(range(world_size), key=lambda j: (load[j], j))
+        load[k] += w
+        if k == rank:
+            mine.append(r)
+    return mine
+
+
+@dataclass(eq=False)
+class _Active:
+    req: SimRequest
+    mm: object
+    remaining: int
+    cost: float
+    admitted: float
+    bytes: int
+    event: object = None         # build finished (stream event)
+
+
+@dataclass
+class ServeStats:
+    makespan: float = 0.0
+    rounds: int = 0
+    max_active: int = 0
+    attempts: int = 0
+    admitted_bytes_peak: int = 0
+    history: list = field(default_factory=list)
+
+
+class Server:
+    """Continuous-batching request loop on one GPU.
+
+    ``hbm_budget``: device bytes the resident instances may hold (default: half of the free
+    memory when the server starts); ``max_slots``: resident instances at most; ``round_ms``:
+    device time one instance's quantum aims at; ``keep_state``: return the final spins."""
+
+    def __init__(self, device=None, hbm_budget=None, max_slots=4096, round_ms=5.0, keep_state=False,
+                 max_inflight=2):
+        import torch
+        from .engine import BatchEngine  # noqa: F401  (binds the engine symbols early)
+        self.torch = torch
+        self.device = torch.device(device) if device is not None else torch.device('cuda', torch.cuda.current_device())
+        if hbm_budget is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            hbm_budget = free // 2
+        self.hbm_budget = int(hbm_budget)
+        self.max_slots = int(max_slots)
+        self.round_ms = float(round_ms)
+        self.keep_state = keep_state
+        self.max_inflight = max(1, int(max_inflight))
+        self.n_sm = torch.cuda.get_device_properties(self.device).multi_processor_count
+        self.sm_rate = 1.5e8          # cost units per second per SM; refined from measured rounds
+        self.stream = torch.cuda.Stream(self.device)
+        self.build_stream = torch.cuda.Stream(self.device)
+        self.stats = ServeStats()
+        self._engine = None
+
+    # -- one round ---------------------------------------------------------------------
+    def _launch_round(self, active: list[_Active]):
+        torch = self.torch
+        quantum = self.sm_rate * self.round_ms * 1e-3
+        sizes = plan_cluster_sizes([a.cost * a.remaining for a in active], self.n_sm)
+        steps = plan_quanta([a.cost for a in active], [a.remaining for a in active], quantum, sizes)
+        if self._engine is None:
+            from .engine import BatchEngine
+            self._engine = BatchEngine([a.mm for a in active], device=self.device, throughput=True)
+        else:
+            self._engine.set_magnets([a.mm for a in active])
+        eng = self._engine
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(self.stream):
+            for a in active:
+                if a.event is not None:
+                    self.stream.wait_event(a.event)
+                    a.event = None
+            e0.record(self.stream)
+            prepared = eng.run(steps, sizes=sizes)
+            e1.record(self.stream)
+        for a, s in zip(active, steps):
+            a.remaining -= s
+        cost = sum(s * a.cost for a, s in zip(active, steps))
+        return dict(prepared=prepared, e0=e0, e1=e1, members=list(active), steps=steps, cost=cost,
+                    ctas=sum(sizes))
+
+    def _retire(self, a: _Active, now: float, t0: float) -> SimResult:
+        mm = a.mm
+        with self.torch.cuda.stream(self.stream):
+            c = mm._read_counters()
+            res = SimResult(rid=a.req.rid, steps=a.req.steps, arrival=a.req.arrival, admitted=a.admitted - t0,
+                            finished=now - t0, switches=int(c['switches']), attempts=int(c['attempted']),
+                            t=float(c['t']), E_tot=float(mm.E_tot), m_avg=float(mm.m_avg),
+                            state=mm._m_dev.cpu().numpy().copy() if self.keep_state else None)
+            st = int(c['status'])
+        if st:
+            raise RuntimeError(f'request {a.req.rid}: device step reported status {st} (HS_ST_* bits)')
+        return res
+
+    # -- the loop ----------------------------------------------------------------------
+    def serve(self, requests, realtime=True) -> list[SimResult]:
+        """Serve ``requests`` (arrival times relative to now when ``realtime``; otherwise all
+        are present at the start). Returns one SimResult per request, in completion order."""
+        torch = self.torch
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        queue = AdmissionQueue()
+        active: list[_Active] = []
+        inflight: deque = deque()
+        results: list[SimResult] = []
+        used_bytes = 0
+        t0 = time.perf_counter()
+        st = self.stats = ServeStats()
+
+        def clock():
+            return time.perf_counter() - t0
+
+        def admit():
+            nonlocal used_bytes
+            now = clock()
+            while pending and (not realtime or pending[0].arrival <= now):
+                queue.push(pending.popleft())
+            if not queue:
+                return False
+            reserved = sum(a.bytes for a in active)
+            new = queue.admit(self.hbm_budget - reserved, self.max_slots - len(active))
+            for r in new:
+                with torch.cuda.stream(self.build_stream):
+                    mm = build_magnets(r.spec, device=self.device)
+                    ev = torch.cuda.Event()
+                    ev.record(self.build_stream)
+                b = footprint_bytes(r.spec)
+                active.append(_Active(r, mm, int(r.steps), float(step_cost(mm)), time.perf_counter(), b, ev))
+            used_bytes = sum(a.bytes for a in active)
+            st.admitted_bytes_peak = max(st.admitted_bytes_peak, used_bytes)
+            return bool(new)
+
+        while pending or queue or active or inflight:
+            admit()
+            runnable = [a for a in active if a.remaining > 0]
+            if runnable and len(inflight) < self.max_inflight:
+                inflight.append(self._launch_round(runnable))
+                st.rounds += 1
+                st.max_active = max(st.max_active, len(runnable))
+                continue
+            if inflight:
+                rd = inflight[0]
+                # overlap: build newly arrived requests while the oldest round runs
+                while not rd['e1'].query():
+                    if not admit():
+                        time.sleep(50e-6)
+                rd['e1'].synchronize()
+                inflight.popleft()
+                ms = rd['e0'].elapsed_time(rd['e1'])
+                if ms > 0.05:
+                    busy = max(1, min(self.n_sm, rd['ctas']))
+                    rate = rd['cost'] / (ms * 1e-3) / busy
+                    self.sm_rate = 0.5 * self.sm_rate + 0.5 * rate
+                st.history.append((clock(), len(rd['members']), ms))
+                now = time.perf_counter()
+                done_ids = set()
+                for a in rd['members']:
+                    if a.remaining <= 0 and not any(a is m for r2 in inflight for m in r2['members']):
+                        results.append(self._retire(a, now, t0))
+                        st.attempts += results[-1].attempts
+                        done_ids.add(id(a))
+                if done_ids:
+                    active[:] = [a for a in active if id(a) not in done_ids]
+                continue
+            if queue and not active:
+                r = queue.waiting[0]
+                raise RuntimeError(f'request {r.rid} needs about {footprint_bytes(r.spec)} device bytes, more than the '
+                                   f'HBM budget of {self.hbm_budget} (or max_slots={self.max_slots} is 0)')
+            if pending and realtime:
+                time.sleep(max(0.0, min(1e-3, pending[0].arrival - clock())))
+        st.makespan = clock()
+        return results
+
+
+def latency_summary(results) -> dict:
+    lat = np.array([r.latency for r in results], dtype=float)
+    if lat.size == 0:
+        return {'p50_s': None, 'p99_s': None, 'mean_s': None}
+    return {'p50_s': float(np.percentile(lat, 50)), 'p99_s': float(np.percentile(lat, 99)), 'mean_s': float(lat.mean())}
+
+
+def fifo_latencies(arrivals, service_times) -> np.ndarray:
+    """Completion latencies of a one-at-a-time server (first come, first served) with the
+    given arrival and service times."""
+    t = 0.0
+    out = []
+    for a, s in zip(arrivals, service_times):
+        t = max(t, a) + s
+        out.append(t - a)
+    return np.asarray(out)

@@ -1,0 +1,130 @@
+"""Host-side serving policy (no GPU): admission by HBM footprint and slots, round quanta,
+FIFO latency model, the seeded request stream, and the per-rank sharding of the stream,
+including a two-rank gloo run that checks the ranks agree on a disjoint, complete split."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from hotspice_b200 import serving as S
+
+
+def _req(rid, n, steps=1000, lattice='OOP_Square', arrival=0.0):
+    return S.SimRequest(rid, dict(lattice=lattice, n=n, T=300.0, seed=rid), steps, arrival)
+
+
+def test_request_stream_is_seeded_and_poisson():
+    a = S.request_stream(2000, rate=200.0, seed=3)
+    b = S.request_stream(2000, rate=200.0, seed=3)
+    assert [(r.spec, r.steps, r.arrival) for r in a] == [(r.spec, r.steps, r.arrival) for r in b]
+    gaps = np.diff([0.0] + [r.arrival for r in a])
+    assert abs(gaps.mean() - 1 / 200.0) < 0.1 / 200.0          # mean inter-arrival 5 ms
+    ns = np.array([r.spec['n'] for r in a])
+    steps = np.array([r.steps for r in a])
+    assert ns.min() >= 64 and ns.max() <= 1024
+    assert steps.min() >= 1000 and steps.max() <= 100000
+    # log-uniform: the median sits near the geometric mean of the range
+    assert abs(np.log(np.median(steps)) - np.log(1e4)) < 0.25
+    assert {r.spec['lattice'] for r in a} == {'OOP_Square', 'IP_Pinwheel', 'IP_Kagome', 'Ising_Square'}
+
+
+def test_footprint_grows_with_cells():
+    small = S.footprint_bytes(dict(lattice='OOP_Square', n=64))
+    big = S.footprint_bytes(dict(lattice='OOP_Square', n=1024))
+    assert big > small * 20
+    assert S.footprint_bytes(dict(lattice='IP_Pinwheel', n=256)) > S.footprint_bytes(dict(lattice='OOP_Square', n=256))
+
+
+def test_admission_respects_bytes_and_slots():
+    q = S.AdmissionQueue(footprint=lambda spec: spec['n'])
+    for i, n in enumerate([5, 3, 4, 1]):
+        q.push(_req(i, n))
+    got = q.admit(free_bytes=8, free_slots=10)
+    assert [r.rid for r in got] == [0, 1]          # 5 + 3 fill the 8 bytes
+    assert [r.rid for r in q.waiting] == [2, 3]
+    assert [r.rid for r in q.admit(free_bytes=2, free_slots=10)] == [3]   # 1 passes the 4 that does not fit
+    q2 = S.AdmissionQueue(footprint=lambda spec: 1)
+    for i in range(5):
+        q2.push(_req(i, 1))
+    assert len(q2.admit(free_bytes=100, free_slots=2)) == 2
+    assert len(q2) == 3
+
+
+def test_admission_bypass_is_bounded():
+    q = S.AdmissionQueue(footprint=lambda spec: spec['n'], max_skip=2)
+    q.push(_req(0, 10))                            # too big for now
+    for i in range(1, 6):
+        q.push(_req(i, 1))
+    assert [r.rid for r in q.admit(3, 100)] == [1, 2, 3]   # small ones pass the big head
+    assert [r.rid for r in q.admit(1, 100)] == [4]
+    assert q.admit(1, 100) == []                   # passed over 3 times: the head now blocks
+    assert [r.rid for r in q.admit(11, 100)] == [0, 5]
+
+
+def test_plan_quanta():
+    steps = S.plan_quanta([100.0, 1000.0, 1e6], [50, 1000, 7], quantum_cost=10000.0)
+    assert steps == [50, 10, 1]                    # capped by what remains; at least one step
+    steps = S.plan_quanta([1000.0, 1000.0], [10**6, 10**6], quantum_cost=10000.0, sizes=[1, 8])
+    assert steps == [10, 80]                       # per CTA of the instance's cluster
+
+
+def test_plan_cluster_sizes():
+    # one request holds almost all the remaining work: it gets the largest cluster
+    assert S.plan_cluster_sizes([1e9, 1e3, 1e3], n_sm=148) == [16, 1, 1]
+    # many equal requests: one CTA each
+    assert S.plan_cluster_sizes([1e6] * 300, n_sm=148) == [1] * 300
+    assert S.plan_cluster_sizes([4e6, 1e6, 1e6], n_sm=4) == [4, 1, 1]
+
+
+def test_fifo_latencies():
+    lat = S.fifo_latencies([0.0, 0.1, 0.2], [0.5, 0.1, 0.1])
+    assert np.allclose(lat, [0.5, 0.5, 0.5])
+
+
+def test_shard_requests_partition():
+    reqs = S.request_stream(300, seed=5)
+    shards = [S.shard_requests(reqs, 3, r) for r in range(3)]
+    ids = sorted(x.rid for s in shards for x in s)
+    assert ids == list(range(300))
+    loads = [sum(x.steps * (S.geometry_shape(x.spec)[0] * S.geometry_shape(x.spec)[1] + 1089) for x in s) for s in shards]
+    assert max(loads) <= 1.5 * min(loads)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(('127.0.0.1', 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out):
+    os.environ.update(MASTER_ADDR='127.0.0.1', MASTER_PORT=str(port))
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        reqs = S.request_stream(200, seed=11)
+        mine = [r.rid for r in S.shard_requests(reqs, world, rank)]
+        gathered = [None] * world
+        dist.all_gather_object(gathered, mine)
+        if rank == 0:
+            out.put(gathered)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_shard_requests_two_ranks_gloo():
+    ctx = mp.get_context('spawn')
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    gathered = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    a, b = map(set, gathered)
+    assert not (a & b)
+    assert a | b == set(range(200))
+    assert abs(len(a) - len(b)) < 100
