@@ -437,21 +437,22 @@ __device__ __forceinline__ bool near_offset(int64_t d, int n, int pbc, int w) {
 // sums in FP64, so that the FP32 tensor-core accumulator only carries the far field).
 __global__ void strips_kernel(const float *K, int nx, int ny, int U, int nsplit, int qspan, int qmin, int pbc, int w,
                               __nv_bfloat16 *out) {
-    const int64_t W = 2 * nx - 1, H = 2 * ny - 1;
-    const int64_t total = (int64_t)U * H * qspan * 64;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-        const int rt = (int)(e % 64);
-        const int64_t q_idx = (e / 64) % qspan;
-        const int64_t dyi = (e / (64 * qspan)) % H;
-        const int s = (int)(e / (64 * qspan * H));
-        const int64_t col = 8 * (q_idx + qmin) + (nx - 128) + (rt >> 3) + (rt & 7);
-        float v = (col >= 0 && col < W) ? K[((int64_t)s * H + dyi) * W + col] : 0.f;
-        if (near_offset(dyi - (ny - 1), ny, pbc, w) && near_offset(col - (nx - 1), nx, pbc, w)) v = 0.f;
+    // one block per kernel row (sublattice s, row dyi); 32-bit index arithmetic within the row
+    const int H = 2 * ny - 1, W = 2 * nx - 1;
+    const int row = blockIdx.x, s = row / H, dyi = row - s * H;
+    const bool near_y = near_offset(dyi - (ny - 1), ny, pbc, w);
+    const float *Krow = K + (int64_t)row * W;
+    const int n = qspan * 64;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        const int rt = e & 63, q = e >> 6;
+        const int col = 8 * (q + qmin) + (nx - 128) + (rt >> 3) + (rt & 7);
+        float v = (col >= 0 && col < W) ? __ldg(Krow + col) : 0.f;
+        if (near_y && near_offset(col - (nx - 1), nx, pbc, w)) v = 0.f;
         float rem = v;
         for (int sp = 0; sp < nsplit; ++sp) {
             const __nv_bfloat16 b = __float2bfloat16_rn(rem);
             rem -= __bfloat162float(b);
-            out[((((int64_t)s * nsplit + sp) * H + dyi) * qspan + q_idx) * 64 + rt] = b;
+            out[(((int64_t)(s * nsplit + sp) * H + dyi) * qspan) * 64 + e] = b;
         }
     }
 }
@@ -566,7 +567,8 @@ int hs_launch_igemm(const HsLattice &L, int nsplit, void *scratch, int64_t scrat
     // near offsets go to the FP64 finalize when the periodic near window does not overlap itself
     const int near_w = (L.nx >= 2 * NEAR_W + 1 && L.ny >= 2 * NEAR_W + 1) ? NEAR_W : -1;
     const int pbc = L.pbc ? 1 : 0;
-    strips_kernel<<<148 * 8, 256, 0, st>>>(L.K, L.nx, L.ny, L.n_sub, nsplit, lo.qspan, lo.qmin, pbc, near_w, strips);
+    const int strip_rows = L.n_sub * (2 * L.ny - 1);
+    strips_kernel<<<strip_rows, 256, 0, st>>>(L.K, L.nx, L.ny, L.n_sub, nsplit, lo.qspan, lo.qmin, pbc, near_w, strips);
     if ((rc = hs_check_launch("strips_kernel"))) return rc;
     // the moment must be uniform (the spins are the exact BF16 operand): spins_bf16_kernel flags it
     spins_bf16_kernel<<<148 * 4, 256, 0, st>>>(L.m, L.moment, L.nx, L.ny, lo.P, lo.rows, first, spins, status);
@@ -579,7 +581,7 @@ int hs_launch_igemm(const HsLattice &L, int nsplit, void *scratch, int64_t scrat
         double *out = pass == 0 ? L.E_dip : L.E_dip_perp;
         const float *Kpass = pass == 0 ? L.K : L.Kps;
         if (pass == 1) {  // perpendicular energy: perp-self kernels
-            strips_kernel<<<148 * 8, 256, 0, st>>>(Kpass, L.nx, L.ny, L.n_sub, nsplit, lo.qspan, lo.qmin, pbc, near_w, strips);
+            strips_kernel<<<strip_rows, 256, 0, st>>>(Kpass, L.nx, L.ny, L.n_sub, nsplit, lo.qspan, lo.qmin, pbc, near_w, strips);
             if ((rc = hs_check_launch("strips_kernel"))) return rc;
         }
         cudaMemsetAsync(out, 0, sizeof(double) * (size_t)L.nx * L.ny, st);

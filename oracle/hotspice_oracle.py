@@ -11,7 +11,7 @@ full-grid array work the reference does per step, so that timing this oracle is 
 fair stand-in for timing the reference's NumPy path (the reference cannot travel
 to machines without its source tree).
 
-Deviations, all documented in DESIGN.md:
+Deviations from the reference (deliberate, each checked by the tests):
 * the full dipolar recompute uses FFT convolution (FP64, ~1e-15 relative) instead of
   SciPy's direct ``convolve2d`` (hotspice/energies.py:303) so that large lattices
   initialise in seconds;

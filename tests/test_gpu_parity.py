@@ -183,3 +183,48 @@ def test_update_single_and_multiple_match_oracle():
         mo.update_energy(idx)
         mp.update_energy(idx)
         assert rel_err(_np(mp.E), mo.E) < E_TOL, k
+
+
+def test_metropolis_poisson_lockstep():
+    """Poisson-disc multisampling in cell units: the device's dart throwing (one warp)
+    consumes the oracle's variates in the same order, so candidates, acceptances, switch
+    counts and the Philox call count agree step by step; the candidates keep the disc
+    distance (r + 1 in the continuous plane, minus the rounding to cell centres)."""
+    from oracle.hotspice_oracle import force_metropolis, metropolis_decision
+    a, n = 200e-9, 48
+    g = np.random.Generator(np.random.PCG64(77))
+    spec = {'lattice': 'OOP_Square', 'a': a, 'moment': 1e-15, 'nx': n, 'ny': n, 'seed': 77, 'kw': {'PBC': True},
+            'energies': [{'type': 'dipolar', 'cutoff': 8 * a}, {'type': 'zeeman', 'B': 1e-3, 'angle': 0.0}],
+            'params': {'UPDATE_SCHEME': 'Metropolis', 'MULTISAMPLING_SCHEME': 'Poisson'}}
+    fx = {'T': 300.0, 'E_B': 5e-20 * np.ones((n, n)), 'm0': g.integers(0, 2, size=(n, n)) * 2 - 1}
+    mo = build_oracle('poisson', spec=spec, fx=fx)
+    mp = build_product('poisson', spec=spec, fx=fx)
+    kw = {'r': 6 * a}
+    near, total = 0, 0
+    for s in range(40):
+        idx, p, u, dt = metropolis_decision(mo, **kw)
+        total += idx.shape[1]
+        if idx.shape[1] > 1:
+            d = np.abs(idx[:, :, None] - idx[:, None, :]).astype(float)
+            d = np.minimum(d, n - d)
+            d2 = (d ** 2).sum(0) + np.eye(idx.shape[1]) * 1e9
+            assert np.sqrt(d2.min()) > 6 + 1 - np.sqrt(2)
+        sw = mp.update(**kw)
+        got = {(int(a_), int(b_)) for a_, b_ in zip(sw[0], sw[1])}
+        acc_dev = np.array([(int(a_), int(b_)) in got for a_, b_ in zip(idx[0], idx[1])])
+        assert len(got) == int(acc_dev.sum()), f'step {s}: device switched a cell that was not a candidate'
+        diff = np.nonzero(acc_dev != (u < p))[0]
+        if diff.size:
+            Emax = np.max(np.abs(mo.E))
+            beta = mo.beta[idx[0], idx[1]]
+            band = p * beta * 2 * 2 * E_TOL * Emax * 1.01 + 1e-12
+            assert np.all(np.abs(u - p)[diff] <= band[diff]), f'step {s}: acceptance differs beyond tolerance'
+            near += diff.size
+        force_metropolis(mo, idx, acc_dev, dt)
+        assert mp._read_counters()['rng_call'] == mo.rng.call, f'step {s}: RNG call count diverged'
+    assert total > 40
+    assert mp.attempted_switches == mo.attempted_switches
+    assert mp.switches == mo.switches
+    assert np.array_equal(_np(mp.m), mo.m)
+    assert rel_err(_np(mp.E), mo.E) < 2 * E_TOL
+    print(f'poisson: 40 steps, {total} candidates, {near} near-threshold acceptances')

@@ -102,3 +102,33 @@ def test_hexagon_known_answer():
             mm = OracleMagnets(g, m_ref, T=300, moment=mom, energies=[dd], m_perp_factor=0)
             assert np.allclose(dd.E[m_ref.astype(bool)], E_th)
             assert rel_err(dd.E, E_ref) < 1e-12
+
+
+def test_poisson_reference_is_degenerate():
+    """The reference's _select_Poisson passes metres into a cell-unit routine
+    (hotspice/core.py:564 -> hotspice/poisson.py:77,99) and so always returns magnet (0,0);
+    the oracle's compatibility mode reproduces the recorded selections."""
+    from oracle.geometry import oop_square
+    from oracle.hotspice_oracle import OracleDipolar, OracleMagnets
+    sel = load_fixture('poisson_reference')['selections']
+    mm = OracleMagnets(oop_square(200e-9, 16), np.ones((16, 16)), T=300, moment=1e-15, energies=[OracleDipolar()],
+                       params=dict(UPDATE_SCHEME='Metropolis', MULTISAMPLING_SCHEME='Poisson'), seed=5,
+                       poisson_compat=True)
+    for s in sel:
+        assert np.array_equal(mm.select(r=mm.calc_r(0.05)), s)
+
+
+@pytest.mark.parametrize('w,h,r', [(48, 48, 6.0), (64, 40, 3.5), (30, 30, 9.0)])
+def test_poisson_disc_cells_keeps_its_distance(w, h, r):
+    """Cell-unit dart throwing (hotspice/poisson.py:72-128): every pair of accepted points is
+    farther apart than r + 1 under the periodic metric, and the background grid is covered
+    (no empty 2(r+1) x 2(r+1) window at the far side of the range)."""
+    from oracle.hotspice_oracle import poisson_disc_cells
+    for seed in range(3):
+        s = PhiloxStream(100 + seed)
+        pts = np.asarray(poisson_disc_cells(w, h, r, 4, s.random), dtype=float)
+        assert len(pts) >= max(1, int(0.3 * w * h / (np.pi * (r + 1) ** 2)))
+        d = np.abs(pts[:, None, :] - pts[None, :, :])
+        d = np.minimum(d, np.array([w, h]) - d)
+        d2 = (d ** 2).sum(-1) + np.eye(len(pts)) * 1e9
+        assert d2.min() > (r + 1) ** 2
