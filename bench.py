@@ -400,7 +400,8 @@ def run_product(args):
         "plain": {"value": plain_value, "unit": UNIT, "instances": plain_n, "steps_each": args.plain_steps,
                   "form": "Magnets.update() per step, one instance at a time", "batched_over_plain": value / plain_value},
         "gpu_launches": args.steps,
-        "roofline": {"bound": "hbm", "kernel": "engine_kernel<1>", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": "engine_kernel<CS> (all cluster-size groups of one bench step)",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "traffic": profile_traffic(), "launch_ms": launch_ms, "algorithmic_bytes_per_launch": alg},
         "clocks": sampler.summary(),

@@ -740,11 +740,17 @@ class Magnets(ABC):
 
     def _igemm_ok(self, d) -> bool:
         """The implicit GEMM covers the full uncropped kernel and a uniform moment."""
+        key = (self._version, id(d), id(d.kernel_set))
+        hit = getattr(self, '_igemm_ok_cache', None)
+        if hit is not None and hit[0] == key:
+            return hit[1]
         ks = d.kernel_set
-        if not (ks.wx == self.nx - 1 and ks.wy == self.ny - 1 and not ks.wrap):
-            return False
-        mom = self._moment_np[self.occupation.astype(bool)]
-        return mom.size == 0 or bool(np.all(mom == mom.flat[0]))
+        ok = ks.wx == self.nx - 1 and ks.wy == self.ny - 1 and not ks.wrap
+        if ok:
+            mom = self._moment_np[self.occupation.astype(bool)]
+            ok = mom.size == 0 or bool(np.all(mom == mom.flat[0]))
+        self._igemm_ok_cache = (key, ok)
+        return ok
 
     def _dipolar_apply(self, d, indices2D, semantics):
         idx = np.asarray(indices2D, dtype=np.int64).reshape(2, -1)
