@@ -28,7 +28,11 @@ namespace cg = cooperative_groups;
 
 namespace {
 
-constexpr int ENG_NT = 512;     // threads per CTA
+#ifndef HS_ENGINE_THREADS
+#define HS_ENGINE_THREADS 512
+#endif
+constexpr int ENG_NT = HS_ENGINE_THREADS;   // threads per CTA
+constexpr int ENG_MIN_CTAS = ENG_NT <= 256 ? 2 : 1;  // resident CTAs per SM the registers are budgeted for
 constexpr int ENG_SWCAP = 512;  // switches staged per CTA in shared memory
 
 struct SwX {                    // staged switch with its window footprint
@@ -323,7 +327,7 @@ HS_DEV WolffScratch wolff_scratch_of(const HsLattice &L, void *base) {
 }
 
 template <int CS>
-__global__ void __launch_bounds__(ENG_NT, 1) engine_kernel(const HsInstance *insts, int n_inst, int *work) {
+__global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsInstance *insts, int n_inst, int *work) {
     __shared__ int s_inst, s_go;
     __shared__ HsKeyIdx s_part[16];
     __shared__ HsKeyIdx s_red[32];

@@ -707,23 +707,43 @@ HS_DEV void hs_barriers_from(const HsLattice &L, double E, double Ep, double EB,
     }
 }
 
-// Néel log-domain keys (see hs_neel.cu) of cells start, start + stride, ... < N, folded into
-// `best`. The loads of NEEL_UNR cells are issued before any of them is used, so that one
-// thread keeps several L2 round trips in flight; the (key, index) minimum does not depend on
-// the visiting order.
-constexpr int NEEL_UNR = 4;
-HS_DEV HsKeyIdx neel_scan_range(const HsLattice &L, int64_t start, int64_t stride, int64_t N, uint64_t call,
+// Néel log-domain keys (see hs_neel.cu) of the occupied cells, folded into `best`. The work
+// is the occupied cells start, start + stride, ... : taken from the occupied-cell list when the
+// lattice is sparse (fewer than 3/4 of its cells hold a magnet), else all cells with an
+// occupation test. The loads of NEEL_UNR cells are issued before any of them is used, so that
+// one thread keeps several L2 round trips in flight. A cell whose key cannot beat the thread's
+// best so far is skipped before the accurate logarithms: log E1 >= log u (E1 = -log(1 - u) >= u)
+// and the two-channel term is >= -ln 2, so log u + (b_low - b_min) beta - ln 2 (less a margin
+// for the fast logarithm) is a lower bound of the key. The (key, index) minimum does not depend
+// on the visiting order or on the skipping (ties go to the smaller index; only cells whose key
+// is strictly larger than a key already seen are skipped).
+#ifndef HS_NEEL_UNROLL
+#define HS_NEEL_UNROLL 4
+#endif
+constexpr int NEEL_UNR = HS_NEEL_UNROLL;
+HS_DEV HsKeyIdx neel_scan_range(const HsLattice &L, int64_t start64, int64_t stride64, int64_t N64, uint64_t call,
                                 double bmin, HsKeyIdx best) {
     const bool two = L.use_perp != 0;
-    for (int64_t base = start; base < N; base += stride * NEEL_UNR) {
+    const bool sparse = 4 * (int64_t)L.n_occ < 3 * N64;
+    const int M = sparse ? L.n_occ : (int)N64;     // cell indices fit in int (HsKeyIdx.idx)
+    const int start = (int)start64, stride = (int)stride64;
+    const double slack = (two ? 0.6931471805599453 : 0.0) + 1e-4;
+    for (int base = start; base < M; base += stride * NEEL_UNR) {
+        int ci[NEEL_UNR];
         int8_t oc[NEEL_UNR], mv[NEEL_UNR];
         double ed[NEEL_UNR], edp[NEEL_UNR];
         float zf[NEEL_UNR], zfp[NEEL_UNR], eb[NEEL_UNR], bt[NEEL_UNR];
 #pragma unroll
         for (int k = 0; k < NEEL_UNR; ++k) {
-            const int64_t i = base + k * stride;
-            const bool v = i < N;
-            oc[k] = v ? L.occ[i] : (int8_t)0;
+            const int j = base + k * stride;
+            const bool v = j < M;
+            ci[k] = v ? (sparse ? __ldg(L.nonzero + j) : j) : 0;
+        }
+#pragma unroll
+        for (int k = 0; k < NEEL_UNR; ++k) {
+            const bool v = base + k * stride < M;
+            const int i = ci[k];
+            oc[k] = v ? (sparse ? (int8_t)1 : L.occ[i]) : (int8_t)0;
             mv[k] = v ? __ldcg(L.m + i) : (int8_t)0;
             ed[k] = (v && L.has_dipolar) ? __ldcg(L.E_dip + i) : 0.0;
             edp[k] = (v && L.has_dipolar && two) ? __ldcg(L.E_dip_perp + i) : 0.0;
@@ -732,29 +752,38 @@ HS_DEV HsKeyIdx neel_scan_range(const HsLattice &L, int64_t start, int64_t strid
             eb[k] = v ? __ldg(L.E_B + i) : 0.f;
             bt[k] = (v && L.beta_uniform <= 0.0) ? __ldg(L.beta + i) : 0.f;
         }
+        // branch-free phases, so the NEEL_UNR Philox chains and barrier evaluations interleave
+        double u[NEEL_UNR], lb[NEEL_UNR], b1v[NEEL_UNR], b2v[NEEL_UNR], btv[NEEL_UNR];
+#pragma unroll
+        for (int k = 0; k < NEEL_UNR; ++k) u[k] = hs_u53(L.seed, call, (uint32_t)ci[k]);
 #pragma unroll
         for (int k = 0; k < NEEL_UNR; ++k) {
-            if (!oc[k]) continue;
-            const int64_t i = base + k * stride;
             double E = ed[k], Ep = edp[k];
             if (L.zee) { E += (double)mv[k] * (double)zf[k]; if (two) Ep += (double)mv[k] * (double)zfp[k]; }
             if (L.has_exchange) {
                 double e, ep;
-                hs_exchange_at(L, (int)(i / L.nx), (int)(i % L.nx), e, ep);
+                hs_exchange_at(L, ci[k] / L.nx, ci[k] % L.nx, e, ep);
                 E += e;
                 if (two) Ep += ep;
             }
-            double b1, b2;
-            hs_barriers_from(L, E, Ep, (double)eb[k], b1, b2);
-            const double beta = L.beta_uniform > 0.0 ? L.beta_uniform : (double)bt[k];
-            const double le1 = (double)hs_log_exp1_f32(hs_u53(L.seed, call, (uint32_t)i));
+            hs_barriers_from(L, E, Ep, (double)eb[k], b1v[k], b2v[k]);
+            btv[k] = L.beta_uniform > 0.0 ? L.beta_uniform : (double)bt[k];
+            const double bm = two ? fmin(b1v[k], b2v[k]) : b1v[k];
+            lb[k] = (double)__logf((float)u[k]) + (bm - bmin) * btv[k] - slack;
+        }
+#pragma unroll
+        for (int k = 0; k < NEEL_UNR; ++k) {
+            if (!oc[k]) continue;
+            if (best.idx >= 0 && lb[k] > best.key) continue;
+            const double b1 = b1v[k], b2 = b2v[k], beta = btv[k];
+            const double le1 = (double)hs_log_exp1_f32(u[k]);
             double key;
             if (!two) key = le1 + (b1 - bmin) * beta;
             else {
                 const double bm = fmin(b1, b2), dd = fabs(b1 - b2);
                 key = le1 + (bm - bmin) * beta - (double)log1pf(expf((float)(-dd * beta)));
             }
-            best = hs_kmin(best, HsKeyIdx{key, (int)i});
+            best = hs_kmin(best, HsKeyIdx{key, ci[k]});
         }
     }
     return best;

@@ -47,41 +47,95 @@ def _bind():
     return lib
 
 
-def cluster_size_for(mm: Magnets) -> int:
-    """Cost model: enough CTAs that one step's scan / update work (cells times window)
-    is spread thin, but no more (cluster barriers cost more with more CTAs)."""
+def step_model(mm: Magnets) -> tuple[float, float, bool]:
+    """Device time of one step on one SM, as (serial us, divisible us, divides over the
+    cluster). Calibrated on B200 with single instances (bench lattices, n = 32..256): a Néel
+    step costs about 8.5 us plus 2.3 ns per cell (3.0 ns with the perpendicular channel) plus
+    about 1 ns per window cell of the update, and the per-cell part spreads over the cluster's
+    CTAs; a Metropolis step about 5 us plus a little per cell and window cell (its selection
+    runs on one CTA); a Wolff step grows its cluster on one CTA."""
     n = mm.nx * mm.ny
     d = mm._dipolar()
-    win = 0
-    if d is not None:
-        ks = d.kernel_set
-        win = (2 * ks.wx + 1) * (2 * ks.wy + 1)
-    if mm.params.UPDATE_SCHEME == Scheme.NEEL:
-        work = n + win
-    elif mm.params.UPDATE_SCHEME == Scheme.WOLFF:
-        return 1
-    else:
-        work = win * 8
-    if work <= 16384:
-        return 1
-    if work <= 65536:
-        return 2
-    if work <= 262144:
-        return 4
-    if work <= 1048576:
-        return 8
-    return 16
+    win = (2 * d.kernel_set.wx + 1) * (2 * d.kernel_set.wy + 1) if d is not None else 9
+    sch = mm.params.UPDATE_SCHEME
+    if sch == Scheme.NEEL:
+        per = 0.0030 if mm.USE_PERP_ENERGY else 0.0023
+        return 8.5, per * n + 0.001 * win, True
+    if sch == Scheme.WOLFF:
+        return 5.0, 0.002 * n, False
+    return 5.0, 0.0001 * n + 0.0005 * win, True
+
+
+def step_time(mm: Magnets, cs: int = 1) -> float:
+    """Modelled device time (us) of one step of ``mm`` on a cluster of ``cs`` CTAs."""
+    s0, p, divides = step_model(mm)
+    if not divides:
+        return s0 + p
+    return s0 + p / cs + 0.25 * (cs - 1)
 
 
 def step_cost(mm: Magnets) -> float:
-    """Relative cost of one update step (cells scanned or window cells updated)."""
-    d = mm._dipolar()
-    win = (2 * d.kernel_set.wx + 1) * (2 * d.kernel_set.wy + 1) if d is not None else 9
-    if mm.params.UPDATE_SCHEME == Scheme.NEEL:
-        return mm.nx * mm.ny + win
-    if mm.params.UPDATE_SCHEME == Scheme.WOLFF:
-        return mm.nx * mm.ny
-    return 2048 + 2 * win
+    """Cost of one update step in SM-microseconds (the model on one CTA)."""
+    return step_time(mm, 1)
+
+
+def cluster_size_for(mm: Magnets) -> int:
+    """Cluster size for an instance run alone: double the CTAs while that cuts the modelled
+    step time by at least 25%."""
+    cs = 1
+    while cs < 16 and step_time(mm, 2 * cs) < 0.75 * step_time(mm, cs):
+        cs *= 2
+    return cs
+
+
+def lpt_makespan(durations, n_workers):
+    """Makespan of longest-processing-time-first list scheduling of ``durations`` on
+    ``n_workers`` identical workers (what the engine's work counter does with instances
+    sorted longest first)."""
+    import heapq
+    if n_workers <= 0:
+        return math.inf
+    heap = [0.0] * min(n_workers, max(1, len(durations)))
+    for d in sorted(durations, reverse=True):
+        t = heapq.heappop(heap)
+        heapq.heappush(heap, t + d)
+    return max(heap)
+
+
+def plan_uniform_size(models, steps, n_sm, sizes=CLUSTER_SIZES):
+    """One cluster size for a whole launch: the size whose longest-first schedule of the
+    modelled run times over the clusters that fit (SM count / size) finishes first. One
+    size per launch keeps clusters of different shapes from fragmenting the GPCs."""
+    def t(m, cs):
+        s0, p, dv = m
+        return s0 + p if not dv else s0 + p / cs + 0.25 * (cs - 1)
+    best, best_t = 1, math.inf
+    for cs in sizes:
+        mk = lpt_makespan([st * t(m, cs) for m, st in zip(models, steps)], n_sm // cs)
+        if mk < best_t * 0.97:
+            best, best_t = cs, mk
+    return best
+
+
+def plan_sizes(models, steps, n_sm, max_cs=16):
+    """Cluster sizes for a batch: start every instance on one CTA; an instance whose run is
+    longer than the even share of the GPU (total SM time / SM count) gets twice the CTAs
+    while that shortens it by at least 20%, until no run exceeds the share (or max_cs).
+    ``models``: (serial us, divisible us, divides) per instance, as step_model gives."""
+    def t(m, cs):
+        s0, p, dv = m
+        return s0 + p if not dv else s0 + p / cs + 0.25 * (cs - 1)
+    cs = [1] * len(models)
+    for _ in range(5):
+        share = sum(st * t(m, c) * c for m, st, c in zip(models, steps, cs)) / n_sm
+        changed = False
+        for i, (m, st) in enumerate(zip(models, steps)):
+            while cs[i] < max_cs and m[2] and st * t(m, cs[i]) > share and t(m, 2 * cs[i]) < 0.8 * t(m, cs[i]):
+                cs[i] *= 2
+                changed = True
+        if not changed:
+            break
+    return cs
 
 
 @dataclass
@@ -97,8 +151,9 @@ class BatchEngine:
     ``progress(t_max, MCsteps_max)`` (the reference's stop rule, per instance)."""
 
     def __init__(self, magnets, cluster_size: int | None = None, device=None, throughput: bool | None = None):
-        """``throughput``: give every instance a single-CTA cluster (best aggregate throughput when
-        there are at least as many instances as SMs); default: on when len(magnets) >= SM count."""
+        """``throughput``: plan one cluster size for the launch from the modelled run times
+        (:func:`plan_uniform_size`); default on when there is more than one instance, otherwise
+        the instance's own size (:func:`cluster_size_for` or its autotuned choice)."""
         self.magnets = list(magnets)
         if not self.magnets:
             raise ValueError('BatchEngine needs at least one Magnets instance')
@@ -108,7 +163,7 @@ class BatchEngine:
                 raise ValueError('all instances of a BatchEngine must live on the same device')
         self.cluster_size = cluster_size
         if throughput is None:
-            throughput = len(self.magnets) >= torch.cuda.get_device_properties(self.device).multi_processor_count
+            throughput = len(self.magnets) > 1
         self.throughput = throughput
         self._cache = None
         self._streams = []
@@ -166,19 +221,11 @@ class BatchEngine:
         return I, [buf, s]
 
     def _throughput_sizes(self, steps):
-        """Cluster sizes for throughput mode: an instance whose step budget costs more than an
-        even share of the GPU (total cost / SM count) gets enough CTAs to finish in about that
-        share, so one large lattice does not leave the rest of the GPU idle at the end."""
+        """Cluster sizes for throughput mode: one size for the launch (:func:`plan_uniform_size`
+        over the modelled step times)."""
         n_sm = torch.cuda.get_device_properties(self.device).multi_processor_count
-        costs = [max(1, st) * step_cost(mm) for mm, st in zip(self.magnets, steps)]
-        share = sum(costs) / n_sm
-        out = []
-        for c in costs:
-            cs = 1
-            while cs < 16 and c / cs > share:
-                cs *= 2
-            out.append(cs)
-        return out
+        cs = plan_uniform_size([step_model(mm) for mm in self.magnets], [max(1, st) for st in steps], n_sm)
+        return [cs] * len(self.magnets)
 
     def _prepare(self, steps, kws, sizes=None):
         groups = {}
@@ -193,9 +240,12 @@ class BatchEngine:
                 raise ValueError(f'cluster size {cs} not in {CLUSTER_SIZES}')
             I, k = self._describe_cached(mm, st, kw)
             keep += k
-            groups.setdefault(cs, []).append(I)
+            groups.setdefault(cs, []).append((st * step_time(mm, cs), j, I))
         out = []
-        for cs, lst in sorted(groups.items()):
+        # largest clusters first (launched first, so the longest runs start first), and inside a
+        # group the longest runs first on the work counter (longest-processing-time order)
+        for cs, lst in sorted(groups.items(), reverse=True):
+            lst = [I for _, _, I in sorted(lst, key=lambda e: (-e[0], e[1]))]
             arr = (HsInstance * len(lst))(*lst)
             raw = np.frombuffer(bytes(arr), dtype=np.uint8)
             # pinned staging + asynchronous copy on the current stream: no host synchronisation

@@ -6,7 +6,8 @@ estimate) and instance slots allow, keeps every admitted Magnets state resident 
 and advances all admitted instances together in *rounds*: one persistent engine launch
 (``hs_engine_run``, hotspice_b200/csrc/hs_engine.cu) per round, in which every instance runs a
 quantum of steps sized so that each gets about the same device time (processor sharing
-between the requests on the GPU). Requests that arrive while a round runs are built on the
+between the requests on the GPU), with cluster sizes planned from each request's remaining
+work. Requests that arrive while a round runs are built on the
 host and admitted into the next round, which is queued on the device behind the running one,
 so their work overlaps with the requests already there. A request retires when its step
 budget is done; its result and completion latency are recorded at that round's end.
@@ -16,7 +17,8 @@ Results do not depend on the mix: each instance draws its variates from its own 
 per-instance step sequence however the steps are cut into rounds and whichever cluster size
 runs them, so a request gives the same final state alone and in any mix.
 
-The scheduling policy (:class:`AdmissionQueue`, :func:`plan_quanta`, :func:`shard_requests`)
+The scheduling policy (:class:`AdmissionQueue`, :func:`plan_quanta`, :func:`shard_requests`,
+and the engine's :func:`~hotspice_b200.engine.plan_sizes`)
 is plain host code; the reference has no serving layer (its experiments call
 ``Magnets.progress`` in a loop, hotspice/core.py:736-760, one simulation at a time).
 """
@@ -29,7 +31,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .engine import step_cost
+from .engine import plan_sizes, step_model, step_time
 
 LATTICE_GEOMETRY = {
     # lattice: (a, moment) of the sweep's instances
@@ -183,30 +185,13 @@ class AdmissionQueue:
         return out
 
 
-def plan_cluster_sizes(remaining_costs, n_sm, sizes=(1, 2, 4, 8, 16)):
-    """CTAs per instance for the next round: an instance whose remaining work exceeds an even
-    share of the GPU (total remaining work / SM count) gets enough CTAs (a power of two, at
-    most 16) to finish in about that share, so large requests do not hold the tail."""
-    share = max(sum(remaining_costs) / max(n_sm, 1), 1.0)
-    out = []
-    for c in remaining_costs:
-        cs = sizes[0]
-        for s in sizes:
-            cs = s
-            if c / s <= share:
-                break
-        out.append(cs)
-    return out
-
-
-def plan_quanta(costs, remaining, quantum_cost, sizes=None):
-    """Steps each active instance runs in the next round: about ``quantum_cost`` cost units
-    per CTA of its cluster (the per-step cost of :func:`hotspice_b200.engine.step_cost`), at
+def plan_quanta(times, remaining, round_us):
+    """Steps each active instance runs in the next round: about ``round_us`` of modelled
+    device time (``times``: modelled time of one step of each instance on its cluster), at
     least one step, at most what remains of its budget."""
-    sizes = sizes or [1] * len(costs)
     out = []
-    for c, r, cs in zip(costs, remaining, sizes):
-        q = max(1, int(quantum_cost * cs // max(c, 1)))
+    for t, r in zip(times, remaining):
+        q = max(1, int(round_us // max(t, 1e-9)))
         out.append(int(min(q, r)))
     return out
 
@@ -232,7 +217,7 @@ class _Active:
     req: SimRequest
     mm: object
     remaining: int
-    cost: float
+    model: tuple
     admitted: float
     bytes: int
     event: object = None         # build finished (stream event)
@@ -253,7 +238,8 @@ class Server:
 
     ``hbm_budget``: device bytes the resident instances may hold (default: half of the free
     memory when the server starts); ``max_slots``: resident instances at most; ``round_ms``:
-    device time one instance's quantum aims at; ``keep_state``: return the final spins."""
+    device time one instance's quantum aims at (from the engine's step-time model, corrected
+    by the measured speed of past rounds); ``keep_state``: return the final spins."""
 
     def __init__(self, device=None, hbm_budget=None, max_slots=4096, round_ms=5.0, keep_state=False,
                  max_inflight=2):
@@ -270,7 +256,7 @@ class Server:
         self.keep_state = keep_state
         self.max_inflight = max(1, int(max_inflight))
         self.n_sm = torch.cuda.get_device_properties(self.device).multi_processor_count
-        self.sm_rate = 1.5e8          # cost units per second per SM; refined from measured rounds
+        self.speed = 1.0              # modelled device-us per measured us; refined from measured rounds
         self.stream = torch.cuda.Stream(self.device)
         self.build_stream = torch.cuda.Stream(self.device)
         self.stats = ServeStats()
@@ -279,9 +265,9 @@ class Server:
     # -- one round ---------------------------------------------------------------------
     def _launch_round(self, active: list[_Active]):
         torch = self.torch
-        quantum = self.sm_rate * self.round_ms * 1e-3
-        sizes = plan_cluster_sizes([a.cost * a.remaining for a in active], self.n_sm)
-        steps = plan_quanta([a.cost for a in active], [a.remaining for a in active], quantum, sizes)
+        sizes = plan_sizes([a.model for a in active], [a.remaining for a in active], self.n_sm)
+        times = [step_time(a.mm, c) for a, c in zip(active, sizes)]
+        steps = plan_quanta(times, [a.remaining for a in active], self.speed * self.round_ms * 1e3)
         if self._engine is None:
             from .engine import BatchEngine
             self._engine = BatchEngine([a.mm for a in active], device=self.device, throughput=True)
@@ -300,8 +286,8 @@ class Server:
             e1.record(self.stream)
         for a, s in zip(active, steps):
             a.remaining -= s
-        cost = sum(s * a.cost for a, s in zip(active, steps))
-        return dict(prepared=prepared, e0=e0, e1=e1, members=list(active), steps=steps, cost=cost,
+        sm_us = sum(s * t * c for s, t, c in zip(steps, times, sizes))
+        return dict(prepared=prepared, e0=e0, e1=e1, members=list(active), steps=steps, sm_us=sm_us,
                     ctas=sum(sizes))
 
     def _retire(self, a: _Active, now: float, t0: float) -> SimResult:
@@ -349,7 +335,7 @@ class Server:
                     ev = torch.cuda.Event()
                     ev.record(self.build_stream)
                 b = footprint_bytes(r.spec)
-                active.append(_Active(r, mm, int(r.steps), float(step_cost(mm)), time.perf_counter(), b, ev))
+                active.append(_Active(r, mm, int(r.steps), step_model(mm), time.perf_counter(), b, ev))
             used_bytes = sum(a.bytes for a in active)
             st.admitted_bytes_peak = max(st.admitted_bytes_peak, used_bytes)
             return bool(new)
@@ -373,8 +359,8 @@ class Server:
                 ms = rd['e0'].elapsed_time(rd['e1'])
                 if ms > 0.05:
                     busy = max(1, min(self.n_sm, rd['ctas']))
-                    rate = rd['cost'] / (ms * 1e-3) / busy
-                    self.sm_rate = 0.5 * self.sm_rate + 0.5 * rate
+                    speed = rd['sm_us'] / (ms * 1e3) / busy
+                    self.speed = min(4.0, max(0.25, 0.5 * self.speed + 0.5 * speed))
                 st.history.append((clock(), len(rd['members']), ms))
                 now = time.perf_counter()
                 done_ids = set()

@@ -65,18 +65,23 @@ def test_admission_bypass_is_bounded():
 
 
 def test_plan_quanta():
-    steps = S.plan_quanta([100.0, 1000.0, 1e6], [50, 1000, 7], quantum_cost=10000.0)
+    steps = S.plan_quanta([10.0, 100.0, 1e4], [50, 1000, 7], round_us=1000.0)
     assert steps == [50, 10, 1]                    # capped by what remains; at least one step
-    steps = S.plan_quanta([1000.0, 1000.0], [10**6, 10**6], quantum_cost=10000.0, sizes=[1, 8])
-    assert steps == [10, 80]                       # per CTA of the instance's cluster
 
 
-def test_plan_cluster_sizes():
-    # one request holds almost all the remaining work: it gets the largest cluster
-    assert S.plan_cluster_sizes([1e9, 1e3, 1e3], n_sm=148) == [16, 1, 1]
-    # many equal requests: one CTA each
-    assert S.plan_cluster_sizes([1e6] * 300, n_sm=148) == [1] * 300
-    assert S.plan_cluster_sizes([4e6, 1e6, 1e6], n_sm=4) == [4, 1, 1]
+def test_plan_sizes():
+    from hotspice_b200.engine import plan_sizes
+    neel_big = (8.5, 150.0, True)                   # ~65k-cell Néel lattice
+    neel_small = (8.5, 2.0, True)
+    wolff = (5.0, 100.0, False)                     # grows on one CTA: never widened
+    # one long run among short ones gets a wide cluster; short runs stay on one CTA
+    cs = plan_sizes([neel_big] + [neel_small] * 200, [1000] + [100] * 200, n_sm=148)
+    assert cs[0] >= 8 and set(cs[1:]) == {1}
+    assert plan_sizes([wolff] * 3, [10**6] * 3, n_sm=148) == [1, 1, 1]
+    # many equal runs that fill the GPU: one CTA each
+    assert plan_sizes([neel_big] * 300, [100] * 300, n_sm=148) == [1] * 300
+    # widening stops when it no longer shortens the run by 20%
+    assert plan_sizes([(8.5, 4.0, True)], [10**6], n_sm=148) == [1]
 
 
 def test_fifo_latencies():
