@@ -153,7 +153,7 @@ HS_DEV bool covers_seg(const HsLattice &L, const SwX &w, int row, int seg128) {
 // by the item of the first switch covering it, which accumulates every covering switch in
 // list order.
 HS_DEV void update_items(const HsLattice &L, const SwX *s_sw, const int *s_pre, int n, int semantics, int gw, int nw,
-                         const HsSwitchList &sw, int nsw_total) {
+                         const HsSwitchList &sw, int nsw_total, float *cache = nullptr) {
     if (n == 0) return;
     const int lane = threadIdx.x & 31;
     const float pref2 = (float)(2.0 * L.dip_pref);
@@ -243,6 +243,19 @@ HS_DEV void update_items(const HsLattice &L, const SwX *s_sw, const int *s_pre, 
                         for (int v = 0; v < 4 && x0 + v < L.nx; ++v) {
                             L.E_dip[i + v] = ev[v];
                             if (L.use_perp) L.E_dip_perp[i + v] = pv[v];
+                        }
+                    }
+                    if (cache) {  // refresh the Néel barrier cache of the cells just written
+                        const bool two = L.use_perp != 0;
+                        for (int v = 0; v < 4 && x0 + v < L.nx; ++v) {
+                            float c = INFINITY;
+                            if (L.occ[i + v]) {
+                                const double m = (double)__ldcg(L.m + i + v);
+                                double E = ev[v], Ep = pv[v];
+                                if (L.zee) { E += m * (double)__ldg(L.zee + i + v); if (two) Ep += m * (double)__ldg(L.zee_perp + i + v); }
+                                c = neel_cache_value(L, E, two ? Ep : 0.0, (double)__ldg(L.E_B + i + v));
+                            }
+                            cache[i + v] = c;
                         }
                     }
                 }
@@ -407,7 +420,12 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
                     Sync<CS>::all();
                 }
                 const bool two = L.use_perp != 0;
-                HsKeyIdx best = neel_scan_range(L, gt, gs, N, call, bmin, HsKeyIdx{0.0, -1});
+                // barrier cache: uniform beta, no exchange (its neighbours change outside the window)
+                float *cache = (unif && !L.has_exchange && I.scratch_bytes >= HS_NEEL_CACHE_OFFSET + 4 * N)
+                                   ? reinterpret_cast<float *>(reinterpret_cast<char *>(I.scratch) + HS_NEEL_CACHE_OFFSET)
+                                   : nullptr;
+                HsKeyIdx best = (cache && st > 0) ? neel_scan_cached(L, cache, gt, gs, N, call, HsKeyIdx{0.0, -1})
+                                                  : neel_scan_range(L, gt, gs, N, call, bmin, HsKeyIdx{0.0, -1}, cache);
                 best = eng_block_kmin(best, s_red);
                 if (threadIdx.x == 0) {
                     if constexpr (CS == 1) s_part[0] = best;
@@ -418,12 +436,19 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
                     HsKeyIdx w{0.0, -1};
                     for (int r = 0; r < CS; ++r) w = hs_kmin(w, s_part[r]);
                     neel_finalize(L, C, sw, w, call, bmin, unif, two, I.attempt_freq);
+                    if (cache && !L.has_dipolar && C->n_sw > 0) {  // no window update: refresh the flipped cell
+                        const int64_t i = w.idx;
+                        const double m = (double)L.m[i];
+                        double E = 0.0, Ep = 0.0;
+                        if (L.zee) { E = m * (double)L.zee[i]; if (two) Ep = m * (double)L.zee_perp[i]; }
+                        cache[i] = neel_cache_value(L, E, Ep, (double)L.E_B[i]);
+                    }
                 }
                 Sync<CS>::all();
                 if (L.has_dipolar) {
                     const int nsw = __ldcg(&C->n_sw);
                     const int n = stage_switches(L, sw, nsw, s_sw, s_pre);
-                    update_items(L, s_sw, s_pre, n, HS_UPDATE_SINGLE, rank * nwarps + warp, CS * nwarps, sw, nsw);
+                    update_items(L, s_sw, s_pre, n, HS_UPDATE_SINGLE, rank * nwarps + warp, CS * nwarps, sw, nsw, cache);
                 }
                 Sync<CS>::all();
             } else {  // Wolff

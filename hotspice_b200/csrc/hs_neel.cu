@@ -125,7 +125,9 @@ neel_scan_kernel(HsLattice L, HsCounters *C, HsSwitchList sw, double attempt_fre
 
 }  // namespace
 
-int64_t hs_neel_scratch(const HsLattice &) { return (int64_t)sizeof(NeelScratch); }
+// The engine keeps its barrier cache (one float per cell) behind the step's own scratch.
+static_assert(sizeof(NeelScratch) <= HS_NEEL_CACHE_OFFSET, "Néel scratch overlaps the barrier cache");
+int64_t hs_neel_scratch(const HsLattice &L) { return HS_NEEL_CACHE_OFFSET + 4 * (int64_t)L.nx * L.ny; }
 
 int hs_launch_neel(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, double attempt_freq,
                    void *scratch, int64_t scratch_bytes, cudaStream_t st) {

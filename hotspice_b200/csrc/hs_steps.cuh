@@ -717,12 +717,22 @@ HS_DEV void hs_barriers_from(const HsLattice &L, double E, double Ep, double EB,
 // for the fast logarithm) is a lower bound of the key. The (key, index) minimum does not depend
 // on the visiting order or on the skipping (ties go to the smaller index; only cells whose key
 // is strictly larger than a key already seen are skipped).
+// Néel barrier cache (engine only): per cell s = b_low * beta (uniform beta), rounded down to
+// float, +inf for an empty cell. It lives in the Néel scratch at this offset and is valid only
+// inside one engine launch (built by the launch's first step, refreshed by the window update).
+constexpr int64_t HS_NEEL_CACHE_OFFSET = 32768;
+HS_DEV float neel_cache_value(const HsLattice &L, double E, double Ep, double EB) {
+    double b1, b2;
+    hs_barriers_from(L, E, Ep, EB, b1, b2);
+    return __double2float_rd(fmin(b1, b2) * L.beta_uniform);
+}
+
 #ifndef HS_NEEL_UNROLL
 #define HS_NEEL_UNROLL 4
 #endif
 constexpr int NEEL_UNR = HS_NEEL_UNROLL;
 HS_DEV HsKeyIdx neel_scan_range(const HsLattice &L, int64_t start64, int64_t stride64, int64_t N64, uint64_t call,
-                                double bmin, HsKeyIdx best) {
+                                double bmin, HsKeyIdx best, float *cache = nullptr) {
     const bool two = L.use_perp != 0;
     const bool sparse = 4 * (int64_t)L.n_occ < 3 * N64;
     const int M = sparse ? L.n_occ : (int)N64;     // cell indices fit in int (HsKeyIdx.idx)
@@ -770,6 +780,7 @@ HS_DEV HsKeyIdx neel_scan_range(const HsLattice &L, int64_t start64, int64_t str
             btv[k] = L.beta_uniform > 0.0 ? L.beta_uniform : (double)bt[k];
             const double bm = two ? fmin(b1v[k], b2v[k]) : b1v[k];
             lb[k] = (double)__logf((float)u[k]) + (bm - bmin) * btv[k] - slack;
+            if (cache && base + k * stride < M) cache[ci[k]] = oc[k] ? __double2float_rd(bm * btv[k]) : INFINITY;
         }
 #pragma unroll
         for (int k = 0; k < NEEL_UNR; ++k) {
@@ -784,6 +795,55 @@ HS_DEV HsKeyIdx neel_scan_range(const HsLattice &L, int64_t start64, int64_t str
                 key = le1 + (bm - bmin) * beta - (double)log1pf(expf((float)(-dd * beta)));
             }
             best = hs_kmin(best, HsKeyIdx{key, ci[k]});
+        }
+    }
+    return best;
+}
+
+// The same scan from the barrier cache (uniform beta, b_min = 0): per cell the cached
+// s = b_low beta, the Philox variate and the lower bound log u + s; the exact key (computed as
+// in neel_scan_range, from the energies) only for the cells the bound does not rule out.
+HS_DEV HsKeyIdx neel_scan_cached(const HsLattice &L, const float *cache, int64_t start64, int64_t stride64, int64_t N64,
+                                 uint64_t call, HsKeyIdx best) {
+    const bool two = L.use_perp != 0;
+    const bool sparse = 4 * (int64_t)L.n_occ < 3 * N64;
+    const int M = sparse ? L.n_occ : (int)N64;
+    const int start = (int)start64, stride = (int)stride64;
+    const double slack = (two ? 0.6931471805599453 : 0.0) + 1e-4;
+    const double beta = L.beta_uniform;
+    for (int base = start; base < M; base += stride * NEEL_UNR) {
+        int ci[NEEL_UNR];
+        float sc[NEEL_UNR];
+        double u[NEEL_UNR];
+#pragma unroll
+        for (int k = 0; k < NEEL_UNR; ++k) {
+            const int j = base + k * stride;
+            ci[k] = j < M ? (sparse ? __ldg(L.nonzero + j) : j) : 0;
+        }
+#pragma unroll
+        for (int k = 0; k < NEEL_UNR; ++k) sc[k] = base + k * stride < M ? __ldcg(cache + ci[k]) : INFINITY;
+#pragma unroll
+        for (int k = 0; k < NEEL_UNR; ++k) u[k] = hs_u53(L.seed, call, (uint32_t)ci[k]);
+#pragma unroll
+        for (int k = 0; k < NEEL_UNR; ++k) {
+            if (sc[k] == INFINITY) continue;
+            const double lbk = (double)__logf((float)u[k]) + (double)sc[k] - slack;
+            if (best.idx >= 0 && lbk > best.key) continue;
+            const int i = ci[k];
+            double E = L.has_dipolar ? __ldcg(L.E_dip + i) : 0.0;
+            double Ep = (L.has_dipolar && two) ? __ldcg(L.E_dip_perp + i) : 0.0;
+            const int mv = __ldcg(L.m + i);
+            if (L.zee) { E += (double)mv * (double)__ldg(L.zee + i); if (two) Ep += (double)mv * (double)__ldg(L.zee_perp + i); }
+            double b1, b2;
+            hs_barriers_from(L, E, Ep, (double)__ldg(L.E_B + i), b1, b2);
+            const double le1 = (double)hs_log_exp1_f32(u[k]);
+            double key;
+            if (!two) key = le1 + b1 * beta;
+            else {
+                const double bm = fmin(b1, b2), dd = fabs(b1 - b2);
+                key = le1 + bm * beta - (double)log1pf(expf((float)(-dd * beta)));
+            }
+            best = hs_kmin(best, HsKeyIdx{key, i});
         }
     }
     return best;
