@@ -153,7 +153,7 @@ HS_DEV bool covers_seg(const HsLattice &L, const SwX &w, int row, int seg128) {
 // by the item of the first switch covering it, which accumulates every covering switch in
 // list order.
 HS_DEV void update_items(const HsLattice &L, const SwX *s_sw, const int *s_pre, int n, int semantics, int gw, int nw,
-                         const HsSwitchList &sw, int nsw_total, float *cache = nullptr) {
+                         const HsSwitchList &sw, int nsw_total) {
     if (n == 0) return;
     const int lane = threadIdx.x & 31;
     const float pref2 = (float)(2.0 * L.dip_pref);
@@ -245,23 +245,91 @@ HS_DEV void update_items(const HsLattice &L, const SwX *s_sw, const int *s_pre, 
                             if (L.use_perp) L.E_dip_perp[i + v] = pv[v];
                         }
                     }
-                    if (cache) {  // refresh the Néel barrier cache of the cells just written
-                        const bool two = L.use_perp != 0;
-                        for (int v = 0; v < 4 && x0 + v < L.nx; ++v) {
-                            float c = INFINITY;
-                            if (L.occ[i + v]) {
-                                const double m = (double)__ldcg(L.m + i + v);
-                                double E = ev[v], Ep = pv[v];
-                                if (L.zee) { E += m * (double)__ldg(L.zee + i + v); if (two) Ep += m * (double)__ldg(L.zee_perp + i + v); }
-                                c = neel_cache_value(L, E, two ? Ep : 0.0, (double)__ldg(L.E_B + i + v));
-                            }
-                            cache[i + v] = c;
-                        }
-                    }
                 }
             }
         }
         it0 += nr;
+    }
+}
+
+// Window update of a single switch (the Néel step): every thread of the cluster takes window
+// cells directly (row-major over the window, consecutive threads on consecutive columns) and
+// issues the loads of its cells together; the barrier cache is refreshed in the same pass. Per
+// cell the arithmetic is that of update_items for one switch (acc = mm_s K, E += 2 pref mm_j acc
+// in the same float order, then E_s negated), so the energies are the same bit for bit; cells
+// outside the window receive nothing there either.
+HS_DEV void update_one(const HsLattice &L, int sy, int sx, float smm, int t0, int nt, float *cache) {
+    const int sub = hs_sub(L, sy, sx);
+    if (sub < 0) return;
+    int hy, wy, hx, wx;
+    hs_window(L, 0, true, hy, wy);
+    hs_window(L, 0, false, hx, wx);
+    int ylo, nrows, xlo, ncols;
+    if (wy) {
+        if (2 * hy + 1 >= L.ny) { ylo = 0; nrows = L.ny; } else { ylo = hs_wrap(sy - hy, L.ny); nrows = 2 * hy + 1; }
+    } else { ylo = max(0, sy - hy); nrows = min(L.ny - 1, sy + hy) - ylo + 1; }
+    if (wx) {
+        if (2 * hx + 1 >= L.nx) { xlo = 0; ncols = L.nx; } else { xlo = hs_wrap(sx - hx, L.nx); ncols = 2 * hx + 1; }
+    } else { xlo = max(0, sx - hx); ncols = min(L.nx - 1, sx + hx) - xlo + 1; }
+    const int total = nrows * ncols;
+    const float pref2 = (float)(2.0 * L.dip_pref);
+    const bool two = L.use_perp != 0;
+    constexpr int U = 4;
+    for (int base = t0; base < total; base += nt * U) {
+        int idx[U], rw[U], cl[U];
+        float kv[U], kp[U], mv[U], zf[U], zp[U], eb[U];
+        double ev[U], pv[U];
+        int8_t oc[U], ms[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            const int c = base + k * nt;
+            const int r = c < total ? c / ncols : 0, q = c < total ? c - r * ncols : 0;
+            int row = ylo + r, col = xlo + q;
+            if (row >= L.ny) row -= L.ny;
+            if (col >= L.nx) col -= L.nx;
+            rw[k] = row; cl[k] = col;
+            idx[k] = row * L.nx + col;
+        }
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            const bool v = base + k * nt < total;
+            const int i = idx[k];
+            kv[k] = v ? hs_kval(L, L.K, sub, rw[k] - sy, cl[k] - sx) : 0.f;
+            kp[k] = (v && two) ? hs_kval(L, L.Kpo, sub, rw[k] - sy, cl[k] - sx) : 0.f;
+            mv[k] = v ? __ldcg(L.mm + i) : 0.f;
+            ev[k] = v ? __ldcg(L.E_dip + i) : 0.0;
+            pv[k] = (v && two) ? __ldcg(L.E_dip_perp + i) : 0.0;
+            if (cache) {
+                oc[k] = v ? L.occ[i] : (int8_t)0;
+                ms[k] = v ? __ldcg(L.m + i) : (int8_t)0;
+                zf[k] = (v && L.zee) ? __ldg(L.zee + i) : 0.f;
+                zp[k] = (v && L.zee && two) ? __ldg(L.zee_perp + i) : 0.f;
+                eb[k] = v ? __ldg(L.E_B + i) : 0.f;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            if (base + k * nt >= total) continue;
+            const int i = idx[k];
+            float acc = 0.f, accp = 0.f;
+            acc += smm * kv[k];
+            if (two) accp += smm * kp[k];
+            double e = ev[k] + (double)(pref2 * (mv[k] * acc));
+            double p = pv[k] + (double)(pref2 * (mv[k] * accp));
+            if (rw[k] == sy && cl[k] == sx) { e = -e; p = -p; }
+            L.E_dip[i] = e;
+            if (two) L.E_dip_perp[i] = p;
+            if (cache) {
+                float c = INFINITY;
+                if (oc[k]) {
+                    const double m = (double)ms[k];
+                    double E = e, Ep = p;
+                    if (L.zee) { E += m * (double)zf[k]; if (two) Ep += m * (double)zp[k]; }
+                    c = neel_cache_value(L, E, two ? Ep : 0.0, (double)eb[k]);
+                }
+                cache[i] = c;
+            }
+        }
     }
 }
 
@@ -341,7 +409,11 @@ HS_DEV WolffScratch wolff_scratch_of(const HsLattice &L, void *base) {
 
 template <int CS>
 __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsInstance *insts, int n_inst, int *work) {
-    __shared__ int s_inst, s_go;
+    __shared__ int s_inst, s_go, s_n1, s_y1, s_x1, s_nsw;
+    __shared__ float s_mm1;
+    __shared__ unsigned long long s_call;
+    __shared__ __align__(16) HsCounters s_C;   // rank 0: the instance's counters for the whole run
+    static_assert(sizeof(HsCounters) % 8 == 0, "HsCounters is copied in 8-byte words");
     __shared__ HsKeyIdx s_part[16];
     __shared__ HsKeyIdx s_red[32];
     __shared__ double s_dred[32];
@@ -367,7 +439,17 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
         const HsLattice &L = s_I.L;
         const HsSwitchList &sw = s_I.sw;
         const HsGridPlan &P = s_I.P;
-        HsCounters *C = s_I.C;
+        // The counters live in rank 0's shared memory while the instance runs (every step reads
+        // and updates them) and go back to global memory when it stops; other CTAs receive the
+        // values they need (Philox call, switch count) through distributed shared memory.
+        HsCounters *const Cg = s_I.C;
+        HsCounters *const C = &s_C;
+        if (rank == 0) {
+            const unsigned long long *src = reinterpret_cast<const unsigned long long *>(Cg);
+            unsigned long long *dst = reinterpret_cast<unsigned long long *>(&s_C);
+            for (int k = threadIdx.x; k < (int)(sizeof(HsCounters) / 8); k += blockDim.x) dst[k] = __ldcg(src + k);
+        }
+        __syncthreads();
         const int scheme = s_I.scheme;
         for (int64_t st = 0;; ++st) {
             if (rank == 0 && threadIdx.x == 0) {
@@ -376,20 +458,25 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
                 else if (C->progress) { go = hs_progress_continue(C, L.n_occ); if (!go) { C->done = 1; C->n_sw = 0; } }
                 else go = st < I.steps;
                 Sync<CS>::publish(&s_go, go);
+                Sync<CS>::publish(&s_call, (unsigned long long)C->rng_call);
             }
             Sync<CS>::all();
             if (!s_go) break;
             if (scheme == HS_SCHEME_METROPOLIS) {
-                if (rank == 0) metro_step_cta(L, C, sw, P, metro_scratch_of(L, P, I.scratch));
+                if (rank == 0) {
+                    metro_step_cta(L, C, sw, P, metro_scratch_of(L, P, I.scratch));
+                    __syncthreads();
+                    if (threadIdx.x == 0) Sync<CS>::publish(&s_nsw, C->n_sw);
+                }
                 Sync<CS>::all();
                 if (L.has_dipolar) {
-                    const int nsw = __ldcg(&C->n_sw);
+                    const int nsw = s_nsw;
                     const int n = stage_switches(L, sw, nsw, s_sw, s_pre);
                     update_items(L, s_sw, s_pre, n, HS_UPDATE_MULTIPLE, rank * nwarps + warp, CS * nwarps, sw, nsw);
                 }
                 Sync<CS>::all();
             } else if (scheme == HS_SCHEME_NEEL) {
-                const uint64_t call = __ldcg(&C->rng_call);
+                const uint64_t call = s_call;
                 const int64_t N = (int64_t)L.nx * L.ny;
                 const int64_t gt = (int64_t)rank * blockDim.x + threadIdx.x, gs = (int64_t)CS * blockDim.x;
                 const bool unif = L.beta_uniform > 0.0;
@@ -436,20 +523,25 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
                     HsKeyIdx w{0.0, -1};
                     for (int r = 0; r < CS; ++r) w = hs_kmin(w, s_part[r]);
                     neel_finalize(L, C, sw, w, call, bmin, unif, two, I.attempt_freq);
-                    if (cache && !L.has_dipolar && C->n_sw > 0) {  // no window update: refresh the flipped cell
+                    const int n1 = C->n_sw;
+                    if (cache && !L.has_dipolar && n1 > 0) {  // no window update: refresh the flipped cell
                         const int64_t i = w.idx;
                         const double m = (double)L.m[i];
                         double E = 0.0, Ep = 0.0;
                         if (L.zee) { E = m * (double)L.zee[i]; if (two) Ep = m * (double)L.zee_perp[i]; }
                         cache[i] = neel_cache_value(L, E, Ep, (double)L.E_B[i]);
                     }
+                    // hand the switch to every CTA through shared memory (no global round trip)
+                    Sync<CS>::publish(&s_n1, n1);
+                    if (n1 > 0) {
+                        Sync<CS>::publish(&s_y1, (int)(w.idx / L.nx));
+                        Sync<CS>::publish(&s_x1, (int)(w.idx % L.nx));
+                        Sync<CS>::publish(&s_mm1, L.mm[w.idx]);
+                    }
                 }
                 Sync<CS>::all();
-                if (L.has_dipolar) {
-                    const int nsw = __ldcg(&C->n_sw);
-                    const int n = stage_switches(L, sw, nsw, s_sw, s_pre);
-                    update_items(L, s_sw, s_pre, n, HS_UPDATE_SINGLE, rank * nwarps + warp, CS * nwarps, sw, nsw, cache);
-                }
+                if (L.has_dipolar && s_n1 > 0)
+                    update_one(L, s_y1, s_x1, s_mm1, rank * blockDim.x + threadIdx.x, CS * blockDim.x, cache);
                 Sync<CS>::all();
             } else {  // Wolff
                 if (rank == 0) wolff_step_cta(L, C, sw, wolff_scratch_of(L, I.scratch));
@@ -457,6 +549,12 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
             }
         }
         Sync<CS>::all();
+        if (rank == 0) {  // counters back to global memory
+            const unsigned long long *src = reinterpret_cast<const unsigned long long *>(&s_C);
+            unsigned long long *dst = reinterpret_cast<unsigned long long *>(Cg);
+            for (int k = threadIdx.x; k < (int)(sizeof(HsCounters) / 8); k += blockDim.x) dst[k] = src[k];
+        }
+        __syncthreads();
     }
 }
 
