@@ -375,6 +375,9 @@ def run_product(args):
     recompute = None
     if rank == 0 and args.recompute_n > 0:
         recompute = run_recompute(dev, n=args.recompute_n)
+    incremental = None
+    if rank == 0 and args.incremental_n > 0:
+        incremental = run_incremental(dev, n=args.incremental_n)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -412,6 +415,8 @@ def run_product(args):
         line["served"] = served
     if recompute is not None:
         line["full_recompute"] = recompute
+    if incremental is not None:
+        line["incremental_update"] = incremental
     if not args.no_cpu_baseline:
         v, secs, st, ni = oracle_sample(specs, seconds_per_instance=args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
@@ -507,6 +512,61 @@ def run_recompute(dev, n=2048, n_check=512, reps=3):
         "check": {"n": n_check, "max_rel_err_vs_fp64_direct": err, "rel_err_E_tot": etot,
                   "igemm_ms": t_ig_check, "fp64_direct_ms": t_direct, "speedup": t_direct / t_ig_check},
     })
+    del mm, d
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_incremental(dev, n=2048, reps=20):
+    """(a) The incremental dipolar update (hs_dipolar_update, update_multiple semantics) on an
+    IP_Pinwheel n x n lattice with a 20a cutoff (81 x 81 windows, perpendicular channel on),
+    timed alone through the C ABI: switches on a grid of disjoint windows (every window cell
+    written once: algorithmic bytes = bytes that must move) and on the Metropolis grid spacing
+    r = 20a (windows overlap; the gather still writes each cell once)."""
+    import ctypes
+    import torch
+    import hotspice_b200 as hs
+    from hotspice_b200 import _lib
+    g = np.random.Generator(np.random.PCG64(SEED + 1))
+    m0 = g.integers(0, 2, size=(n, n)) * 2 - 1
+    mm = hs.ASI.IP_Pinwheel(A1, n, T=300.0, E_B=6e-20, moment=1e-15, pattern=m0,
+                            energies=[hs.DipolarEnergy(cutoff_range=20 * A1), hs.ZeemanEnergy(1e-3, math.radians(22.5))],
+                            params=hs.SimParams(UPDATE_SCHEME='Metropolis'), seed=SEED, device=dev)
+    d = mm._dipolar()
+    ks = d.kernel_set
+    W = (2 * ks.wx + 1) * (2 * ks.wy + 1)
+    lib = _lib.load()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    out = {"workload": f"IP_Pinwheel {n}x{n} ({n * n // 2} magnets), a=300nm, dipolar cutoff 20a "
+                       f"(window {2 * ks.wx + 1}x{2 * ks.wy + 1}), perpendicular energy on, FP64 energy accumulators",
+           "bytes_per_window_cell": 28}
+    hbm, kind = measured_peaks()
+    for label, spacing in (("disjoint windows", 2 * ks.wx + 2), ("grid spacing r=20a", 40)):
+        ys, xs = np.meshgrid(np.arange(0, n - 1, spacing), np.arange(0, n - 1, spacing), indexing='ij')
+        ys, xs = ys.ravel(), xs.ravel()
+        xs = xs + ((ys + xs) % 2 == 0)            # pinwheel occupation: (x + y) odd
+        k = len(ys)
+        t, sl = mm._switch_list(k)
+        t[0, :k].copy_(torch.as_tensor(ys, dtype=torch.int32))
+        t[1, :k].copy_(torch.as_tensor(xs, dtype=torch.int32))
+        t[2, :k].zero_()                            # exact windows
+        L = mm._lattice_struct(d)
+        for _ in range(3):
+            _lib.check(lib.hs_dipolar_update(ctypes.byref(L), ctypes.byref(sl), None, k, _lib.HS_UPDATE_MULTIPLE, None,
+                                             stream), 'hs_dipolar_update')
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            lib.hs_dipolar_update(ctypes.byref(L), ctypes.byref(sl), None, k, _lib.HS_UPDATE_MULTIPLE, None, stream)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        us = e0.elapsed_time(e1) * 1e3 / reps
+        alg = k * W * 28
+        out[label] = {"switches": int(k), "us_per_launch": us, "window_cells_per_s": k * W / (us * 1e-6),
+                      "roofline": {"bound": "hbm", "kernel": "dip_update_kernel<4>", "achieved": alg / (us * 1e-6) / 1e9,
+                                   "peak": hbm, "unit": "GB/s", "frac": alg / (us * 1e-6) / 1e9 / hbm,
+                                   "peak_kind": f"{kind} hbm_gbs"}}
     del mm, d
     torch.cuda.empty_cache()
     return out
@@ -620,9 +680,16 @@ def main():
     ap.add_argument('--served', type=int, default=64, help='requests of the served arrival stream (0: skip)')
     ap.add_argument('--recompute-n', type=int, default=2048, help='lattice side of the full-recompute timing (0: skip)')
     ap.add_argument('--only-recompute', action='store_true', help='run only the full-recompute timing and print it')
+    ap.add_argument('--incremental-n', type=int, default=2048, help='lattice side of the incremental-update timing (0: skip)')
+    ap.add_argument('--only-incremental', action='store_true', help='run only the incremental-update timing and print it')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)
+    elif args.only_incremental:
+        import torch
+        dev = torch.device('cuda', 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({"incremental_update": run_incremental(dev, n=args.incremental_n)}))
     elif args.only_recompute:
         import torch
         dev = torch.device('cuda', 0)

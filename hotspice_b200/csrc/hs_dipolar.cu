@@ -1,11 +1,12 @@
 // (a) incremental dipolar energy update and (b, checker) direct full recompute.
 //
 // The incremental update is a deterministic gather: the lattice is cut into tiles of
-// HS_TY rows x (32*VEC) columns, every CTA keeps the switches whose window reaches its
-// tile (in their original order, so the summation order never depends on scheduling),
-// and each thread owns VEC consecutive cells of one row: it reads E and mm once (float4
-// when the row is 16-byte aligned), accumulates sum_s mm_s * K_s(j - s) over the switches,
-// and writes E back once. Semantics follow hotspice/energies.py:310-366:
+// 16 rows x (32*VEC) columns (8 warps, 2 rows each), every CTA keeps the switches whose
+// window reaches its tile (in their original order, so the summation order never depends on
+// scheduling; all warps scan the list together, 1024 switches per round), and each thread
+// owns VEC consecutive cells of 2 rows: it reads E and mm once (float4 when the row is
+// 16-byte aligned), accumulates sum_s mm_s * K_s(j - s) over the switches, and writes E
+// back once. Semantics follow hotspice/energies.py:310-366:
 //   HS_UPDATE_SINGLE   E_j += 2 pref mm_j acc_j; then E_s = -E_s          (update_single)
 //   HS_UPDATE_MULTIPLE E_s = -E_s for every switch; E_j += 2 pref mm_j acc_j (update_multiple)
 // A switch in "truncated" mode (more than SIMULTANEOUS_SWITCHES_CONVOLUTION_OR_SUM_CUTOFF
@@ -18,8 +19,15 @@
 
 namespace {
 
+constexpr int UPD_WARPS = 8;                       // warps per CTA
+constexpr int UPD_RPW = 2;                         // rows per warp
+constexpr int UPD_TY = UPD_WARPS * UPD_RPW;        // rows per tile
+constexpr int UPD_SCAN = 2;                        // switches per lane per staging round
+constexpr int UPD_ROUND = UPD_WARPS * 32 * UPD_SCAN;
+constexpr int UPD_LOC = 2048;                      // staged switches per pass
+
 template <int VEC>
-__global__ void __launch_bounds__(32 * HS_TY)
+__global__ void __launch_bounds__(32 * UPD_WARPS, 4)
 dip_update_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev, int n_host, int semantics,
                   const HsCounters *C) {
     if (C && C->done) return;
@@ -27,129 +35,186 @@ dip_update_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev, int n_h
     if (nsw <= 0) return;
     constexpr int TX = 32 * VEC;
     const int tiles_x = (L.nx + TX - 1) / TX;
-    const int ty0 = (blockIdx.x / tiles_x) * HS_TY;
+    const int ty0 = (blockIdx.x / tiles_x) * UPD_TY;
     const int tx0 = (blockIdx.x % tiles_x) * TX;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int y = ty0 + warp;
     const int x0 = tx0 + lane * VEC;
 
-    __shared__ SwInfo s_sw[HS_LOC];
-    __shared__ int s_n;
-    float acc[VEC], accp[VEC];
-    bool touched[VEC], negate[VEC];
+    __shared__ SwInfo s_sw[UPD_LOC];
+    __shared__ int s_cnt[UPD_WARPS];
+    float acc[UPD_RPW][VEC], accp[UPD_RPW][VEC];
+    unsigned touched = 0u, negate = 0u;   // bit r * VEC + v
 #pragma unroll
-    for (int v = 0; v < VEC; ++v) { acc[v] = 0.f; accp[v] = 0.f; touched[v] = false; negate[v] = false; }
+    for (int r = 0; r < UPD_RPW; ++r)
+#pragma unroll
+        for (int v = 0; v < VEC; ++v) { acc[r][v] = 0.f; accp[r][v] = 0.f; }
 
     const float pref2 = (float)(2.0 * L.dip_pref);
-    __shared__ int s_next;
-    for (int base = 0; base < nsw; base = s_next) {
-        // Stage, in order, the switches of [base, ...) whose window reaches this tile.
-        if (warp == 0) {
-            int n = 0, s = base;
-            while (s < nsw && n <= HS_LOC - 32) {
-                const int k = s + lane;
-                bool hit = false;
-                SwInfo w{};
-                if (k < nsw) {
-                    w.y = sw.y[k]; w.x = sw.x[k]; w.mode = sw.mode ? sw.mode[k] : 0;
-                    w.sub = hs_sub(L, w.y, w.x);
-                    if (w.sub >= 0) {
-                        int hy, wy_, hx, wx_;
-                        hs_window(L, w.mode, true, hy, wy_);
-                        hs_window(L, w.mode, false, hx, wx_);
-                        hit = hs_axis_overlap(w.y, hy, wy_, L.ny, ty0, HS_TY) &&
-                              hs_axis_overlap(w.x, hx, wx_, L.nx, tx0, TX);
-                        w.mm = L.mm[(int64_t)w.y * L.nx + w.x];
-                    } else {
-                        // no kernel for this unit-cell site: only the sign flip of E applies
-                        hit = semantics == HS_UPDATE_MULTIPLE && w.y >= ty0 && w.y < ty0 + HS_TY &&
-                              w.x >= tx0 && w.x < tx0 + TX;
-                        w.mm = 0.f;
+    const bool vec_rows = VEC == 4 && x0 + 3 < L.nx && (L.nx & 3) == 0;
+    for (int base = 0; base < nsw;) {
+        // Stage, in list order, the switches of [base, ...) whose window reaches this tile. All
+        // warps scan: warp w takes the block [s + w 32 UPD_SCAN, ...) of each round, its hits are
+        // compacted in order behind those of the warps before it.
+        int n = 0, s = base;
+        while (s < nsw && n + UPD_ROUND <= UPD_LOC) {
+            int ky[UPD_SCAN], kx[UPD_SCAN], kmode[UPD_SCAN];
+            bool val[UPD_SCAN];
+#pragma unroll
+            for (int u = 0; u < UPD_SCAN; ++u) {
+                const int k = s + (warp * UPD_SCAN + u) * 32 + lane;
+                val[u] = k < nsw;
+                ky[u] = val[u] ? sw.y[k] : 0;
+                kx[u] = val[u] ? sw.x[k] : 0;
+                kmode[u] = (val[u] && sw.mode) ? sw.mode[k] : 0;
+            }
+            SwInfo w[UPD_SCAN];
+            bool hit[UPD_SCAN];
+#pragma unroll
+            for (int u = 0; u < UPD_SCAN; ++u) {
+                w[u] = SwInfo{ky[u], kx[u], kmode[u], -1, 0.f};
+                hit[u] = false;
+                if (!val[u]) continue;
+                w[u].sub = hs_sub(L, ky[u], kx[u]);
+                if (w[u].sub >= 0) {
+                    int hy, wy_, hx, wx_;
+                    hs_window(L, kmode[u], true, hy, wy_);
+                    hs_window(L, kmode[u], false, hx, wx_);
+                    hit[u] = hs_axis_overlap(ky[u], hy, wy_, L.ny, ty0, UPD_TY) &&
+                             hs_axis_overlap(kx[u], hx, wx_, L.nx, tx0, TX);
+                } else {
+                    // no kernel for this unit-cell site: only the sign flip of E applies
+                    hit[u] = semantics == HS_UPDATE_MULTIPLE && ky[u] >= ty0 && ky[u] < ty0 + UPD_TY &&
+                             kx[u] >= tx0 && kx[u] < tx0 + TX;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < UPD_SCAN; ++u)
+                if (hit[u] && w[u].sub >= 0) w[u].mm = L.mm[(int64_t)ky[u] * L.nx + kx[u]];
+            unsigned bal[UPD_SCAN];
+            int wc = 0;
+#pragma unroll
+            for (int u = 0; u < UPD_SCAN; ++u) { bal[u] = __ballot_sync(0xffffffffu, hit[u]); wc += __popc(bal[u]); }
+            if (lane == 0) s_cnt[warp] = wc;
+            __syncthreads();
+            int off = n, tot = n;
+#pragma unroll
+            for (int q = 0; q < UPD_WARPS; ++q) { if (q < warp) off += s_cnt[q]; tot += s_cnt[q]; }
+            const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+            for (int u = 0; u < UPD_SCAN; ++u) {
+                if (hit[u]) s_sw[off + __popc(bal[u] & below)] = w[u];
+                off += __popc(bal[u]);
+            }
+            __syncthreads();
+            n = tot;
+            s += UPD_ROUND;
+        }
+        const int KW = 2 * L.dip_wx + 1, KH = 2 * L.dip_wy + 1;
+        for (int q = 0; q < n; ++q) {
+            const SwInfo w = s_sw[q];
+            if (w.sub >= 0 && !w.mode && !L.dip_wrap) {
+                // exact window without wrapping: one kernel row per target row, consecutive
+                // columns across the lanes (the same values hs_contrib would add)
+                const int64_t kb = (int64_t)w.sub * KH * KW + (L.dip_wx - w.x);
+#pragma unroll
+                for (int r = 0; r < UPD_RPW; ++r) {
+                    const int y = ty0 + warp * UPD_RPW + r;
+                    if (y >= L.ny) continue;
+                    const int dy = y - w.y;
+                    const bool rowin = dy >= -L.dip_wy && dy <= L.dip_wy;
+                    const float *Kr = L.K + kb + (int64_t)(dy + L.dip_wy) * KW;
+                    const float *Kpr = L.use_perp ? L.Kpo + kb + (int64_t)(dy + L.dip_wy) * KW : nullptr;
+#pragma unroll
+                    for (int v = 0; v < VEC; ++v) {
+                        const int x = x0 + v;
+                        if (x >= L.nx) continue;
+                        touched |= 1u << (r * VEC + v);
+                        const int dx = x - w.x;
+                        if (rowin && dx >= -L.dip_wx && dx <= L.dip_wx) {
+                            acc[r][v] += w.mm * __ldg(Kr + x);
+                            if (L.use_perp) accp[r][v] += w.mm * __ldg(Kpr + x);
+                            if (dy == 0 && dx == 0) negate |= 1u << (r * VEC + v);
+                        }
                     }
                 }
-                const unsigned bal = __ballot_sync(0xffffffffu, hit);
-                if (hit) s_sw[n + __popc(bal & ((1u << lane) - 1u))] = w;
-                n += __popc(bal);
-                s += 32;
+                continue;
             }
-            if (lane == 0) { s_n = n; s_next = s; }
-        }
-        __syncthreads();
-        const int n = s_n;
-        if (y < L.ny) {
-            for (int q = 0; q < n; ++q) {
-                const SwInfo w = s_sw[q];
+#pragma unroll
+            for (int r = 0; r < UPD_RPW; ++r) {
+                const int y = ty0 + warp * UPD_RPW + r;
+                if (y >= L.ny) continue;
 #pragma unroll
                 for (int v = 0; v < VEC; ++v) {
                     const int x = x0 + v;
                     if (x >= L.nx) continue;
                     if (w.sub >= 0) {
-                        float a = acc[v], ap = accp[v];
+                        float a = acc[r][v], ap = accp[r][v];
                         hs_contrib(L, w, y, x, a, ap);
-                        acc[v] = a; accp[v] = ap;
+                        acc[r][v] = a; accp[r][v] = ap;
                     }
-                    touched[v] = true;
-                    if (w.y == y && w.x == x) negate[v] = true;
+                    touched |= 1u << (r * VEC + v);
+                    if (w.y == y && w.x == x) negate |= 1u << (r * VEC + v);
                 }
             }
         }
         __syncthreads();
+        base = s;
     }
-    if (y >= L.ny) return;
-    const int64_t row = (int64_t)y * L.nx;
-    if (VEC == 4 && x0 + 3 < L.nx && (L.nx & 3) == 0) {
-        bool any = touched[0] || touched[1] || touched[2] || touched[3];
-        if (!any) return;
-        const float4 mm4 = *reinterpret_cast<const float4 *>(L.mm + row + x0);
-        const float mmv[4] = {mm4.x, mm4.y, mm4.z, mm4.w};
-        const double2 e01 = *reinterpret_cast<const double2 *>(L.E_dip + row + x0);
-        const double2 e23 = *reinterpret_cast<const double2 *>(L.E_dip + row + x0 + 2);
-        double ev[4] = {e01.x, e01.y, e23.x, e23.y};
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            if (semantics == HS_UPDATE_MULTIPLE) {
-                if (negate[v]) ev[v] = -ev[v];
-                ev[v] += (double)(pref2 * (mmv[v] * acc[v]));
-            } else {
-                ev[v] += (double)(pref2 * (mmv[v] * acc[v]));
-                if (negate[v]) ev[v] = -ev[v];
+    for (int r = 0; r < UPD_RPW; ++r) {
+        const int y = ty0 + warp * UPD_RPW + r;
+        if (y >= L.ny) continue;
+        const int64_t row = (int64_t)y * L.nx;
+        if (vec_rows) {
+            if (!((touched >> (r * VEC)) & 0xFu)) continue;
+            const float4 mm4 = *reinterpret_cast<const float4 *>(L.mm + row + x0);
+            const float mmv[4] = {mm4.x, mm4.y, mm4.z, mm4.w};
+            const double2 e01 = *reinterpret_cast<const double2 *>(L.E_dip + row + x0);
+            const double2 e23 = *reinterpret_cast<const double2 *>(L.E_dip + row + x0 + 2);
+            double ev[4] = {e01.x, e01.y, e23.x, e23.y};
+            double pv[4] = {0.0, 0.0, 0.0, 0.0};
+            if (L.use_perp) {
+                const double2 p01 = *reinterpret_cast<const double2 *>(L.E_dip_perp + row + x0);
+                const double2 p23 = *reinterpret_cast<const double2 *>(L.E_dip_perp + row + x0 + 2);
+                pv[0] = p01.x; pv[1] = p01.y; pv[2] = p23.x; pv[3] = p23.y;
             }
-        }
-        *reinterpret_cast<double2 *>(L.E_dip + row + x0) = make_double2(ev[0], ev[1]);
-        *reinterpret_cast<double2 *>(L.E_dip + row + x0 + 2) = make_double2(ev[2], ev[3]);
-        if (L.use_perp) {
-            const double2 p01 = *reinterpret_cast<const double2 *>(L.E_dip_perp + row + x0);
-            const double2 p23 = *reinterpret_cast<const double2 *>(L.E_dip_perp + row + x0 + 2);
-            double pv[4] = {p01.x, p01.y, p23.x, p23.y};
 #pragma unroll
             for (int v = 0; v < 4; ++v) {
+                const bool ng = (negate >> (r * VEC + v)) & 1u;
                 if (semantics == HS_UPDATE_MULTIPLE) {
-                    if (negate[v]) pv[v] = -pv[v];
-                    pv[v] += (double)(pref2 * (mmv[v] * accp[v]));
+                    if (ng) { ev[v] = -ev[v]; pv[v] = -pv[v]; }
+                    ev[v] += (double)(pref2 * (mmv[v] * acc[r][v]));
+                    pv[v] += (double)(pref2 * (mmv[v] * accp[r][v]));
                 } else {
-                    pv[v] += (double)(pref2 * (mmv[v] * accp[v]));
-                    if (negate[v]) pv[v] = -pv[v];
+                    ev[v] += (double)(pref2 * (mmv[v] * acc[r][v]));
+                    pv[v] += (double)(pref2 * (mmv[v] * accp[r][v]));
+                    if (ng) { ev[v] = -ev[v]; pv[v] = -pv[v]; }
                 }
             }
-            *reinterpret_cast<double2 *>(L.E_dip_perp + row + x0) = make_double2(pv[0], pv[1]);
-            *reinterpret_cast<double2 *>(L.E_dip_perp + row + x0 + 2) = make_double2(pv[2], pv[3]);
+            *reinterpret_cast<double2 *>(L.E_dip + row + x0) = make_double2(ev[0], ev[1]);
+            *reinterpret_cast<double2 *>(L.E_dip + row + x0 + 2) = make_double2(ev[2], ev[3]);
+            if (L.use_perp) {
+                *reinterpret_cast<double2 *>(L.E_dip_perp + row + x0) = make_double2(pv[0], pv[1]);
+                *reinterpret_cast<double2 *>(L.E_dip_perp + row + x0 + 2) = make_double2(pv[2], pv[3]);
+            }
+            continue;
         }
-        return;
-    }
 #pragma unroll
-    for (int v = 0; v < VEC; ++v) {
-        const int x = x0 + v;
-        if (x >= L.nx || !touched[v]) continue;
-        const float mmv = L.mm[row + x];
-        double e = L.E_dip[row + x];
-        if (semantics == HS_UPDATE_MULTIPLE) { if (negate[v]) e = -e; e += (double)(pref2 * (mmv * acc[v])); }
-        else { e += (double)(pref2 * (mmv * acc[v])); if (negate[v]) e = -e; }
-        L.E_dip[row + x] = e;
-        if (L.use_perp) {
-            double p = L.E_dip_perp[row + x];
-            if (semantics == HS_UPDATE_MULTIPLE) { if (negate[v]) p = -p; p += (double)(pref2 * (mmv * accp[v])); }
-            else { p += (double)(pref2 * (mmv * accp[v])); if (negate[v]) p = -p; }
-            L.E_dip_perp[row + x] = p;
+        for (int v = 0; v < VEC; ++v) {
+            const int x = x0 + v;
+            if (x >= L.nx || !((touched >> (r * VEC + v)) & 1u)) continue;
+            const bool ng = (negate >> (r * VEC + v)) & 1u;
+            const float mmv = L.mm[row + x];
+            double e = L.E_dip[row + x];
+            if (semantics == HS_UPDATE_MULTIPLE) { if (ng) e = -e; e += (double)(pref2 * (mmv * acc[r][v])); }
+            else { e += (double)(pref2 * (mmv * acc[r][v])); if (ng) e = -e; }
+            L.E_dip[row + x] = e;
+            if (L.use_perp) {
+                double p = L.E_dip_perp[row + x];
+                if (semantics == HS_UPDATE_MULTIPLE) { if (ng) p = -p; p += (double)(pref2 * (mmv * accp[r][v])); }
+                else { p += (double)(pref2 * (mmv * accp[r][v])); if (ng) p = -p; }
+                L.E_dip_perp[row + x] = p;
+            }
         }
     }
 }
@@ -209,9 +274,9 @@ int hs_launch_dipolar_update(const HsLattice &L, const HsSwitchList &sw, const i
                              int semantics, const HsCounters *C, cudaStream_t st) {
     const bool vec = (L.nx % 4) == 0;
     const int TX = vec ? 128 : 32;
-    const int tiles = ((L.nx + TX - 1) / TX) * ((L.ny + HS_TY - 1) / HS_TY);
-    if (vec) dip_update_kernel<4><<<tiles, 32 * HS_TY, 0, st>>>(L, sw, n_sw_dev, n_host, semantics, C);
-    else dip_update_kernel<1><<<tiles, 32 * HS_TY, 0, st>>>(L, sw, n_sw_dev, n_host, semantics, C);
+    const int tiles = ((L.nx + TX - 1) / TX) * ((L.ny + UPD_TY - 1) / UPD_TY);
+    if (vec) dip_update_kernel<4><<<tiles, 32 * UPD_WARPS, 0, st>>>(L, sw, n_sw_dev, n_host, semantics, C);
+    else dip_update_kernel<1><<<tiles, 32 * UPD_WARPS, 0, st>>>(L, sw, n_sw_dev, n_host, semantics, C);
     return hs_check_launch("dip_update_kernel");
 }
 

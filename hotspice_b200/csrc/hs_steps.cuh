@@ -5,8 +5,6 @@
 
 // ---- dipolar window helpers ----------------------------------------------------------
 
-constexpr int HS_TY = 8;          // rows per tile (one warp per row)
-constexpr int HS_LOC = 512;       // switches staged in shared memory per pass
 
 struct SwInfo { int y, x, mode, sub; float mm; };
 
