@@ -47,31 +47,35 @@ def _bind():
     return lib
 
 
-def step_model(mm: Magnets) -> tuple[float, float, bool]:
-    """Device time of one step on one SM, as (serial us, divisible us, divides over the
-    cluster). Calibrated on B200 with single instances (bench lattices, n = 32..256): a Néel
-    step costs about 8.5 us plus 2.3 ns per cell (3.0 ns with the perpendicular channel) plus
-    about 1 ns per window cell of the update, and the per-cell part spreads over the cluster's
-    CTAs; a Metropolis step about 5 us plus a little per cell and window cell (its selection
-    runs on one CTA); a Wolff step grows its cluster on one CTA."""
+def step_model(mm: Magnets) -> tuple[float, float, float]:
+    """Device time of one step as (fixed us, cell-dependent us on one CTA, exponent alpha): on a
+    cluster of cs CTAs a step takes fixed + part / cs**alpha. Calibrated on B200 with single
+    instances of the bench lattices (n = 32..512, cluster sizes 1, 4, 16): the cell-dependent
+    part grows like c N^beta with the lattice's occupancy class (dense / half / sparse, which
+    also carries the perpendicular channel of the in-plane lattices), Néel scans spread over the
+    cluster like cs^0.62 and Metropolis steps like cs^0.5; a Wolff step grows its cluster on one
+    CTA and costs 10-17 us above the critical temperature."""
     n = mm.nx * mm.ny
-    d = mm._dipolar()
-    win = (2 * d.kernel_set.wx + 1) * (2 * d.kernel_set.wy + 1) if d is not None else 9
+    f = mm.n / max(n, 1)
+    cls = 0 if f >= 0.75 else (1 if f >= 0.45 else 2)
     sch = mm.params.UPDATE_SCHEME
     if sch == Scheme.NEEL:
-        per = 0.0030 if mm.USE_PERP_ENERGY else 0.0023
-        return 8.5, per * n + 0.001 * win, True
+        c, beta = ((0.0116, 0.786), (0.0198, 0.716), (0.0431, 0.646))[cls]
+        return 9.0, c * n ** beta, 0.62
     if sch == Scheme.WOLFF:
-        return 5.0, 0.002 * n, False
-    return 5.0, 0.0001 * n + 0.0005 * win, True
+        return 11.0 + 6e-6 * n, 0.0, 0.0
+    c, beta = ((0.0037, 0.70), (0.0068, 0.70), (0.0061, 0.73))[cls]
+    return 5.0, c * n ** beta, 0.5
+
+
+def _t(m, cs):
+    s0, p, alpha = m
+    return s0 + (p / cs ** alpha if alpha > 0 else p) + 0.1 * (cs - 1)
 
 
 def step_time(mm: Magnets, cs: int = 1) -> float:
     """Modelled device time (us) of one step of ``mm`` on a cluster of ``cs`` CTAs."""
-    s0, p, divides = step_model(mm)
-    if not divides:
-        return s0 + p
-    return s0 + p / cs + 0.25 * (cs - 1)
+    return _t(step_model(mm), cs)
 
 
 def step_cost(mm: Magnets) -> float:
@@ -106,9 +110,7 @@ def plan_uniform_size(models, steps, n_sm, sizes=CLUSTER_SIZES):
     """One cluster size for a whole launch: the size whose longest-first schedule of the
     modelled run times over the clusters that fit (SM count / size) finishes first. One
     size per launch keeps clusters of different shapes from fragmenting the GPCs."""
-    def t(m, cs):
-        s0, p, dv = m
-        return s0 + p if not dv else s0 + p / cs + 0.25 * (cs - 1)
+    t = _t
     best, best_t = 1, math.inf
     for cs in sizes:
         mk = lpt_makespan([st * t(m, cs) for m, st in zip(models, steps)], n_sm // cs)
@@ -121,16 +123,14 @@ def plan_sizes(models, steps, n_sm, max_cs=16):
     """Cluster sizes for a batch: start every instance on one CTA; an instance whose run is
     longer than the even share of the GPU (total SM time / SM count) gets twice the CTAs
     while that shortens it by at least 20%, until no run exceeds the share (or max_cs).
-    ``models``: (serial us, divisible us, divides) per instance, as step_model gives."""
-    def t(m, cs):
-        s0, p, dv = m
-        return s0 + p if not dv else s0 + p / cs + 0.25 * (cs - 1)
+    ``models``: (fixed us, cell-dependent us, alpha) per instance, as step_model gives."""
+    t = _t
     cs = [1] * len(models)
     for _ in range(5):
         share = sum(st * t(m, c) * c for m, st, c in zip(models, steps, cs)) / n_sm
         changed = False
         for i, (m, st) in enumerate(zip(models, steps)):
-            while cs[i] < max_cs and m[2] and st * t(m, cs[i]) > share and t(m, 2 * cs[i]) < 0.8 * t(m, cs[i]):
+            while cs[i] < max_cs and m[2] > 0 and st * t(m, cs[i]) > share and t(m, 2 * cs[i]) < 0.8 * t(m, cs[i]):
                 cs[i] *= 2
                 changed = True
         if not changed:

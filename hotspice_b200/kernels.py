@@ -32,19 +32,34 @@ class KernelSet:
     asymmetry: float = 0.0   # see kernel_asymmetry()
 
 
-def _site_kernels(nx, ny, ux, uy, y, x, dx_cell, dy_cell, ori, occ, in_plane, cutoff, decay, I):
-    """Unfolded FP64 kernels (normal, perp-self, perp-other) of unit-cell site (y, x)."""
+def _site_axes(nx, ny, ux, uy, y, x, dx_cell, dy_cell):
+    """Unit-cell phases (rows, cols) and positions (ry, rx) of every kernel offset of site
+    (y, x), accumulated over the phase-shifted spacings along the full offset range."""
     H, W = 2 * ny - 1, 2 * nx - 1
     # unit-cell phase of kernel column 0 / row 0 (so that column nx-1 is site x itself)
     cols = (x - (nx - 1) + np.arange(W)) % ux
     rows = (y - (ny - 1) + np.arange(H)) % uy
-    # positions relative to the centre, accumulated over the phase-shifted spacings
     cx = np.cumsum(dx_cell[cols])
     cy = np.cumsum(dy_cell[rows])
-    rx = (cx - cx[nx - 1])[None, :]
-    ry = (cy - cy[ny - 1])[:, None]
+    return rows, cols, cy - cy[ny - 1], cx - cx[nx - 1]
+
+
+def _site_kernels(nx, ny, ux, uy, y, x, dx_cell, dy_cell, ori, occ, in_plane, cutoff, decay, I, hw=None):
+    """Unfolded FP64 kernels (normal, perp-self, perp-other) of unit-cell site (y, x); with
+    ``hw = (hy, hx)`` only the offsets |dy| <= hy, |dx| <= hx (the distances still come from
+    the full-range cumulative sums, so every entry is the same as in the full kernel)."""
+    rows, cols, ryv, rxv = _site_axes(nx, ny, ux, uy, y, x, dx_cell, dy_cell)
+    if hw is not None:
+        hy, hx = hw
+        rows, ryv = rows[ny - 1 - hy:ny + hy], ryv[ny - 1 - hy:ny + hy]
+        cols, rxv = cols[nx - 1 - hx:nx + hx], rxv[nx - 1 - hx:nx + hx]
+        cy0, cx0 = hy, hx
+    else:
+        cy0, cx0 = ny - 1, nx - 1
+    rx = rxv[None, :]
+    ry = ryv[:, None]
     r2 = rx * rx + ry * ry
-    r2[ny - 1, nx - 1] = np.inf
+    r2[cy0, cx0] = np.inf
     r2 = np.where(r2 > cutoff * cutoff, np.inf, r2)
     rinv = r2 ** -0.5
     r3 = rinv ** (-decay)
@@ -89,7 +104,7 @@ def build_kernels(mm, cutoff=np.inf, decay_exponent=-3) -> KernelSet:
     ori = mm.orientation[:uy, :ux] if mm.in_plane else None
     occ = mm.occupation[:uy, :ux]
     sub_of = -np.ones((uy, ux), dtype=np.int32)
-    ks, kps, kpo = [], [], []
+    sites = []
     for y in range(uy):
         for x in range(ux):
             if mm.in_plane:
@@ -97,19 +112,36 @@ def build_kernels(mm, cutoff=np.inf, decay_exponent=-3) -> KernelSet:
                     continue
             elif occ[y, x] == 0:
                 continue
-            k, a, b = _site_kernels(nx, ny, ux, uy, y, x, dx_cell, dy_cell, ori, occ, mm.in_plane,
-                                    cutoff, decay_exponent, I)
-            sub_of[y, x] = len(ks)
-            ks.append(k); kps.append(a); kpo.append(b)
-    if not ks:
+            sites.append((y, x))
+    if not sites:
         raise ValueError('no occupied unit-cell site: nothing to build a dipolar kernel for')
+    # with a finite cutoff, build only the offsets whose row and column distances are within it
+    # (a superset of the non-zero entries), unless periodic images must be folded in
+    hw = None
+    if np.isfinite(cutoff):
+        hy = hx = 0
+        for (y, x) in sites:
+            _, _, ryv, rxv = _site_axes(nx, ny, ux, uy, y, x, dx_cell, dy_cell)
+            iy = np.nonzero(np.abs(ryv) <= cutoff)[0]
+            ix = np.nonzero(np.abs(rxv) <= cutoff)[0]
+            hy = max(hy, int(np.max(np.abs(iy - (ny - 1)))) if iy.size else 0)
+            hx = max(hx, int(np.max(np.abs(ix - (nx - 1)))) if ix.size else 0)
+        if not mm.PBC or (2 * hy + 1 <= ny and 2 * hx + 1 <= nx):
+            hw = (hy, hx)
+    ks, kps, kpo = [], [], []
+    for (y, x) in sites:
+        k, a, b = _site_kernels(nx, ny, ux, uy, y, x, dx_cell, dy_cell, ori, occ, mm.in_plane,
+                                cutoff, decay_exponent, I, hw)
+        sub_of[y, x] = len(ks)
+        ks.append(k); kps.append(a); kpo.append(b)
     K, Kps, Kpo = np.asarray(ks), np.asarray(kps), np.asarray(kpo)
-    asym = kernel_asymmetry(K, sub_of, nx, ny)
+    cy0, cx0 = (hw[0], hw[1]) if hw is not None else (ny - 1, nx - 1)
+    asym = kernel_asymmetry(K, sub_of, nx, ny, center=(cy0, cx0))
     nz = (K != 0) | (Kps != 0) | (Kpo != 0)
     rows = np.nonzero(nz.any(axis=(0, 2)))[0]
     cols = np.nonzero(nz.any(axis=(0, 1)))[0]
-    wy = int(np.max(np.abs(rows - (ny - 1)))) if rows.size else 0
-    wx = int(np.max(np.abs(cols - (nx - 1)))) if cols.size else 0
+    wy = int(np.max(np.abs(rows - cy0))) if rows.size else 0
+    wx = int(np.max(np.abs(cols - cx0))) if cols.size else 0
     finite = np.isfinite(cutoff)
     if mm.PBC and not (finite and 2 * wy + 1 <= ny and 2 * wx + 1 <= nx):
         for arr in (K, Kps, Kpo):
@@ -120,13 +152,13 @@ def build_kernels(mm, cutoff=np.inf, decay_exponent=-3) -> KernelSet:
         wrap = bool(mm.PBC)
         if not finite:
             wy, wx = ny - 1, nx - 1
-    sl = np.s_[:, ny - 1 - wy:ny + wy, nx - 1 - wx:nx + wx]
+    sl = np.s_[:, cy0 - wy:cy0 + wy + 1, cx0 - wx:cx0 + wx + 1]
     scale = 1e-7  # mu0 / 4 pi
     return KernelSet(K[sl] * scale, Kps[sl] * scale, Kpo[sl] * scale, sub_of, wx, wy, wrap,
                      wy == ny - 1 and wx == nx - 1 and not wrap, asym)
 
 
-def kernel_asymmetry(K, sub_of, nx, ny):
+def kernel_asymmetry(K, sub_of, nx, ny, center=None):
     """max |K_s(d) - K_s'(-d)| / max |K| over all sites s and offsets d, s' the site at d.
 
     The interaction of two magnets must not depend on which one is the kernel's centre, and
@@ -137,7 +169,8 @@ def kernel_asymmetry(K, sub_of, nx, ny):
     non-zero value means the incremental energies drift from a full recompute by design (the
     reference drifts identically)."""
     uy, ux = sub_of.shape
-    H, W = 2 * ny - 1, 2 * nx - 1
+    H, W = K.shape[1], K.shape[2]
+    cy0, cx0 = center if center is not None else (ny - 1, nx - 1)
     flip = K[:, ::-1, ::-1]
     worst = 0.0
     for ys in range(uy):
@@ -145,8 +178,8 @@ def kernel_asymmetry(K, sub_of, nx, ny):
             s = sub_of[ys, xs]
             if s < 0:
                 continue
-            rows = (ys - (ny - 1) + np.arange(H)) % uy
-            cols = (xs - (nx - 1) + np.arange(W)) % ux
+            rows = (ys - cy0 + np.arange(H)) % uy
+            cols = (xs - cx0 + np.arange(W)) % ux
             tgt = sub_of[rows[:, None], cols[None, :]]
             other = np.where(tgt >= 0, flip[np.clip(tgt, 0, None), np.arange(H)[:, None], np.arange(W)[None, :]], 0.0)
             worst = max(worst, float(np.max(np.abs(K[s] - other))))

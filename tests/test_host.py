@@ -30,8 +30,8 @@ def expand_window(ks, nx, ny, K):
     for p in range(2 * ny - 1):
         for q in range(2 * nx - 1):
             dy, dx = p - (ny - 1), q - (nx - 1)
-            if ks.wrap:
-                dy = ((dy + ny // 2) % ny) - ny // 2 if False else (dy % ny if (dy % ny) * 2 < ny else dy % ny - ny)
+            if ks.wrap:  # minimum image, as hs_minimage
+                dy = dy % ny if (dy % ny) * 2 < ny else dy % ny - ny
                 dx = dx % nx if (dx % nx) * 2 < nx else dx % nx - nx
             if abs(dy) <= ks.wy and abs(dx) <= ks.wx:
                 out[:, p, q] = K[:, dy + ks.wy, dx + ks.wx]
@@ -51,6 +51,44 @@ def test_kernel_windows_match_reference(name):
         assert rel_err(full, ref) < 1e-12, name
     if np.isfinite(cut):
         assert ks.wy < mm.ny - 1 or ks.wx < mm.nx - 1 or not ks.wrap
+
+
+@pytest.mark.parametrize('kind,n,PBC,cut_a', [('oop', 40, False, 6), ('oop', 40, True, 6), ('pin', 48, False, 8),
+                                              ('pin', 48, True, 8), ('kag', 40, False, 3), ('kag', 44, True, 3)])
+def test_windowed_kernels_equal_full_construction(kind, n, PBC, cut_a):
+    """With a finite cutoff the kernels are built on the cutoff window only; every entry must
+    be the same bits as in the full (2ny-1, 2nx-1) construction, which builds the distances
+    from the same full-range cumulative sums."""
+    import hotspice_b200.kernels as KM
+    from oracle import geometry as G
+    from oracle.geometry import unitcell
+    a = 300e-9
+    g = {'oop': G.oop_square, 'pin': G.ip_pinwheel, 'kag': G.ip_kagome}[kind](a, n, PBC=PBC) if kind == 'kag' \
+        else {'oop': G.oop_square, 'pin': G.ip_pinwheel}[kind](a, n)
+    ux, uy = unitcell(g)
+    mm = SimpleNamespace(nx=g.nx, ny=g.ny, unitcell=SimpleNamespace(x=ux, y=uy), dx=g.dx, dy=g.dy,
+                         orientation=g.orientation, occupation=g.occupation, in_plane=g.in_plane, PBC=PBC,
+                         major_axis=0.0, minor_axis=0.0)
+    cut = cut_a * a
+    ks = KM.build_kernels(mm, cut)
+    dxc, dyc = np.asarray(g.dx[:ux], float), np.asarray(g.dy[:uy], float)
+    ori = g.orientation[:uy, :ux] if g.in_plane else None
+    occ = g.occupation[:uy, :ux]
+    for y in range(uy):
+        for x in range(ux):
+            if ks.sub_of[y, x] < 0:
+                continue
+            full = KM._site_kernels(g.nx, g.ny, ux, uy, y, x, dxc, dyc, ori, occ, g.in_plane, cut, -3, 0.0)
+            win = KM._site_kernels(g.nx, g.ny, ux, uy, y, x, dxc, dyc, ori, occ, g.in_plane, cut, -3, 0.0,
+                                   (ks.wy, ks.wx))
+            for f, w in zip(full, win):
+                assert np.array_equal(f[g.ny - 1 - ks.wy:g.ny + ks.wy, g.nx - 1 - ks.wx:g.nx + ks.wx], w)
+                # nothing non-zero outside the window
+                mask = np.ones_like(f, dtype=bool)
+                mask[g.ny - 1 - ks.wy:g.ny + ks.wy, g.nx - 1 - ks.wx:g.nx + ks.wx] = False
+                assert not np.any(f[mask])
+            s = ks.sub_of[y, x]
+            assert np.array_equal(full[0][g.ny - 1 - ks.wy:g.ny + ks.wy, g.nx - 1 - ks.wx:g.nx + ks.wx] * 1e-7, ks.K[s])
 
 
 def test_pbc_cutoff_window_is_minimum_image():

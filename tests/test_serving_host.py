@@ -70,18 +70,22 @@ def test_plan_quanta():
 
 
 def test_plan_sizes():
-    from hotspice_b200.engine import plan_sizes
-    neel_big = (8.5, 150.0, True)                   # ~65k-cell Néel lattice
-    neel_small = (8.5, 2.0, True)
-    wolff = (5.0, 100.0, False)                     # grows on one CTA: never widened
+    from hotspice_b200.engine import plan_sizes, plan_uniform_size, lpt_makespan
+    neel_big = (9.0, 600.0, 0.62)                   # ~500^2-cell Néel lattice
+    neel_small = (9.0, 2.0, 0.62)
+    wolff = (12.0, 0.0, 0.0)                        # grows on one CTA: never widened
     # one long run among short ones gets a wide cluster; short runs stay on one CTA
-    cs = plan_sizes([neel_big] + [neel_small] * 200, [1000] + [100] * 200, n_sm=148)
+    cs = plan_sizes([neel_big] + [neel_small] * 200, [5000] + [100] * 200, n_sm=148)
     assert cs[0] >= 8 and set(cs[1:]) == {1}
     assert plan_sizes([wolff] * 3, [10**6] * 3, n_sm=148) == [1, 1, 1]
     # many equal runs that fill the GPU: one CTA each
     assert plan_sizes([neel_big] * 300, [100] * 300, n_sm=148) == [1] * 300
     # widening stops when it no longer shortens the run by 20%
-    assert plan_sizes([(8.5, 4.0, True)], [10**6], n_sm=148) == [1]
+    assert plan_sizes([(9.0, 2.0, 0.62)], [10**6], n_sm=148) == [1]
+    # one size per launch: a few long runs want wide clusters, many short ones want one CTA each
+    assert plan_uniform_size([neel_big] * 4, [10**4] * 4, n_sm=148) >= 8
+    assert plan_uniform_size([neel_small] * 600, [100] * 600, n_sm=148) == 1
+    assert lpt_makespan([5, 4, 3, 3, 3], 2) == 10
 
 
 def test_fifo_latencies():
