@@ -239,10 +239,12 @@ class Server:
     ``hbm_budget``: device bytes the resident instances may hold (default: half of the free
     memory when the server starts); ``max_slots``: resident instances at most; ``round_ms``:
     device time one instance's quantum aims at (from the engine's step-time model, corrected
-    by the measured speed of past rounds); ``keep_state``: return the final spins."""
+    by the measured speed of past rounds) while requests arrive, ``tail_round_ms`` once they
+    have all arrived; ``keep_state``: return the final spins; ``builders``: threads that build
+    admitted requests (host set-up overlaps the device rounds)."""
 
     def __init__(self, device=None, hbm_budget=None, max_slots=4096, round_ms=5.0, keep_state=False,
-                 max_inflight=2):
+                 max_inflight=2, tail_round_ms=20.0, builders=2):
         import torch
         from .engine import BatchEngine  # noqa: F401  (binds the engine symbols early)
         self.torch = torch
@@ -261,13 +263,16 @@ class Server:
         self.build_stream = torch.cuda.Stream(self.device)
         self.stats = ServeStats()
         self._engine = None
+        self.tail_round_ms = float(tail_round_ms)
+        import concurrent.futures
+        self._builder = concurrent.futures.ThreadPoolExecutor(max_workers=max(1, int(builders)))
 
     # -- one round ---------------------------------------------------------------------
-    def _launch_round(self, active: list[_Active]):
+    def _launch_round(self, active: list[_Active], round_ms: float):
         torch = self.torch
         sizes = plan_sizes([a.model for a in active], [a.remaining for a in active], self.n_sm)
         times = [step_time(a.mm, c) for a, c in zip(active, sizes)]
-        steps = plan_quanta(times, [a.remaining for a in active], self.speed * self.round_ms * 1e3)
+        steps = plan_quanta(times, [a.remaining for a in active], self.speed * round_ms * 1e3)
         if self._engine is None:
             from .engine import BatchEngine
             self._engine = BatchEngine([a.mm for a in active], device=self.device, throughput=True)
@@ -320,37 +325,57 @@ class Server:
         def clock():
             return time.perf_counter() - t0
 
+        building: list = []      # (request, footprint, future) of admitted requests being built
+
+        def build(r):
+            # runs on the builder thread: its own stream, an event the rounds wait on
+            torch.cuda.set_device(self.device)
+            with torch.cuda.stream(self.build_stream):
+                mm = build_magnets(r.spec, device=self.device)
+                ev = torch.cuda.Event()
+                ev.record(self.build_stream)
+            return mm, ev
+
         def admit():
+            """Move arrived requests to the queue, start building those that fit (the builder
+            thread works while rounds run) and activate the ones that are built."""
             nonlocal used_bytes
             now = clock()
             while pending and (not realtime or pending[0].arrival <= now):
                 queue.push(pending.popleft())
-            if not queue:
-                return False
-            reserved = sum(a.bytes for a in active)
-            new = queue.admit(self.hbm_budget - reserved, self.max_slots - len(active))
-            for r in new:
-                with torch.cuda.stream(self.build_stream):
-                    mm = build_magnets(r.spec, device=self.device)
-                    ev = torch.cuda.Event()
-                    ev.record(self.build_stream)
-                b = footprint_bytes(r.spec)
-                active.append(_Active(r, mm, int(r.steps), step_model(mm), time.perf_counter(), b, ev))
-            used_bytes = sum(a.bytes for a in active)
+            changed = False
+            if queue:
+                reserved = sum(a.bytes for a in active) + sum(b for _, b, _ in building)
+                new = queue.admit(self.hbm_budget - reserved, self.max_slots - len(active) - len(building))
+                for r in new:
+                    building.append((r, footprint_bytes(r.spec), self._builder.submit(build, r)))
+            still = []
+            for r, b, fut in building:
+                if fut.done():
+                    mm, ev = fut.result()
+                    active.append(_Active(r, mm, int(r.steps), step_model(mm), time.perf_counter(), b, ev))
+                    changed = True
+                else:
+                    still.append((r, b, fut))
+            building[:] = still
+            used_bytes = sum(a.bytes for a in active) + sum(b for _, b, _ in building)
             st.admitted_bytes_peak = max(st.admitted_bytes_peak, used_bytes)
-            return bool(new)
+            return changed
 
-        while pending or queue or active or inflight:
+        while pending or queue or active or inflight or building:
             admit()
             runnable = [a for a in active if a.remaining > 0]
             if runnable and len(inflight) < self.max_inflight:
-                inflight.append(self._launch_round(runnable))
+                # short rounds while requests still arrive (they join at round boundaries),
+                # longer ones once the stream has ended
+                rms = self.round_ms if (pending or queue or building) else max(self.round_ms, self.tail_round_ms)
+                inflight.append(self._launch_round(runnable, rms))
                 st.rounds += 1
                 st.max_active = max(st.max_active, len(runnable))
                 continue
             if inflight:
                 rd = inflight[0]
-                # overlap: build newly arrived requests while the oldest round runs
+                # overlap: activate newly built requests while the oldest round runs
                 while not rd['e1'].query():
                     if not admit():
                         time.sleep(50e-6)
@@ -371,6 +396,13 @@ class Server:
                         done_ids.add(id(a))
                 if done_ids:
                     active[:] = [a for a in active if id(a) not in done_ids]
+                continue
+            if building:
+                for _, _, fut in building:
+                    if fut.done():
+                        break
+                else:
+                    time.sleep(100e-6)
                 continue
             if queue and not active:
                 r = queue.waiting[0]
