@@ -146,6 +146,17 @@ class _Prepared:
     keep: list
 
 
+class CapturedRun:
+    """A CUDA graph holding one engine launch (see :meth:`BatchEngine.capture`); it keeps the
+    instance descriptors it points to alive."""
+
+    def __init__(self, graph, prepared, engine):
+        self.graph, self.prepared, self.engine = graph, prepared, engine
+
+    def replay(self):
+        self.graph.replay()
+
+
 class BatchEngine:
     """Advance several Magnets at once: ``run(steps)`` (fixed step budgets) or
     ``progress(t_max, MCsteps_max)`` (the reference's stop rule, per instance)."""
@@ -289,6 +300,29 @@ class BatchEngine:
         prepared = self._cache[1]
         self.launch(prepared)
         return prepared
+
+    def capture(self, steps, sizes=None, **kwargs):
+        """Record the launch of ``run(steps, ...)`` in a CUDA graph and return a
+        :class:`CapturedRun`; each ``replay()`` advances every instance by ``steps`` again
+        with no host work (the work counters are reset inside the graph). The instances'
+        step controls are set before the capture; set them again (``run`` or ``capture``)
+        after changing them on the host."""
+        steps_l = [int(steps)] * len(self.magnets) if np.isscalar(steps) else [int(x) for x in steps]
+        kws = [dict(kwargs) for _ in self.magnets]
+        for mm, kw in zip(self.magnets, kws):
+            mm._set_control(progress=0, done=0, t_max=float(kw.pop('t_max', math.inf)))
+        prepared = self._prepare(steps_l, kws, sizes)
+        for p in prepared:          # occupancy queries happen outside the capture
+            self._max(p.cs)
+        if len(prepared) > 1 and len(self._streams) < len(prepared):
+            self._streams += [torch.cuda.Stream(self.device) for _ in range(len(prepared) - len(self._streams))]
+        side = torch.cuda.Stream(self.device)
+        side.wait_stream(torch.cuda.current_stream(self.device))
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=side):
+            self.launch(prepared, stream=side)
+        torch.cuda.current_stream(self.device).wait_stream(side)
+        return CapturedRun(g, prepared, self)
 
     def progress(self, t_max=1.0, MCsteps_max=4.0, **kwargs):
         """The reference's progress() for every instance at once; returns [(dt, dMCsteps)]."""
