@@ -296,7 +296,7 @@ def run_product(args):
     launch_ms = dev_ms / args.steps
     hbm, peak_kind = measured_peaks()
     achieved = alg / (launch_ms * 1e-3) / 1e9
-    cluster_sizes = sorted({p.cs for p in eng._prepare([1] * len(mms), [{}] * len(mms))})
+    cluster_sizes = sorted({p.cs for p in graph.prepared})
 
     # ---- energy error of the batch against an FP64 recompute ------------------------------
     # Only instances whose kernel is symmetric: with a pair of magnets exactly at the cutoff
