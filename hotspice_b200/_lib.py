@@ -33,7 +33,8 @@ class HsLattice(C.Structure):
         ('in_plane', C.c_int32), ('use_perp', C.c_int32), ('n_occ', C.c_int32), ('barrier_method', C.c_int32),
         ('has_dipolar', C.c_int32), ('dip_wx', C.c_int32), ('dip_wy', C.c_int32), ('dip_wrap', C.c_int32),
         ('n_sub', C.c_int32), ('has_exchange', C.c_int32), ('nn_h', C.c_int32), ('nn_w', C.c_int32),
-        ('trunc_cutoff', C.c_int32), ('trunc_size', C.c_int32), ('nn', C.c_int8 * 28),
+        ('trunc_cutoff', C.c_int32), ('trunc_size', C.c_int32), ('dip_keep_perp_sign', C.c_int32),
+        ('nn', C.c_int8 * 28),
     ]
 
 

@@ -29,7 +29,7 @@ import numpy as np
 import torch
 
 from . import _lib, config
-from .energies import DipolarEnergy, Energy, ExchangeEnergy, ZeemanEnergy
+from .energies import DiMonopolarEnergy, DipolarEnergy, Energy, ExchangeEnergy, ZeemanEnergy
 from .utils import as_2D_array, check_repetition, full_obj_name, lower_than
 
 __all__ = ['kB', 'SimParams', 'Magnets', 'Scheme', 'EngineConfig', 'Unitcell']
@@ -396,6 +396,8 @@ class Magnets(ABC):
         for e in self._energies:
             if isinstance(e, ZeemanEnergy):
                 e.set_field()
+            elif isinstance(e, DiMonopolarEnergy):
+                e._moment_changed()
         self._state_changed()
 
     @property
@@ -487,6 +489,10 @@ class Magnets(ABC):
 
     # energies -----------------------------------------------------------------------
     def add_energy(self, energy: Energy, exist_ok=False, verbose=True):
+        if isinstance(energy, DipolarEnergy) and any(isinstance(e, DipolarEnergy) and type(e) is not type(energy)
+                                                     for e in self._energies):
+            raise NotImplementedError('the sm_100a path holds one magnetostatic kernel per lattice: '
+                                      'DipolarEnergy and DiMonopolarEnergy cannot be combined')
         energy.initialize(self)
         for i, e in enumerate(self._energies):
             if type(e) is type(energy):
@@ -666,6 +672,7 @@ class Magnets(ABC):
             L.sub_of = d._sub_of.data_ptr()
             L.dip_wx, L.dip_wy, L.dip_wrap, L.n_sub = ks.wx, ks.wy, int(ks.wrap), ks.K.shape[0]
             L.dip_pref = float(d.prefactor)
+            L.dip_keep_perp_sign = int(d._keep_perp_sign)
         else:
             if not hasattr(self, '_sub_of_dummy'):
                 self._sub_of_dummy = torch.full((self.unitcell.x * self.unitcell.y,), -1, device=self.device, dtype=torch.int32)

@@ -9,6 +9,8 @@
 // back once. Semantics follow hotspice/energies.py:310-366:
 //   HS_UPDATE_SINGLE   E_j += 2 pref mm_j acc_j; then E_s = -E_s          (update_single)
 //   HS_UPDATE_MULTIPLE E_s = -E_s for every switch; E_j += 2 pref mm_j acc_j (update_multiple)
+// E_perp follows E, except that with L.dip_keep_perp_sign a list of more than one switch
+// leaves E_perp_s unnegated (DiMonopolarEnergy.update_multiple, hotspice/energies.py:718-719).
 // A switch in "truncated" mode (more than SIMULTANEOUS_SWITCHES_CONVOLUTION_OR_SUM_CUTOFF
 // switches on its sublattice, hotspice/energies.py:343-353) contributes only the
 // (2k+1)^2 crop of its kernel with wrap (PBC) or zero fill, like convolve2d(..., 'same').
@@ -50,6 +52,8 @@ dip_update_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev, int n_h
         for (int v = 0; v < VEC; ++v) { acc[r][v] = 0.f; accp[r][v] = 0.f; }
 
     const float pref2 = (float)(2.0 * L.dip_pref);
+    // a one-switch update is update_single in the reference (hotspice/core.py:250-253)
+    const bool flip_perp = !(L.dip_keep_perp_sign && nsw > 1);
     const bool vec_rows = VEC == 4 && x0 + 3 < L.nx && (L.nx & 3) == 0;
     for (int base = 0; base < nsw;) {
         // Stage, in list order, the switches of [base, ...) whose window reaches this tile. All
@@ -182,7 +186,7 @@ dip_update_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev, int n_h
             for (int v = 0; v < 4; ++v) {
                 const bool ng = (negate >> (r * VEC + v)) & 1u;
                 if (semantics == HS_UPDATE_MULTIPLE) {
-                    if (ng) { ev[v] = -ev[v]; pv[v] = -pv[v]; }
+                    if (ng) { ev[v] = -ev[v]; if (flip_perp) pv[v] = -pv[v]; }
                     ev[v] += (double)(pref2 * (mmv[v] * acc[r][v]));
                     pv[v] += (double)(pref2 * (mmv[v] * accp[r][v]));
                 } else {
@@ -211,7 +215,7 @@ dip_update_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev, int n_h
             L.E_dip[row + x] = e;
             if (L.use_perp) {
                 double p = L.E_dip_perp[row + x];
-                if (semantics == HS_UPDATE_MULTIPLE) { if (ng) p = -p; p += (double)(pref2 * (mmv * accp[r][v])); }
+                if (semantics == HS_UPDATE_MULTIPLE) { if (ng && flip_perp) p = -p; p += (double)(pref2 * (mmv * accp[r][v])); }
                 else { p += (double)(pref2 * (mmv * accp[r][v])); if (ng) p = -p; }
                 L.E_dip_perp[row + x] = p;
             }

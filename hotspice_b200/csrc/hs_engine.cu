@@ -158,6 +158,7 @@ HS_DEV void update_items(const HsLattice &L, const SwX *s_sw, const int *s_pre, 
     const int lane = threadIdx.x & 31;
     const float pref2 = (float)(2.0 * L.dip_pref);
     const bool vec = (L.nx & 3) == 0;
+    const bool flip_perp = !(L.dip_keep_perp_sign && nsw_total > 1);  // one switch: update_single
     int it0 = 0;
     for (int k = 0; k < n; ++k) {
         const SwX &wk = s_sw[k];
@@ -223,7 +224,7 @@ HS_DEV void update_items(const HsLattice &L, const SwX *s_sw, const int *s_pre, 
 #pragma unroll
                     for (int v = 0; v < 4; ++v) {
                         if (semantics == HS_UPDATE_MULTIPLE) {
-                            if (neg[v]) { ev[v] = -ev[v]; pv[v] = -pv[v]; }
+                            if (neg[v]) { ev[v] = -ev[v]; if (flip_perp) pv[v] = -pv[v]; }
                             ev[v] += (double)(pref2 * (mv[v] * acc[v]));
                             pv[v] += (double)(pref2 * (mv[v] * accp[v]));
                         } else {

@@ -22,7 +22,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .kernels import build_kernels
+from .kernels import build_dimonopolar_kernels, build_kernels
 
 
 class Energy:
@@ -172,9 +172,16 @@ class DipolarEnergy(Energy):
             self._initialize()
             self.update()
 
+    # DiMonopolarEnergy.update_multiple leaves E_perp of the switched magnets as it is
+    # (hotspice/energies.py:718-719); DipolarEnergy.update_multiple negates it (334).
+    _keep_perp_sign = False
+
     def _initialize(self):
+        self._install(build_kernels(self.mm, self._cutoff_range, self.decay_exponent))
+
+    def _install(self, ks):
+        """Upload the kernels of ``ks`` and allocate the FP64 energy accumulators."""
         mm = self.mm
-        ks = build_kernels(mm, self._cutoff_range, self.decay_exponent)
         self.kernel_set = ks
         dev = mm.device
         self._K = torch.as_tensor(ks.K, device=dev, dtype=torch.float32).contiguous()
@@ -236,6 +243,108 @@ class DipolarEnergy(Energy):
 
     def set_NN_interaction(self, value):
         self.prefactor = value / self.get_NN_interaction()
+
+
+class DiMonopolarEnergy(DipolarEnergy):
+    """Magnetostatic interaction with every magnet a pair of opposite magnetic charges
+    q = moment / d a distance d apart along its axis (hotspice/energies.py:394-751).
+
+    E_i = prefactor * q_i^2 * m_i * sum_j K_s(i)(j - i) m_j with the monopole-pair kernels of
+    :func:`hotspice_b200.kernels.build_dimonopolar_kernels`. For a uniform moment mu and
+    spacing d this is the dipolar update with the device field mm = m * mu and the kernels
+    scaled by q^2 / mu^2 = 1 / d^2, so the same sm_100a kernels (incremental update, direct
+    and tensor-core recompute, engine) run it unchanged. Two reference details are kept:
+    q^2 is fixed when the energy is initialised (a later change of the moment does not change
+    it, so the device kernels are rescaled by q^2 / mu_new^2), and an update of more than one
+    switch leaves E_perp of the switched magnets unnegated.
+
+    Supported: in-plane lattices (the reference reads ``original_angles``, which only in-plane
+    lattices have), a uniform moment on the occupied cells and a scalar (or uniform) ``d``;
+    anything else raises NotImplementedError."""
+
+    _keep_perp_sign = True
+
+    def __init__(self, prefactor=1, d=200e-9, small_d=200e-9):
+        self._prefactor = prefactor
+        self.d = d
+        self.small_d = small_d
+
+    @staticmethod
+    def _uniform(values, what):
+        v = np.asarray(values, dtype=float)
+        if v.size == 0 or not np.all(v == v.flat[0]):
+            raise NotImplementedError(f'DiMonopolarEnergy on the sm_100a path needs a uniform {what}')
+        return float(v.flat[0])
+
+    def _moment(self):
+        mm = self.mm
+        return self._uniform(np.asarray(mm._moment_np)[np.asarray(mm.occupation) != 0], 'moment')
+
+    def _initialize(self):
+        mm = self.mm
+        d = self._uniform(self.d, 'monopole spacing d')
+        mu = self._moment()
+        self._charge_sq = (mu / d) ** 2          # energies.py:414-415, fixed from here on
+        ks = build_dimonopolar_kernels(mm, d, self.small_d, scale=1.0)
+        self._K_phys = ks
+        self._mu_kernels = mu
+        self._install(self._scaled(ks, self._charge_sq / mu ** 2))
+
+    @staticmethod
+    def _scaled(ks, f):
+        from dataclasses import replace
+        return replace(ks, K=ks.K * f, Kps=ks.Kps * f, Kpo=ks.Kpo * f)
+
+    def _moment_changed(self):
+        """The magnets' moment changed: keep q^2 from the initialisation (as the reference
+        does) by rescaling the device kernels to q^2 / mu_new^2. The energies are not
+        recomputed (the reference's are not either)."""
+        mu = self._moment()
+        if mu == self._mu_kernels:
+            return
+        ks = self._scaled(self._K_phys, self._charge_sq / mu ** 2)
+        self.kernel_set = ks
+        dev = self.mm.device
+        self._K.copy_(torch.as_tensor(ks.K, device=dev, dtype=torch.float32))
+        if self._Kpo is not None:
+            self._Kpo.copy_(torch.as_tensor(ks.Kpo, device=dev, dtype=torch.float32))
+            self._Kps.copy_(torch.as_tensor(ks.Kps, device=dev, dtype=torch.float32))
+        self._mu_kernels = mu
+        self.mm._state_changed()
+
+    @property
+    def charge(self):
+        """q = moment / d [A m] (energies.py:414), as fixed at initialisation."""
+        return torch.full((self.mm.ny, self.mm.nx), math.sqrt(self._charge_sq), device=self.mm.device, dtype=torch.float64)
+
+    @property
+    def charge_sq(self):
+        return torch.full((self.mm.ny, self.mm.nx), self._charge_sq, device=self.mm.device, dtype=torch.float64)
+
+    @property
+    def kernel_unitcell(self):
+        """The monopole-pair kernels in J / (A m)^2 * m, as the reference stores them."""
+        return self._K_phys.K
+
+    @property
+    def kernel_perpself_unitcell(self):
+        return self._K_phys.Kps
+
+    @property
+    def kernel_perpother_unitcell(self):
+        return self._K_phys.Kpo
+
+    def get_NN_interaction(self):
+        """hotspice/energies.py:372-387 as inherited by the reference's DiMonopolarEnergy: the
+        largest nearest-neighbour kernel entry times prefactor * <moment>^2."""
+        ks = self._K_phys
+        NN = np.asarray(self.mm._get_nearest_neighbors())
+        hy, hx = NN.shape[0] // 2, NN.shape[1] // 2
+        largest = 0.0
+        for k in ks.K:
+            win = k[ks.wy - hy:ks.wy + hy + 1, ks.wx - hx:ks.wx + hx + 1]
+            largest = max(largest, float(np.max(np.abs(win * NN))))
+        return largest * self.prefactor * self.mm.moment_avg ** 2
 
 
 class ExchangeEnergy(Energy):

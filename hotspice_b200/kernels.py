@@ -1,4 +1,5 @@
-"""FP64 host construction of the dipolar interaction kernels and their device windows.
+"""FP64 host construction of the dipolar (and two-monopole) interaction kernels and their
+device windows.
 
 Restates DipolarEnergy._initialize (hotspice/energies.py:176-288): one kernel per occupied
 unit-cell site, K_s[d] for every offset d = (dy, dx) in [-(n-1), n-1]^2, built from the
@@ -185,3 +186,100 @@ def kernel_asymmetry(K, sub_of, nx, ny, center=None):
             worst = max(worst, float(np.max(np.abs(K[s] - other))))
     den = float(np.max(np.abs(K)))
     return worst / den if den > 0 else 0.0
+
+
+def _charge_axis(n, u, spacing):
+    """Positions of the big-grid columns -(n-1) .. n-1+u relative to column 0, accumulated from
+    the per-cell spacings as hotspice/energies.py:419-429 does (same summation order)."""
+    idx = np.arange(-(n - 1), n + u)
+    c = np.zeros(idx.size)
+    c[1:] = np.cumsum(np.asarray(spacing, dtype=float)[idx % n])[:-1]
+    return c - c[n - 1]
+
+
+def _inv_distances(ax, ay, cx, cy, f32):
+    """1/r between the charges (ax[i], ay[i]) of every window cell and the centre charges
+    (cx[j], cy[j]) for the pairs NN, SS, NS, SN (index 0 = north, 1 = south). The cross pairs
+    of the centre magnet with itself are excluded, coincident charges give 0 (r^2 = 0 is
+    replaced by infinity), and ``f32`` rounds r^2 to float32 first, as the reference does for
+    the parallel kernel (hotspice/energies.py:494-513)."""
+    H, W = ax[0].shape
+    out = []
+    for i, j in ((0, 0), (1, 1), (0, 1), (1, 0)):
+        ddx = ax[i] - cx[j]
+        ddy = ay[i] - cy[j]
+        if i != j:
+            ddx[H // 2, W // 2] = 0.0
+            ddy[H // 2, W // 2] = 0.0
+        r2 = ddx ** 2 + ddy ** 2
+        if f32:
+            r2 = r2.astype(np.float32)
+        r2[r2 == 0] = np.inf
+        out.append((r2 ** -0.5).astype(np.float64))
+    return out
+
+
+def build_dimonopolar_kernels(mm, d, small_d, scale=1.0) -> KernelSet:
+    """Kernels of the two-monopole (dumbbell) interaction, hotspice/energies.py:406-680.
+
+    Each magnet is a pair of charges +q, -q at +-d/2 along its original angle. The kernel of
+    unit-cell site s at offset o is 1e-7 * occ(s + o) * (1/r_NN + 1/r_SS - 1/r_NS - 1/r_SN)
+    between the magnet at o and the one at the centre; 'perp-self' turns the centre pair by
+    90 degrees with spacing ``small_d``, 'perp-other' turns every other pair instead. With PBC
+    the 8 neighbouring images are folded in, so the window is always the full lattice.
+    ``scale`` multiplies every entry (the energy class folds the charge factor 1/d^2 in, so
+    the device field stays m * moment). The distances are taken on each centre's window
+    only; every entry is computed by the same operations as in the reference's full grid."""
+    nx, ny = mm.nx, mm.ny
+    ux, uy = mm.unitcell.x, mm.unitcell.y
+    H, W = 2 * ny - 1, 2 * nx - 1
+    xl = _charge_axis(nx, ux, mm.dx)
+    yl = _charge_axis(ny, uy, mm.dy)
+    ang_uc = np.asarray(mm.original_angles, dtype=float)[:uy, :ux]
+    occ_uc = np.asarray(mm.occupation)[:uy, :ux]
+    sub_of = -np.ones((uy, ux), dtype=np.int32)
+    ks, kps, kpo = [], [], []
+    for yu in range(uy):
+        for xu in range(ux):
+            if occ_uc[yu, xu] == 0:
+                continue
+            # window of the centre magnet at big-grid (ny-1+yu, nx-1+xu): big rows yu .. yu+H-1
+            rows, cols = np.arange(yu, yu + H), np.arange(xu, xu + W)
+            XX, YY = np.meshgrid(xl[cols], yl[rows])
+            ang = ang_uc[((rows - (ny - 1)) % uy)[:, None], ((cols - (nx - 1)) % ux)[None, :]]
+            cos_a, sin_a = np.cos(ang), np.sin(ang)
+            cos_p, sin_p = np.cos(ang + np.pi / 2), np.sin(ang + np.pi / 2)
+            par_x = (XX + d / 2 * cos_a, XX - d / 2 * cos_a)
+            par_y = (YY + d / 2 * sin_a, YY - d / 2 * sin_a)
+            perp_x = (XX + small_d / 2 * cos_p, XX - small_d / 2 * cos_p)
+            perp_y = (YY + small_d / 2 * sin_p, YY - small_d / 2 * sin_p)
+            c = (ny - 1, nx - 1)
+            # parallel: every pair along its axis
+            r_par = _inv_distances(par_x, par_y, [a[c] for a in par_x], [a[c] for a in par_y], True)
+            # perp-self: the centre pair turned (spacing small_d)
+            sx, sy = [a.copy() for a in par_x], [a.copy() for a in par_y]
+            for k in (0, 1):
+                sx[k][c], sy[k][c] = perp_x[k][c], perp_y[k][c]
+            r_ps = _inv_distances(sx, sy, [a[c] for a in sx], [a[c] for a in sy], False)
+            # perp-other: every pair but the centre one turned
+            ox, oy = [a.copy() for a in perp_x], [a.copy() for a in perp_y]
+            for k in (0, 1):
+                ox[k][c], oy[k][c] = par_x[k][c], par_y[k][c]
+            r_po = _inv_distances(ox, oy, [a[c] for a in ox], [a[c] for a in oy], False)
+            sy0 = (uy - ((ny - 1) % uy) + yu) % uy
+            sx0 = (ux - ((nx - 1) % ux) + xu) % ux
+            occ = occ_uc[((sy0 + np.arange(H)) % uy)[:, None], ((sx0 + np.arange(W)) % ux)[None, :]].astype(np.float64)
+            out = []
+            for r in (r_par, r_ps, r_po):
+                k = r[0] * occ + r[1] * occ + (-r[2] * occ) + (-r[3] * occ)
+                if mm.PBC:
+                    _fold(k, nx, ny)
+                k *= 1e-7  # mu0 / 4 pi
+                out.append(k * scale)
+            sub_of[yu, xu] = len(ks)
+            ks.append(out[0]); kps.append(out[1]); kpo.append(out[2])
+    if not ks:
+        raise ValueError('no occupied unit-cell site: nothing to build a monopole kernel for')
+    K, Kps, Kpo = np.asarray(ks), np.asarray(kps), np.asarray(kpo)
+    asym = kernel_asymmetry(K, sub_of, nx, ny)
+    return KernelSet(K, Kps, Kpo, sub_of, nx - 1, ny - 1, False, True, asym)

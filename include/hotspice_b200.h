@@ -103,6 +103,9 @@ typedef struct HsLattice {
     int32_t nn_h, nn_w;         /* exchange nearest-neighbour mask size (odd, <= 5x5)        */
     int32_t trunc_cutoff;       /* SIMULTANEOUS_SWITCHES_CONVOLUTION_OR_SUM_CUTOFF           */
     int32_t trunc_size;         /* REDUCED_KERNEL_SIZE                                       */
+    int32_t dip_keep_perp_sign; /* 1: HS_UPDATE_MULTIPLE leaves E_dip_perp of the switched cells
+                                   unnegated (DiMonopolarEnergy.update_multiple,
+                                   hotspice/energies.py:718-719); 0: negated (DipolarEnergy)   */
     int8_t  nn[28];             /* nearest-neighbour mask, row-major                         */
 } HsLattice;
 

@@ -150,11 +150,21 @@ class OracleDipolar(OracleEnergy):
         self.kernels, self.kernels_perpself, self.kernels_perpother, self.kernel_index = \
             build_dipolar_kernels(self.mm, self.cutoff_range, self.decay_exponent)
 
+    flip_perp_multiple = True   # update_multiple negates E_perp of the switched magnets
+
+    # The interaction of a source magnet s with a target j is pref * src_s * m_j * tgt_j * K(j - s):
+    # src = m * moment and tgt = moment for dipoles.
+    def _src(self):
+        return self.mm.m * self.mm.moment
+
+    def _tgt(self):
+        return self.mm.moment
+
     def update(self):
         """hotspice/energies.py:290-308 (FFT convolution instead of direct)."""
         mm = self.mm
         ux, uy = mm.unitcell
-        mmom = mm.m * mm.moment
+        mmom = self._src()
         tot = np.zeros_like(mm.m)
         totp = np.zeros_like(mm.m)
         for y in range(uy):
@@ -167,9 +177,9 @@ class OracleDipolar(OracleEnergy):
                 tot += pm * signal.fftconvolve(self.kernels[n, ::-1, ::-1], mmom, mode='valid')
                 if mm.USE_PERP_ENERGY:
                     totp += pm * signal.fftconvolve(self.kernels_perpself[n, ::-1, ::-1], mmom, mode='valid')
-        self.E = self.prefactor * mm.moment * tot
+        self.E = self.prefactor * self._tgt() * tot
         if mm.USE_PERP_ENERGY:
-            self.E_perp = self.prefactor * mm.moment * totp
+            self.E_perp = self.prefactor * self._tgt() * totp
 
     def _window(self, k, y, x):
         ny, nx = self.mm.ny, self.mm.nx
@@ -183,11 +193,11 @@ class OracleDipolar(OracleEnergy):
         n = self.kernel_index[y % uy, x % ux]
         if n < 0:
             return
-        mmom = mm.m * mm.moment
-        self.E += 2 * (self.prefactor * mmom[y, x] * (mmom * self._window(self.kernels[n], y, x)))
+        src, tm = self._src(), mm.m * self._tgt()
+        self.E += 2 * (self.prefactor * src[y, x] * (tm * self._window(self.kernels[n], y, x)))
         self.E[y, x] *= -1
         if mm.USE_PERP_ENERGY:
-            self.E_perp += 2 * (self.prefactor * mmom[y, x] * (mmom * self._window(self.kernels_perpother[n], y, x)))
+            self.E_perp += 2 * (self.prefactor * src[y, x] * (tm * self._window(self.kernels_perpother[n], y, x)))
             self.E_perp[y, x] *= -1
 
     def update_multiple(self, idx):
@@ -197,8 +207,9 @@ class OracleDipolar(OracleEnergy):
         mm = self.mm
         perp = mm.USE_PERP_ENERGY
         self.E[idx[0], idx[1]] *= -1
-        mmom = mm.m * mm.moment
-        if perp:
+        mmom = self._src()
+        tm = mm.m * self._tgt()
+        if perp and self.flip_perp_multiple:
             self.E_perp[idx[0], idx[1]] *= -1
         ux, uy = mm.unitcell
         sub = (idx[1] % ux) + (idx[0] % uy) * ux
@@ -223,9 +234,9 @@ class OracleDipolar(OracleEnergy):
                     conv += mmom[y, x] * self._window(K, y, x)
                     if perp:
                         convp += mmom[y, x] * self._window(Kp, y, x)
-            self.E += 2 * (self.prefactor * (mmom * conv))
+            self.E += 2 * (self.prefactor * (tm * conv))
             if perp:
-                self.E_perp += 2 * (self.prefactor * (mmom * convp))
+                self.E_perp += 2 * (self.prefactor * (tm * convp))
 
     @property
     def E_tot(self):
@@ -257,6 +268,124 @@ def truncated_window_sum(mm, here, mmom, K):
             oky, okx = (ty >= 0) & (ty < ny), (tx >= 0) & (tx < nx)
             out[np.ix_(ty[oky], tx[okx])] += w[np.ix_(oky, okx)]
     return out
+
+
+class OracleDiMonopolar(OracleDipolar):
+    """hotspice/energies.py:394-751: every magnet is a pair of opposite magnetic charges
+    q = moment / d a distance d apart along its axis; the kernel sums the four charge-charge
+    terms. Targets carry q^2 and sources their bare spin (update: energies.py:684-697,
+    update_single: 699-716, update_multiple: 718-751)."""
+    shortname = 'dimonopolar'
+    flip_perp_multiple = False  # energies.py:718-719 negates E only
+
+    def __init__(self, prefactor=1.0, d=200e-9, small_d=200e-9):
+        super().__init__(prefactor=prefactor)
+        self.d = d
+        self.small_d = small_d
+
+    def _initialize(self):
+        mm = self.mm
+        ux, uy = mm.unitcell
+        dist_uc = np.broadcast_to(np.asarray(self.d, dtype=float), (uy, ux))
+        dist = np.tile(dist_uc, (math.ceil(mm.ny / uy), math.ceil(mm.nx / ux)))[:mm.ny, :mm.nx]
+        self.charge_sq = (mm.moment / dist) ** 2
+        self.kernels, self.kernels_perpself, self.kernels_perpother, self.kernel_index = \
+            build_dimonopolar_kernels(mm, self.d, self.small_d)
+
+    def _src(self):
+        return self.mm.m
+
+    def _tgt(self):
+        return self.charge_sq
+
+
+def build_dimonopolar_kernels(mm, d, small_d):
+    """Monopole-pair kernels, one per occupied unit-cell site (hotspice/energies.py:406-680).
+
+    Charges sit at +-d/2 along each magnet's original angle, on a grid of offsets from
+    -(n-1) to n-1+u built from the cumulative cell spacings. For the magnet at the kernel's
+    centre the kernel is sum of 1/r over its N-N and S-S pairs minus its N-S and S-N pairs
+    with every other magnet (the squared distances rounded to float32, as the reference
+    does), masked by the occupation; 'perp-self' rotates the centre magnet's pair by 90 deg
+    with spacing small_d, 'perp-other' rotates every other magnet's. PBC folds in the 8
+    neighbouring images; the result is scaled by mu0 / 4 pi = 1e-7."""
+    nx, ny = mm.nx, mm.ny
+    ux, uy = mm.unitcell
+    scalar_d = np.ndim(d) == 0
+    dist_uc = np.broadcast_to(np.asarray(d, dtype=float), (uy, ux))
+
+    def axis(n, u, spacing):
+        idx = np.arange(-(n - 1), n + u)
+        c = np.zeros(idx.size)
+        c[1:] = np.cumsum(np.asarray(spacing, dtype=float)[idx % n])[:-1]
+        return c - c[n - 1]
+    XX, YY = np.meshgrid(axis(nx, ux, mm.dx), axis(ny, uy, mm.dy))
+    ry = (np.arange(XX.shape[0]) - (ny - 1)) % uy
+    rx = (np.arange(XX.shape[1]) - (nx - 1)) % ux
+    dist = np.full(XX.shape, float(d)) if scalar_d else dist_uc[ry[:, None], rx[None, :]]
+    # the reference reads original_angles; the geometry's angles differ from them only on
+    # unoccupied cells, whose kernel entries the occupation mask zeroes
+    ang = mm.geom.angles[:uy, :ux][ry[:, None], rx[None, :]]
+    cN_x, cS_x = XX + dist / 2 * np.cos(ang), XX - dist / 2 * np.cos(ang)
+    cN_y, cS_y = YY + dist / 2 * np.sin(ang), YY - dist / 2 * np.sin(ang)
+    rot = ang + np.pi / 2
+    pN_x, pS_x = XX + small_d / 2 * np.cos(rot), XX - small_d / 2 * np.cos(rot)
+    pN_y, pS_y = YY + small_d / 2 * np.sin(rot), YY - small_d / 2 * np.sin(rot)
+
+    def rinv4(ax, ay, bx, by, y, x, f32):
+        """1/r of NN, SS, NS, SN between the charges (ax, ay) of every magnet and the centre
+        magnet (y, x) with charges (bx, by); index 0 = N, 1 = S."""
+        out = []
+        for i, j in ((0, 0), (1, 1), (0, 1), (1, 0)):
+            dx_ = ax[i] - bx[j][y, x]
+            dy_ = ay[i] - by[j][y, x]
+            if i != j:
+                dx_ = dx_.copy(); dy_ = dy_.copy()
+                dx_[y, x] = 0.0; dy_[y, x] = 0.0
+            r2 = dx_ ** 2 + dy_ ** 2
+            if f32:
+                r2 = r2.astype(np.float32)
+            r2[r2 == 0] = np.inf
+            out.append((r2 ** -0.5).astype(np.float64)[y - ny + 1:y + ny, x - nx + 1:x + nx])
+        return out
+
+    rinv, rinv_ps, rinv_po = [], [], []
+    for y in range(ny - 1, ny - 1 + uy):
+        for x in range(nx - 1, nx - 1 + ux):
+            rinv.append(rinv4((cN_x, cS_x), (cN_y, cS_y), (cN_x, cS_x), (cN_y, cS_y), y, x, True))
+            # centre magnet rotated
+            sx = [cN_x.copy(), cS_x.copy()]; sy = [cN_y.copy(), cS_y.copy()]
+            sx[0][y, x], sx[1][y, x] = pN_x[y, x], pS_x[y, x]
+            sy[0][y, x], sy[1][y, x] = pN_y[y, x], pS_y[y, x]
+            rinv_ps.append(rinv4(sx, sy, sx, sy, y, x, False))
+            # every other magnet rotated
+            ox = [pN_x.copy(), pS_x.copy()]; oy = [pN_y.copy(), pS_y.copy()]
+            ox[0][y, x], ox[1][y, x] = cN_x[y, x], cS_x[y, x]
+            oy[0][y, x], oy[1][y, x] = cN_y[y, x], cS_y[y, x]
+            rinv_po.append(rinv4(ox, oy, ox, oy, y, x, False))
+    occ_uc = mm.occupation[:uy, :ux]
+    big = np.tile(occ_uc, (2 * math.ceil(ny / uy) + 1, 2 * math.ceil(nx / ux) + 1))
+    index = -np.ones((uy, ux), dtype=int)
+    Ks, Kps, Kpo = [], [], []
+    n = 0
+    for yu in range(uy):
+        for xu in range(ux):
+            if occ_uc[yu, xu] == 0:
+                n += 1
+                continue
+            sx0 = (ux - ((nx - 1) % ux) + xu) % ux
+            sy0 = (uy - ((ny - 1) % uy) + yu) % uy
+            occ = big[sy0:sy0 + 2 * ny - 1, sx0:sx0 + 2 * nx - 1]
+            ks = []
+            for r in (rinv[n], rinv_ps[n], rinv_po[n]):
+                k = r[0] * occ + r[1] * occ + (-r[2] * occ) + (-r[3] * occ)
+                if mm.PBC:
+                    fold_periodic_images(k, nx, ny)
+                ks.append(k * 1e-7)
+            n += 1
+            index[yu, xu] = len(Ks)
+            Ks.append(ks[0]); Kps.append(ks[1]); Kpo.append(ks[2])
+    return np.asarray(Ks), np.asarray(Kps), np.asarray(Kpo), index
 
 
 def build_dipolar_kernels(mm, cutoff_range=np.inf, decay_exponent=-3):

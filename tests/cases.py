@@ -36,11 +36,13 @@ def oracle_geometry(spec):
 
 
 def oracle_energies(spec):
-    from oracle.hotspice_oracle import OracleDipolar, OracleExchange, OracleZeeman
+    from oracle.hotspice_oracle import OracleDiMonopolar, OracleDipolar, OracleExchange, OracleZeeman
     out = []
     for e in spec['energies']:
         if e['type'] == 'dipolar':
             out.append(OracleDipolar(cutoff_range=e.get('cutoff', np.inf)))
+        elif e['type'] == 'dimonopolar':
+            out.append(OracleDiMonopolar(e.get('prefactor', 1.0), e['d'], e['small_d']))
         elif e['type'] == 'zeeman':
             out.append(OracleZeeman(e['B'], e.get('angle', 0.0)))
         elif e['type'] == 'exchange':
@@ -59,6 +61,15 @@ def build_oracle(name, spec=None, fx=None, **over):
               PBC=spec.get('kw', {}).get('PBC', False), params=params, seed=spec['seed'])
     kw.update(over)
     return OracleMagnets(g, fx['m0'], **kw)
+
+
+def dipolar_like(mm):
+    """The DipolarEnergy or DiMonopolarEnergy of an instance (oracle or product), or None."""
+    for name in ('dipolar', 'dimonopolar'):
+        for e in getattr(mm, 'energies', None) or getattr(mm, '_energies', ()):
+            if e.shortname == name:
+                return e
+    return None
 
 
 def rel_err(a, b):

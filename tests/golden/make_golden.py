@@ -109,6 +109,8 @@ def run_spec(hs, spec):
     for e in spec['energies']:
         if e['type'] == 'dipolar':
             energies.append(E.DipolarEnergy(cutoff_range=e.get('cutoff', np.inf)))
+        elif e['type'] == 'dimonopolar':
+            energies.append(E.DiMonopolarEnergy(prefactor=e.get('prefactor', 1.0), d=e['d'], small_d=e['small_d']))
         elif e['type'] == 'zeeman':
             energies.append(E.ZeemanEnergy(magnitude=e['B'], angle=e.get('angle', 0.0)))
         elif e['type'] == 'exchange':
@@ -129,7 +131,7 @@ def run_spec(hs, spec):
     route_rng(mm, stream)
     rec = dict(m0=m0, E_B=np.asarray(EB, dtype=float) * np.ones((ny, nx)), occupation=mm.occupation,
                unitcell=np.array([mm.unitcell.x, mm.unitcell.y]), PBC=np.array(mm.PBC))
-    dip = mm.get_energy('dipolar')
+    dip = mm.get_energy('dipolar', verbose=False) or mm.get_energy('dimonopolar', verbose=False)
     if dip is not None:
         rec['kernels'] = dip.kernel_unitcell
         rec['kernels_perpself'] = dip.kernel_perpself_unitcell
@@ -212,8 +214,18 @@ SPECS = {
                            progress=dict(t_max=1e-3, MCsteps_max=0.5)),
     'progress_pin16_metro': dict(BASE_PIN, nx=16, ny=16, seed=52, energies=[dict(type='dipolar', cutoff=1.2e-6)], steps=0,
                                  params=dict(UPDATE_SCHEME='Metropolis'), progress=dict(t_max=1.0, MCsteps_max=3.0, r=900e-9)),
+    # DiMonopolarEnergy (two opposite charges per magnet): two-channel Néel with E_perp
+    'neel_pin16_dimono': dict(BASE_PIN, nx=16, ny=16, seed=61,
+                              energies=[dict(type='dimonopolar', d=120e-9, small_d=60e-9),
+                                        dict(type='zeeman', B=1e-3, angle=math.radians(22.5))], steps=150),
+    'neel_kagome_dimono': dict(BASE_PIN, lattice='IP_Kagome', a=1e-6, nx=12, ny=11, seed=62,
+                               energies=[dict(type='dimonopolar', prefactor=0.7, d=400e-9, small_d=150e-9)], steps=100),
+    # multi-switch updates (E_perp keeps its sign there) and METROPOLIS_TIME barriers from E_perp
+    'metro_sq16_dimono_pbc': dict(BASE_PIN, lattice='IP_Square', a=400e-9, nx=16, ny=16, seed=63, kw=dict(PBC=True),
+                                  T=1500.0, energies=[dict(type='dimonopolar', d=150e-9, small_d=70e-9)], steps=60,
+                                  params=dict(METROPOLIS_TIME=True), update_kw=dict(r=600e-9)),
 }
-for name in ('metro_pin32_grid', 'metro_pin24_pbc', 'metro_oop32_trunc_pbc', 'metro_oop30_trunc',
+for name in ('metro_sq16_dimono_pbc', 'metro_pin32_grid', 'metro_pin24_pbc', 'metro_oop32_trunc_pbc', 'metro_oop30_trunc',
              'metro_oop16_time', 'metro_kagome_grid', 'metro_oop16_single'):
     SPECS[name].setdefault('params', {})['UPDATE_SCHEME'] = 'Metropolis'
 
@@ -245,12 +257,13 @@ def hexagon_kat(hs):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--ref', default='/root/reference')
-    ap.add_argument('--only', default=None)
+    ap.add_argument('--only', default=None, help='comma-separated scenario names; merged into specs.json')
     args = ap.parse_args()
     hs = load_reference(args.ref)
+    only = set(args.only.split(',')) if args.only else None
     meta = {}
     for name, spec in SPECS.items():
-        if args.only and name != args.only:
+        if only and name not in only:
             continue
         spec = dict(spec)
         if spec['T'] == 'field':
@@ -262,7 +275,13 @@ def main():
         meta[name] = jspec
         print(f'{name}: steps={spec.get("steps", 0)} switches={int(rec["switches"][-1]) if len(rec["switches"]) else 0} '
               f'calls={int(rec["calls"][-1]) if len(rec["calls"]) else 0}')
-    if not args.only:
+    if only:
+        with open(os.path.join(HERE, 'specs.json')) as f:
+            merged = json.load(f)
+        merged.update(meta)
+        with open(os.path.join(HERE, 'specs.json'), 'w') as f:
+            json.dump(merged, f, indent=1, default=float)
+    else:
         hex_cases, E_theory = hexagon_kat(hs)
         np.savez_compressed(os.path.join(HERE, 'hexagon_kat.npz'), E_theory=E_theory,
                             **{f'{k}_{i}': v[i] for k, v in hex_cases.items() for i in range(3)})

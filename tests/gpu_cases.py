@@ -20,6 +20,8 @@ def build_product(name, spec=None, fx=None, engine=None, **over):
             energies.append(hs.ZeemanEnergy(e['B'], e.get('angle', 0.0)))
         elif e['type'] == 'exchange':
             energies.append(hs.ExchangeEnergy(e['J']))
+        elif e['type'] == 'dimonopolar':
+            energies.append(hs.DiMonopolarEnergy(e.get('prefactor', 1.0), e['d'], e['small_d']))
     params = dict(spec.get('params', {}))
     kw = dict(T=fx['T'], E_B=fx['E_B'], moment=spec['moment'], pattern=fx['m0'], energies=energies,
               params=hs.SimParams(**params), PBC=spec.get('kw', {}).get('PBC', False), seed=spec['seed'],

@@ -3,7 +3,7 @@ size, and identical results for an instance run alone or inside a mixed batch.""
 import numpy as np
 import pytest
 
-from cases import load_specs
+from cases import dipolar_like, load_specs
 from gpu_cases import build_product
 
 pytestmark = pytest.mark.gpu
@@ -11,7 +11,7 @@ SPECS = load_specs()
 
 
 def _state(mm):
-    d = mm.get_energy('dipolar', verbose=False)
+    d = dipolar_like(mm)
     c = mm._read_counters()
     return (mm._m_dev.cpu().numpy(), None if d is None else d._E.cpu().numpy(),
             None if d is None or d._Ep is None else d._Ep.cpu().numpy(),
@@ -28,7 +28,8 @@ def _assert_same(a, b, what):
 
 STEP_CASES = ['neel_oop16', 'neel_oop12x9_pbc', 'neel_oop16_Tfield', 'neel_pin16_perp', 'neel_kagome_perp',
               'neel_oop16_exchange', 'metro_pin32_grid', 'metro_pin24_pbc', 'metro_oop32_trunc_pbc',
-              'metro_oop30_trunc', 'metro_oop16_time', 'metro_kagome_grid', 'metro_oop16_single', 'wolff_oop32_pbc']
+              'metro_oop30_trunc', 'metro_oop16_time', 'metro_kagome_grid', 'metro_oop16_single', 'wolff_oop32_pbc',
+              'neel_pin16_dimono', 'neel_kagome_dimono', 'metro_sq16_dimono_pbc']
 
 
 @pytest.mark.parametrize('name', STEP_CASES)

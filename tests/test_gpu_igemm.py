@@ -18,14 +18,14 @@ TOL = {3: 1e-6,      # 3 BF16 splits (the default): FP64 near field, FP32 chunks
 TOL_SPLIT1 = 1e-2    # plain BF16 kernel (8-bit significand)
 
 
-def _make(kind, n, ny=None, PBC=False, seed=5):
+def _make(kind, n, ny=None, PBC=False, seed=5, monopoles=False):
     import hotspice_b200 as hs
     cls = {'oop': hs.ASI.OOP_Square, 'pin': hs.ASI.IP_Pinwheel, 'kag': hs.ASI.IP_Kagome,
            'sq': hs.ASI.IP_Square}[kind]
     a = {'oop': 200e-9, 'pin': 300e-9, 'kag': 500e-9, 'sq': 300e-9}[kind]
     kw = dict(nx=n, ny=ny) if ny is not None else dict(n=n)
     mm = cls(a, **kw, T=300, E_B=5e-20, moment=1e-15, pattern='random', PBC=PBC, seed=seed,
-             energies=[hs.DipolarEnergy()])
+             energies=[hs.DiMonopolarEnergy(d=0.4 * a, small_d=0.15 * a) if monopoles else hs.DipolarEnergy()])
     return mm
 
 
@@ -62,6 +62,15 @@ def test_igemm_matches_fp64(kind, n, ny, PBC, nsplit):
     print(f'{kind} {mm.nx}x{mm.ny} PBC={PBC} nsplit={nsplit}: rel err {err:.2e} perp {errp:.2e}')
     assert err <= TOL[nsplit]
     assert errp <= TOL[nsplit]
+
+
+@pytest.mark.parametrize('kind,n,PBC', [('pin', 96, False), ('kag', 40, True), ('sq', 130, False)])
+def test_igemm_monopole_kernels(kind, n, PBC):
+    """DiMonopolarEnergy runs through the same GEMM (kernels scaled by 1/d^2)."""
+    mm = _make(kind, n, PBC=PBC, monopoles=True)
+    err, errp = _compare(mm, 3)
+    print(f'monopoles {kind} {mm.nx}x{mm.ny} PBC={PBC}: rel err {err:.2e} perp {errp:.2e}')
+    assert err <= TOL[3] and errp <= TOL[3]
 
 
 def test_igemm_split_levels():

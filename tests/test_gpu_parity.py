@@ -12,7 +12,7 @@ Tolerances (stated by the build's precision design):
 import numpy as np
 import pytest
 
-from cases import build_oracle, load_fixture, load_specs, rel_err
+from cases import build_oracle, dipolar_like, load_fixture, load_specs, rel_err
 from gpu_cases import build_product
 
 pytestmark = pytest.mark.gpu
@@ -39,11 +39,11 @@ def test_philox_device_matches_numpy():
         assert np.array_equal(_np(out), uniform53(seed, call, n))
 
 
-@pytest.mark.parametrize('name', [n for n in SPECS if any(e['type'] == 'dipolar' for e in SPECS[n]['energies'])])
+@pytest.mark.parametrize('name', [n for n in SPECS if any(e['type'] in ('dipolar', 'dimonopolar') for e in SPECS[n]['energies'])])
 def test_full_recompute_matches_oracle(name):
     fx = load_fixture(name)
     mp = build_product(name)
-    d = mp.get_energy('dipolar')
+    d = dipolar_like(mp)
     assert rel_err(_np(d.E), fx['E_dip_init']) < 1e-6
     if mp.USE_PERP_ENERGY:
         assert rel_err(_np(d.E_perp), fx['E_dip_perp_init']) < 1e-6
@@ -60,6 +60,14 @@ def _near_neel(mo, keys, i_dev, i_or, beta_max):
     Emax = np.max(np.abs(mo.E))
     tol = 2 * 2 * 2 * E_TOL * Emax * beta_max + 1e-9
     return keys[i_dev] - keys[i_or] <= tol
+
+
+def _check_perp(mp, mo):
+    """The magnetostatic E_perp after the run (its sign at switched magnets differs between
+    DipolarEnergy and DiMonopolarEnergy multi-switch updates)."""
+    dp, do = dipolar_like(mp), dipolar_like(mo)
+    if dp is not None and mp.USE_PERP_ENERGY:
+        assert rel_err(_np(dp.E_perp), do.E_perp) < 2 * E_TOL
 
 
 @pytest.mark.parametrize('name', [n for n in SPECS if _scheme(SPECS[n]) in ('Neel',) and SPECS[n].get('steps')])
@@ -88,6 +96,7 @@ def test_neel_lockstep(name):
     assert mp.switches == mo.switches
     assert np.array_equal(_np(mp.m), mo.m)
     assert rel_err(_np(mp.E), mo.E) < 2 * E_TOL
+    _check_perp(mp, mo)
     assert mp.t == pytest.approx(mo.t, rel=2e-2)
     print(f'{name}: {spec["steps"]} steps, {near} near-threshold decisions')
 
@@ -120,6 +129,7 @@ def test_metropolis_lockstep(name):
     assert mp.switches == mo.switches
     assert np.array_equal(_np(mp.m), mo.m)
     assert rel_err(_np(mp.E), mo.E) < 2 * E_TOL
+    _check_perp(mp, mo)
     if spec.get('params', {}).get('METROPOLIS_TIME'):
         assert mp.t == pytest.approx(mo.t, rel=2e-2)
     print(f'{name}: {spec["steps"]} steps, {near} near-threshold acceptances')

@@ -53,6 +53,26 @@ def test_kernel_windows_match_reference(name):
         assert ks.wy < mm.ny - 1 or ks.wx < mm.nx - 1 or not ks.wrap
 
 
+@pytest.mark.parametrize('name', [n for n in SPECS if any(e['type'] == 'dimonopolar' for e in SPECS[n]['energies'])])
+def test_dimonopolar_kernels_match_reference(name):
+    """The monopole-pair kernels (built on each centre's window) against the reference's
+    full-grid construction; unoccupied cells carry angle 0 in the geometry, which the
+    occupation mask makes irrelevant."""
+    from hotspice_b200.kernels import build_dimonopolar_kernels
+    spec, fx = SPECS[name], load_fixture(name)
+    mm = _mock(spec, fx)
+    mm.original_angles = oracle_geometry(spec).angles
+    e = [e for e in spec['energies'] if e['type'] == 'dimonopolar'][0]
+    ks = build_dimonopolar_kernels(mm, e['d'], e['small_d'])
+    assert np.array_equal(ks.sub_of, fx['kernel_index'])
+    assert ks.full and not ks.wrap and (ks.wy, ks.wx) == (mm.ny - 1, mm.nx - 1)
+    for win, ref in ((ks.K, fx['kernels']), (ks.Kps, fx['kernels_perpself']), (ks.Kpo, fx['kernels_perpother'])):
+        assert win.shape == ref.shape
+        assert rel_err(win, ref) < 1e-15, name
+    scaled = build_dimonopolar_kernels(mm, e['d'], e['small_d'], scale=1 / e['d'] ** 2)
+    assert rel_err(scaled.K * e['d'] ** 2, fx['kernels']) < 1e-15
+
+
 @pytest.mark.parametrize('kind,n,PBC,cut_a', [('oop', 40, False, 6), ('oop', 40, True, 6), ('pin', 48, False, 8),
                                               ('pin', 48, True, 8), ('kag', 40, False, 3), ('kag', 44, True, 3)])
 def test_windowed_kernels_equal_full_construction(kind, n, PBC, cut_a):
