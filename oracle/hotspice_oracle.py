@@ -663,6 +663,78 @@ class OracleMagnets:
         self.update_energy(c)
         return c
 
+    # -- relaxation ----------------------------------------------------------------------
+    def minimize(self, ignore_barrier=True, _frac=0.3):
+        """hotspice/core.py:763-797: switch, one at a time, the magnet with the most energy to
+        gain; when some magnets gain more than kBT, switch a random ceil(frac n) of those n at
+        once. Stops when no switch lowers the energy, or a magnet was picked a third time.
+        Only ``ignore_barrier=True`` is restated: with False the reference compares the
+        (barrier, barrier) tuple that E_barrier() returns."""
+        if not ignore_barrier:
+            raise NotImplementedError('minimize(ignore_barrier=False) indexes a (barrier, barrier) tuple')
+        visited = np.zeros_like(self.m)
+        while True:
+            barrier = self.switch_energy()
+            nob = np.where(barrier < -self.kBT)
+            n = nob[0].size
+            if n != 0:
+                rand = self.rng.choice(n, size=math.ceil(n * _frac), replace=False)
+                idx = (nob[0][rand], nob[1][rand])
+            else:
+                idx = divmod(int(np.argmin(barrier)), self.nx)
+                if barrier[idx] >= 0:
+                    break
+                visited[idx] += 1
+                if np.any(visited[idx] >= 3):
+                    break
+            idx = np.asarray(idx).reshape(2, -1)
+            self.m[idx[0], idx[1]] *= -1
+            self.switches += idx.shape[1]
+            self.attempted_switches += idx.shape[1]
+            self.update_energy(idx)
+
+    def minimize_all(self, ignore_barrier=True, _simultaneous=False, decide=None):
+        """hotspice/core.py:799-825: in a random order of the (2 ux) x (2 uy) subgrids (one
+        subgrid when simultaneous), switch every magnet of the subgrid whose switch lowers the
+        energy (or, with ignore_barrier False, whose switch_energy/2 + E_B < 0).
+        ``decide(subset, mask)`` may replace the mask (lock-step tests)."""
+        ux, uy = self.unitcell
+        sx, sy = (1, 1) if _simultaneous else (2 * ux, 2 * uy)
+        order = self.rng.permutation(sx * sy)
+        for i in order:
+            y, x = divmod(int(i), sx)
+            if not self.occupation[y, x]:
+                continue
+            sub = np.asarray(np.meshgrid(np.arange(y, self.ny, sy), np.arange(x, self.nx, sx))).reshape(2, -1)
+            dE = self.switch_energy(sub)
+            mask = dE < 0 if ignore_barrier else dE / 2 + self.E_B[sub[0], sub[1]] < 0
+            if decide is not None:
+                mask = decide(sub, mask, dE)
+            sel = sub[:, mask]
+            if sel.size > 0:
+                self.m[sel[0], sel[1]] = -self.m[sel[0], sel[1]]
+                self.switches += sel.shape[1]
+                self.attempted_switches += sel.shape[1]
+                self.update_energy(sel)
+
+    def relax(self, **kwargs):
+        """hotspice/core.py:827-861: repeated minimize_all sweeps until a sweep switches
+        nothing, the state equals the one two sweeps before (a 2-cycle), or
+        int(sqrt(nx^2 + ny^2)) sweeps were made. Returns the number of sweeps."""
+        n, n_max = 0, int(math.sqrt(self.nx ** 2 + self.ny ** 2))
+        prev = [self.m.copy(), np.zeros_like(self.m), np.zeros_like(self.m)]
+        switches = self.switches
+        while not np.allclose(prev[2], prev[0]) and n < n_max:
+            n += 1
+            self.minimize_all(**kwargs)
+            if switches == self.switches:
+                break
+            switches = self.switches
+            prev[2] = prev[1].copy()
+            prev[1] = prev[0].copy()
+            prev[0] = self.m.copy()
+        return n
+
     def calc_r(self, Q):
         """hotspice/core.py:720-733."""
         r = (8e-7 * self.moment ** 2 / (Q * self.kBT)) ** (1 / 3)

@@ -68,6 +68,8 @@ class PhiloxStream:
       integers(lo, hi, size)  -> lo + floor(u * (hi - lo))
       randint                 -> integers
       choice(n, size)         -> floor(u * n)
+      choice(n, size, replace=False) -> the first `size` of argsort(u over n elements, stable)
+      permutation(n)          -> argsort(u over n elements, stable)
     """
 
     def __init__(self, seed: int, call: int = 0):
@@ -114,9 +116,22 @@ class PhiloxStream:
     def choice(self, a, size=None, replace=True, p=None):
         if not np.isscalar(a):
             raise NotImplementedError("PhiloxStream.choice only supports an integer population")
+        if not replace:
+            k = 1 if size is None else int(np.prod(size))
+            if k > int(a):
+                raise ValueError("Cannot take a larger sample than population when 'replace=False'")
+            u, _ = self._draw(int(a), 'choice')
+            r = np.argsort(np.atleast_1d(u), kind='stable')[:k]
+            return int(r[0]) if size is None else r.reshape(size)
         u, _ = self._draw(size, 'choice')
         r = np.floor(np.asarray(u) * int(a)).astype(np.int64)
         return int(r) if size is None else r
+
+    def permutation(self, x):
+        if not np.isscalar(x):
+            raise NotImplementedError("PhiloxStream.permutation only supports an integer length")
+        u, _ = self._draw(int(x), 'permutation')
+        return np.argsort(np.atleast_1d(u), kind='stable')
 
     def normal(self, *args, **kwargs):
         raise NotImplementedError("normal() is not on the hot path: pass E_B as an explicit array")

@@ -63,6 +63,14 @@ def build_oracle(name, spec=None, fx=None, **over):
     return OracleMagnets(g, fx['m0'], **kw)
 
 
+def run_relaxation(mm, spec):
+    """The relax() / minimize() call a scenario ends with, if any (oracle or product)."""
+    if spec.get('relax') is not None:
+        mm.relax(**spec['relax'])
+    if spec.get('minimize') is not None:
+        mm.minimize(**spec['minimize'])
+
+
 def dipolar_like(mm):
     """The DipolarEnergy or DiMonopolarEnergy of an instance (oracle or product), or None."""
     for name in ('dipolar', 'dimonopolar'):

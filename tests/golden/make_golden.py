@@ -68,6 +68,7 @@ def route_rng(mm, stream):
     np.random.randint = stream.randint
     np.random.choice = stream.choice
     np.random.random = stream.random
+    np.random.permutation = stream.permutation
 
 
 def lognormal_EB(mean, sigma, shape, seed):
@@ -158,6 +159,11 @@ def run_spec(hs, spec):
         dt, dmc = mm.progress(**spec['progress'])
         rec['progress'] = np.array([dt, dmc])
         rec['progress_calls'] = np.array(stream.call)
+    if spec.get('relax') is not None:
+        mm.relax(**spec['relax'])
+    if spec.get('minimize') is not None:
+        mm.minimize(**spec['minimize'])
+    rec['final_counts'] = np.array([mm.switches, mm.attempted_switches, stream.call], dtype=np.int64)
     rec['m_final'] = mm.m.copy()
     rec['E_final'] = mm.E.copy()
     if dip is not None:
@@ -224,6 +230,21 @@ SPECS = {
     'metro_sq16_dimono_pbc': dict(BASE_PIN, lattice='IP_Square', a=400e-9, nx=16, ny=16, seed=63, kw=dict(PBC=True),
                                   T=1500.0, energies=[dict(type='dimonopolar', d=150e-9, small_d=70e-9)], steps=60,
                                   params=dict(METROPOLIS_TIME=True), update_kw=dict(r=600e-9)),
+    # relax() / _minimize_all() (sub-grid sweeps) and minimize() (sequential), from random states
+    'relax_oop24': dict(BASE_OOP, nx=24, ny=24, seed=71, energies=[dict(type='dipolar')], steps=0, relax={}),
+    'relax_pin20_pbc_barrier': dict(BASE_PIN, nx=20, ny=20, seed=72, kw=dict(PBC=True), E_B=3e-20,
+                                    energies=[dict(type='dipolar', cutoff=6 * 300e-9), dict(type='zeeman', B=2e-3, angle=0.4)],
+                                    steps=0, relax=dict(ignore_barrier=False)),
+    'relax_kagome_exchange': dict(BASE_PIN, lattice='IP_Kagome', a=1e-6, nx=20, ny=17, seed=73,
+                                  energies=[dict(type='dipolar', cutoff=3e-6), dict(type='exchange', J=2e-20)],
+                                  steps=0, relax={}),
+    'relax_oop16_simultaneous': dict(BASE_OOP, nx=16, ny=16, seed=74, energies=[dict(type='dipolar'), dict(type='zeeman', B=5e-4)],
+                                     steps=0, relax=dict(_simultaneous=True)),
+    'relax_sq16_dimono': dict(BASE_PIN, lattice='IP_Square', a=400e-9, nx=16, ny=16, seed=75,
+                              energies=[dict(type='dimonopolar', d=150e-9, small_d=70e-9)], steps=0, relax={}),
+    'minimize_oop16': dict(BASE_OOP, nx=16, ny=16, seed=76, energies=[dict(type='dipolar'), dict(type='zeeman', B=3e-4)],
+                           steps=0, minimize={}),
+    'minimize_pin16': dict(BASE_PIN, nx=16, ny=16, seed=77, energies=[dict(type='dipolar')], steps=0, minimize={}),
 }
 for name in ('metro_sq16_dimono_pbc', 'metro_pin32_grid', 'metro_pin24_pbc', 'metro_oop32_trunc_pbc', 'metro_oop30_trunc',
              'metro_oop16_time', 'metro_kagome_grid', 'metro_oop16_single'):

@@ -5,7 +5,7 @@ counters, time and RNG call counts must agree exactly and energies to FP64 round
 import numpy as np
 import pytest
 
-from cases import build_oracle, dipolar_like, load_fixture, load_specs, rel_err
+from cases import build_oracle, dipolar_like, load_fixture, load_specs, rel_err, run_relaxation
 from oracle.philox import PhiloxStream, philox4x32_10, uniform53
 
 SPECS = load_specs()
@@ -65,6 +65,9 @@ def test_oracle_matches_reference(name):
         assert mm.t == pytest.approx(fx["t"][s], rel=1e-9, abs=0)
     assert np.array_equal(sw_y, fx['sw_y']) and np.array_equal(sw_x, fx['sw_x'])
     assert np.array_equal(sw_step, fx['sw_step'])
+    run_relaxation(mm, spec)
+    if 'final_counts' in fx:
+        assert [mm.switches, mm.attempted_switches, mm.rng.call] == fx['final_counts'].tolist()
     assert np.array_equal(mm.m, fx['m_final'])
     assert rel_err(mm.E, fx['E_final']) < 1e-11
     if dip is not None:
