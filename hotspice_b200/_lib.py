@@ -88,6 +88,16 @@ SIGNATURES = {
                                              C.POINTER(HsGridPlan), P]),
     'hs_wolff_scratch_bytes': (C.c_int64, [C.POINTER(HsLattice)]),
     'hs_wolff_step': (C.c_int, [C.POINTER(HsLattice), P, C.POINTER(HsSwitchList), P, C.c_int64, P]),
+    'hs_relax_scratch_bytes': (C.c_int64, [C.POINTER(HsLattice)]),
+    'hs_relax_begin': (C.c_int, [C.POINTER(HsLattice), P, C.c_int64, P]),
+    'hs_relax_permute': (C.c_int, [C.POINTER(HsLattice), P, C.c_int32, P, C.c_int64, P]),
+    'hs_relax_subset': (C.c_int, [C.POINTER(HsLattice), P, C.POINTER(HsSwitchList), C.c_int32, C.c_int32, C.c_int32,
+                                  P, C.c_int64, P]),
+    'hs_minimize_all': (C.c_int, [C.POINTER(HsLattice), P, C.POINTER(HsSwitchList), C.c_int32, C.c_int32, P,
+                                  C.c_int64, P]),
+    'hs_relax_check': (C.c_int, [C.POINTER(HsLattice), P, C.c_int32, P, C.c_int64, P]),
+    'hs_minimize_begin': (C.c_int, [C.POINTER(HsLattice), P, C.c_int64, P]),
+    'hs_minimize_step': (C.c_int, [C.POINTER(HsLattice), P, C.POINTER(HsSwitchList), C.c_double, P, C.c_int64, P]),
     'hs_engine_run': (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, P, P]),
     'hs_engine_max_clusters': (C.c_int, [C.c_int32]),
     'hs_exchange_energy': (C.c_int, [C.POINTER(HsLattice), P, P, P]),

@@ -992,6 +992,113 @@ class Magnets(ABC):
             self._set_control(progress=0, done=0, t_max=t_max)
         cache[1].launch(cache[2])
 
+    # ------------------------------------------------------------------ relaxation
+    def _relax_args(self):
+        L = self._lattice_struct()
+        nbytes = self._lib.hs_relax_scratch_bytes(L)
+        if nbytes < 0:
+            _lib.check(-1, 'hs_relax_scratch_bytes')
+        buf = self._get_scratch('relax', nbytes)
+        _, s = self._switch_list(self.nx * self.ny)
+        return L, s, buf
+
+    @staticmethod
+    def _relax_word(buf, k):
+        """Word k of the relax scratch's header: 0 = stop rule fired, 1 = sweeps made."""
+        return int(buf[4 * k:4 * k + 4].cpu().view(torch.int32)[0])
+
+    def _replay(self, key, enqueue):
+        """Run ``enqueue(stream)`` once, as a CUDA graph when graphs are enabled (cached under
+        ``key``; every kernel it launches reads its control state from device memory)."""
+        if not self.engine.use_graphs:
+            enqueue(self._stream())
+            return
+        g = self._graphs.get(key)
+        if g is None:
+            g = torch.cuda.CUDAGraph()
+            s = torch.cuda.Stream(self.device)
+            s.wait_stream(torch.cuda.current_stream(self.device))
+            with torch.cuda.graph(g, stream=s):
+                enqueue(s.cuda_stream)
+            torch.cuda.current_stream(self.device).wait_stream(s)
+            self._graphs[key] = g
+        g.replay()
+
+    def _minimize_all(self, ignore_barrier=True, _simultaneous=False):
+        """hotspice/core.py:799-825: one sweep over the (2 ux) x (2 uy) subgrids in a random
+        order (one Philox call), switching in each subgrid every magnet whose switch lowers
+        the energy (or, without ignore_barrier, whose switch_energy/2 + E_B < 0)."""
+        if _simultaneous:
+            warnings.warn("_simultaneous=True in _minimize_all(). I hope you know what you are doing, as this is very nonphysical ;)", stacklevel=2)
+        L, s, buf = self._relax_args()
+        st = self._stream()
+        _lib.check(self._lib.hs_relax_begin(L, buf.data_ptr(), buf.numel(), st), 'hs_relax_begin')
+        _lib.check(self._lib.hs_minimize_all(L, self._counters.data_ptr(), s, int(bool(ignore_barrier)),
+                                             int(bool(_simultaneous)), buf.data_ptr(), buf.numel(), st),
+                   'hs_minimize_all')
+
+    def relax(self, verbose=False, **kwargs):
+        """hotspice/core.py:827-861: _minimize_all sweeps until one switches nothing, the state
+        equals the one two sweeps before, or int(sqrt(nx^2 + ny^2)) sweeps were made. The
+        sweeps and the stop rule run on the device (``EngineConfig.graph_steps`` sweeps per
+        CUDA-graph replay, one host check per replay). Returns nothing, like the reference;
+        the number of sweeps is kept in ``self.relax_sweeps``."""
+        ignore_barrier = bool(kwargs.pop('ignore_barrier', True))
+        simultaneous = bool(kwargs.pop('_simultaneous', False))
+        if kwargs:
+            raise TypeError(f"relax() got unexpected keyword arguments {sorted(kwargs)}")
+        if simultaneous:
+            warnings.warn("_simultaneous=True in _minimize_all(). I hope you know what you are doing, as this is very nonphysical ;)", stacklevel=2)
+        n_max = int(math.sqrt(self.nx ** 2 + self.ny ** 2))
+        self.relax_sweeps = 0
+        if not bool(torch.any(self._m_dev != 0)):   # allclose(zeros, m): the loop never starts
+            return
+        L, s, buf = self._relax_args()
+        lib, C = self._lib, self._counters.data_ptr()
+        st = self._stream()
+        _lib.check(lib.hs_relax_begin(L, buf.data_ptr(), buf.numel(), st), 'hs_relax_begin')
+        P = 1 if simultaneous else 4 * self.unitcell.x * self.unitcell.y
+        K = max(1, min(int(self.engine.graph_steps), n_max, 2048 // (3 * P + 3)))   # about 2k graph nodes
+
+        def sweeps(stream):
+            for _ in range(K):
+                _lib.check(lib.hs_minimize_all(L, C, s, int(ignore_barrier), int(simultaneous), buf.data_ptr(),
+                                               buf.numel(), stream), 'hs_minimize_all')
+                _lib.check(lib.hs_relax_check(L, C, n_max, buf.data_ptr(), buf.numel(), stream), 'hs_relax_check')
+        key = ('relax', ignore_barrier, simultaneous, K, buf.data_ptr(), s.y, self._version)
+        for _ in range((n_max + K - 1) // K):
+            self._replay(key, sweeps)
+            if self._relax_word(buf, 0):
+                break
+        self.relax_sweeps = self._relax_word(buf, 1)
+        if verbose:
+            print(f"Used {self.relax_sweeps} (out of {n_max}) steps in relax().")
+
+    def minimize(self, ignore_barrier=True, verbose=False, _frac=0.3):
+        """hotspice/core.py:763-797, on the device: per iteration, with n magnets gaining more
+        than kBT by switching, ceil(frac n) of them switch (one Philox call chooses them);
+        otherwise the magnet with the most to gain switches, unless nothing gains or it was
+        picked a third time. ``ignore_barrier=False`` is refused: there the reference compares
+        the (barrier, barrier) tuple returned by E_barrier() and indexes the result as if it
+        were one array."""
+        if not ignore_barrier:
+            raise NotImplementedError('minimize(ignore_barrier=False) has no well-defined reference result')
+        L, s, buf = self._relax_args()
+        lib, C = self._lib, self._counters.data_ptr()
+        st = self._stream()
+        _lib.check(lib.hs_minimize_begin(L, buf.data_ptr(), buf.numel(), st), 'hs_minimize_begin')
+        K = max(1, int(self.engine.graph_steps))
+        frac = float(_frac)
+
+        def iterations(stream):
+            for _ in range(K):
+                _lib.check(lib.hs_minimize_step(L, C, s, frac, buf.data_ptr(), buf.numel(), stream), 'hs_minimize_step')
+        key = ('minimize', frac, K, buf.data_ptr(), s.y, self._version)
+        while True:
+            self._replay(key, iterations)
+            if self._relax_word(buf, 0):
+                break
+
     def _snapshot(self):
         d = self._dipolar()
         return {'m': self._m_dev.clone(), 'mm': self._mm_dev.clone(), 'C': self._counters.clone(),

@@ -191,6 +191,70 @@ int hs_wolff_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, voi
     return hs_launch_wolff(*L, C, *sw, scratch, scratch_bytes, (cudaStream_t)stream);
 }
 
+int64_t hs_relax_scratch_bytes(const HsLattice *L) {
+    if (check_lattice(L, "hs_relax_scratch_bytes")) return -1;
+    return hs_relax_scratch(*L);
+}
+
+int hs_relax_begin(const HsLattice *L, void *scratch, int64_t scratch_bytes, void *stream) {
+    int rc = check_lattice(L, "hs_relax_begin");
+    if (rc) return rc;
+    if (!scratch) { hs_set_error("hs_relax_begin: null scratch"); return HS_EINVAL; }
+    return hs_relax_begin_impl(*L, scratch, scratch_bytes, (cudaStream_t)stream);
+}
+
+int hs_relax_permute(const HsLattice *L, HsCounters *C, int32_t simultaneous, void *scratch, int64_t scratch_bytes,
+                     void *stream) {
+    int rc = check_lattice(L, "hs_relax_permute");
+    if (rc) return rc;
+    if (!C || !scratch) { hs_set_error("hs_relax_permute: null argument"); return HS_EINVAL; }
+    return hs_relax_permute_impl(*L, C, simultaneous, scratch, scratch_bytes, (cudaStream_t)stream);
+}
+
+int hs_relax_subset(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, int32_t i, int32_t ignore_barrier,
+                    int32_t simultaneous, void *scratch, int64_t scratch_bytes, void *stream) {
+    int rc = check_lattice(L, "hs_relax_subset");
+    if (rc) return rc;
+    if (!C || !sw || !scratch) { hs_set_error("hs_relax_subset: null argument"); return HS_EINVAL; }
+    return hs_relax_subset_impl(*L, C, *sw, i, ignore_barrier, simultaneous, scratch, scratch_bytes,
+                                (cudaStream_t)stream);
+}
+
+int hs_minimize_all(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, int32_t ignore_barrier,
+                    int32_t simultaneous, void *scratch, int64_t scratch_bytes, void *stream) {
+    int rc = hs_relax_permute(L, C, simultaneous, scratch, scratch_bytes, stream);
+    if (rc) return rc;
+    const int P = simultaneous ? 1 : 4 * L->ux * L->uy;
+    for (int i = 0; i < P; ++i) {
+        rc = hs_relax_subset(L, C, sw, i, ignore_barrier, simultaneous, scratch, scratch_bytes, stream);
+        if (rc) return rc;
+    }
+    return HS_OK;
+}
+
+int hs_relax_check(const HsLattice *L, HsCounters *C, int32_t n_max, void *scratch, int64_t scratch_bytes,
+                   void *stream) {
+    int rc = check_lattice(L, "hs_relax_check");
+    if (rc) return rc;
+    if (!C || !scratch || n_max < 1) { hs_set_error("hs_relax_check: bad argument"); return HS_EINVAL; }
+    return hs_relax_check_impl(*L, C, n_max, scratch, scratch_bytes, (cudaStream_t)stream);
+}
+
+int hs_minimize_begin(const HsLattice *L, void *scratch, int64_t scratch_bytes, void *stream) {
+    int rc = check_lattice(L, "hs_minimize_begin");
+    if (rc) return rc;
+    if (!scratch) { hs_set_error("hs_minimize_begin: null scratch"); return HS_EINVAL; }
+    return hs_minimize_begin_impl(*L, scratch, scratch_bytes, (cudaStream_t)stream);
+}
+
+int hs_minimize_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, double frac, void *scratch,
+                     int64_t scratch_bytes, void *stream) {
+    int rc = check_lattice(L, "hs_minimize_step");
+    if (rc) return rc;
+    if (!C || !sw || !scratch) { hs_set_error("hs_minimize_step: null argument"); return HS_EINVAL; }
+    return hs_minimize_step_impl(*L, C, *sw, frac, scratch, scratch_bytes, (cudaStream_t)stream);
+}
+
 int hs_engine_run(const HsInstance *insts, int32_t n_inst, int32_t cluster_size, int32_t n_clusters, int32_t *work,
                   void *stream) {
     if (!insts || !work || n_inst < 0 || n_clusters <= 0) { hs_set_error("hs_engine_run: bad arguments"); return HS_EINVAL; }

@@ -30,6 +30,17 @@ int hs_launch_philox(uint64_t seed, uint64_t call, int32_t n, double *out, cudaS
 int64_t hs_igemm_scratch(const HsLattice &L, int nsplit);
 int hs_launch_igemm(const HsLattice &L, int nsplit, void *scratch, int64_t scratch_bytes, cudaStream_t st);
 
+int64_t hs_relax_scratch(const HsLattice &L);
+int hs_relax_begin_impl(const HsLattice &L, void *scratch, int64_t bytes, cudaStream_t st);
+int hs_relax_permute_impl(const HsLattice &L, HsCounters *C, int simultaneous, void *scratch, int64_t bytes,
+                          cudaStream_t st);
+int hs_relax_subset_impl(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, int i, int ignore_barrier,
+                         int simultaneous, void *scratch, int64_t bytes, cudaStream_t st);
+int hs_relax_check_impl(const HsLattice &L, HsCounters *C, int n_max, void *scratch, int64_t bytes, cudaStream_t st);
+int hs_minimize_begin_impl(const HsLattice &L, void *scratch, int64_t bytes, cudaStream_t st);
+int hs_minimize_step_impl(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, double frac, void *scratch,
+                          int64_t bytes, cudaStream_t st);
+
 int hs_launch_engine(const HsInstance *insts, int n_inst, int cluster_size, int n_clusters, int *work,
                      cudaStream_t st);
 int hs_engine_max_clusters_impl(int cluster_size);

@@ -18,6 +18,9 @@
  *                            _select_Poisson (hotspice/core.py:659-677, 456-570)
  *   hs_wolff_step            Magnets._update_Wolff + _select_cluster_exchange
  *                            (hotspice/core.py:711-718, 588-602)
+ *   hs_minimize_all / hs_relax_check
+ *                            Magnets._minimize_all / relax (hotspice/core.py:799-861)
+ *   hs_minimize_step         one iteration of Magnets.minimize (hotspice/core.py:763-797)
  *   hs_exchange_energy       ExchangeEnergy.update (hotspice/energies.py:771-781)
  *   hs_philox_uniform        the variate stream that replaces numpy.random in the hot path
  */
@@ -218,6 +221,39 @@ int hs_metropolis_step_noalloc(const HsLattice *L, HsCounters *C, const HsSwitch
 int64_t hs_wolff_scratch_bytes(const HsLattice *L);
 int hs_wolff_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw,
                   void *scratch, int64_t scratch_bytes, void *stream);
+
+/* ---- relaxation: relax() / _minimize_all() / minimize() (hotspice/core.py:763-861) ---------- */
+/* One scratch layout serves all of these; its first 8 bytes are {int32 done; int32 sweeps}:
+ * `done` is set when relax()'s stop rule (or minimize()'s) has fired, after which every call
+ * below does nothing until the next hs_relax_begin / hs_minimize_begin; `sweeps` counts the
+ * relax sweeps made. Switch list capacity: nx * ny. */
+int64_t hs_relax_scratch_bytes(const HsLattice *L);
+/* Start relax(): clears the stop state, records m as the state "two sweeps before". */
+int hs_relax_begin(const HsLattice *L, void *scratch, int64_t scratch_bytes, void *stream);
+/* One _minimize_all sweep (core.py:799-825): draws the subgrid order (one Philox call, a
+ * stable argsort of (2ux)(2uy) variates, or of 1 when `simultaneous`), then for each subgrid
+ * switches every magnet with switch_energy < 0 (ignore_barrier) or switch_energy / 2 + E_B < 0,
+ * and updates the energies (DipolarEnergy.update_single / update_multiple semantics). */
+int hs_minimize_all(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, int32_t ignore_barrier,
+                    int32_t simultaneous, void *scratch, int64_t scratch_bytes, void *stream);
+/* The two halves of hs_minimize_all: the order, then subgrid i (0 <= i < number of subgrids). */
+int hs_relax_permute(const HsLattice *L, HsCounters *C, int32_t simultaneous, void *scratch,
+                     int64_t scratch_bytes, void *stream);
+int hs_relax_subset(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, int32_t i,
+                    int32_t ignore_barrier, int32_t simultaneous, void *scratch, int64_t scratch_bytes,
+                    void *stream);
+/* relax()'s stop rule after a sweep (core.py:842-857): nothing switched, the state equals the
+ * one two sweeps before, or n_max = int(sqrt(nx^2 + ny^2)) sweeps were made. */
+int hs_relax_check(const HsLattice *L, HsCounters *C, int32_t n_max, void *scratch, int64_t scratch_bytes,
+                   void *stream);
+/* Start minimize(): clears the stop state and the per-magnet pick counts. */
+int hs_minimize_begin(const HsLattice *L, void *scratch, int64_t scratch_bytes, void *stream);
+/* One iteration of minimize(ignore_barrier=True) (core.py:771-797): with n magnets whose
+ * switch_energy < -kBT, switches ceil(frac n) of them, chosen by one Philox call over n
+ * elements (the smallest keys); else switches the first argmin of switch_energy if it is < 0
+ * and was not picked three times; else sets `done`. */
+int hs_minimize_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, double frac, void *scratch,
+                     int64_t scratch_bytes, void *stream);
 
 /* ---- persistent multi-instance engine -------------------------------------------------------- */
 /* Advances n_inst instances (device array `insts`) in one launch of n_clusters thread-block

@@ -698,24 +698,30 @@ class OracleMagnets:
         subgrid when simultaneous), switch every magnet of the subgrid whose switch lowers the
         energy (or, with ignore_barrier False, whose switch_energy/2 + E_B < 0).
         ``decide(subset, mask)`` may replace the mask (lock-step tests)."""
+        sx, sy = self.subgrid_steps(_simultaneous)
+        for i in self.rng.permutation(sx * sy):
+            self.minimize_subgrid(int(i), sx, sy, ignore_barrier, decide)
+
+    def subgrid_steps(self, simultaneous=False):
         ux, uy = self.unitcell
-        sx, sy = (1, 1) if _simultaneous else (2 * ux, 2 * uy)
-        order = self.rng.permutation(sx * sy)
-        for i in order:
-            y, x = divmod(int(i), sx)
-            if not self.occupation[y, x]:
-                continue
-            sub = np.asarray(np.meshgrid(np.arange(y, self.ny, sy), np.arange(x, self.nx, sx))).reshape(2, -1)
-            dE = self.switch_energy(sub)
-            mask = dE < 0 if ignore_barrier else dE / 2 + self.E_B[sub[0], sub[1]] < 0
-            if decide is not None:
-                mask = decide(sub, mask, dE)
-            sel = sub[:, mask]
-            if sel.size > 0:
-                self.m[sel[0], sel[1]] = -self.m[sel[0], sel[1]]
-                self.switches += sel.shape[1]
-                self.attempted_switches += sel.shape[1]
-                self.update_energy(sel)
+        return (1, 1) if simultaneous else (2 * ux, 2 * uy)
+
+    def minimize_subgrid(self, i, sx, sy, ignore_barrier=True, decide=None):
+        """The body of the loop of hotspice/core.py:812-825 for subgrid number i."""
+        y, x = divmod(i, sx)
+        if not self.occupation[y, x]:
+            return
+        sub = np.asarray(np.meshgrid(np.arange(y, self.ny, sy), np.arange(x, self.nx, sx))).reshape(2, -1)
+        dE = self.switch_energy(sub)
+        mask = dE < 0 if ignore_barrier else dE / 2 + self.E_B[sub[0], sub[1]] < 0
+        if decide is not None:
+            mask = decide(sub, mask, dE)
+        sel = sub[:, mask]
+        if sel.size > 0:
+            self.m[sel[0], sel[1]] = -self.m[sel[0], sel[1]]
+            self.switches += sel.shape[1]
+            self.attempted_switches += sel.shape[1]
+            self.update_energy(sel)
 
     def relax(self, **kwargs):
         """hotspice/core.py:827-861: repeated minimize_all sweeps until a sweep switches

@@ -1,0 +1,144 @@
+"""relax() / _minimize_all() / minimize() on the device against the reference fixtures and the
+oracle (hotspice/core.py:763-861).
+
+* Whole runs: the final state, the switch / attempt counts and the Philox call count equal
+  the reference's; energies within the stated tolerance (max|dE| / max|E| <= 2e-6).
+* Sub-grid lock-step: every subgrid's switch set equals the oracle's, except decisions whose
+  |switch_energy| lies within the effect of a 1e-6 relative energy error (near-threshold);
+  those are counted and the oracle follows the device.
+* Larger lattices: size-independent properties (a relax that stopped because nothing switched
+  leaves no magnet that gains by switching; the incrementally updated energies equal a full
+  recompute; minimize leaves no magnet gaining more than kBT).
+"""
+import numpy as np
+import pytest
+import torch
+
+from cases import build_oracle, dipolar_like, load_fixture, load_specs, rel_err, run_relaxation
+from gpu_cases import build_product
+
+pytestmark = pytest.mark.gpu
+SPECS = load_specs()
+E_TOL = 1e-6
+RELAX = [n for n in SPECS if SPECS[n].get('relax') is not None]
+MINIMIZE = [n for n in SPECS if SPECS[n].get('minimize') is not None]
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+@pytest.mark.parametrize('name', RELAX + MINIMIZE)
+def test_matches_reference(name):
+    spec, fx = SPECS[name], load_fixture(name)
+    mp = build_product(name)
+    run_relaxation(mp, spec)
+    c = mp._read_counters()
+    assert [int(c['switches']), int(c['attempted']), int(c['rng_call'])] == fx['final_counts'].tolist()
+    assert np.array_equal(_np(mp.m), fx['m_final'])
+    assert rel_err(_np(mp.E), fx['E_final']) < 2 * E_TOL
+    d = dipolar_like(mp)
+    if d is not None:
+        assert rel_err(_np(d.E), fx['E_dip_final']) < 2 * E_TOL
+        if mp.USE_PERP_ENERGY:
+            assert rel_err(_np(d.E_perp), fx['E_dip_perp_final']) < 2 * E_TOL
+
+
+@pytest.mark.parametrize('name', RELAX)
+def test_subgrid_lockstep(name):
+    """Three _minimize_all sweeps, subgrid by subgrid, through hs_relax_permute / hs_relax_subset."""
+    from hotspice_b200 import _lib
+    spec = SPECS[name]
+    kw = spec['relax']
+    ib, sim = bool(kw.get('ignore_barrier', True)), bool(kw.get('_simultaneous', False))
+    mp, mo = build_product(name), build_oracle(name)
+    lib = mp._lib
+    L, s, buf = mp._relax_args()
+    C = mp._counters.data_ptr()
+    st = mp._stream()
+    _lib.check(lib.hs_relax_begin(L, buf.data_ptr(), buf.numel(), st))
+    sx, sy = mo.subgrid_steps(sim)
+    near = 0
+    for sweep in range(3):
+        _lib.check(lib.hs_relax_permute(L, C, int(sim), buf.data_ptr(), buf.numel(), st))
+        order = mo.rng.permutation(sx * sy)
+        for i, o in enumerate(order):
+            _lib.check(lib.hs_relax_subset(L, C, s, i, int(ib), int(sim), buf.data_ptr(), buf.numel(), st))
+            n = int(mp._read_counters()['n_sw'])
+            t, _ = mp._sw
+            got = {(int(a), int(b)) for a, b in zip(*t[:2, :n].cpu().numpy())}
+
+            def decide(sub, mask, dE):
+                nonlocal near
+                dev = np.array([(int(a), int(b)) in got for a, b in zip(sub[0], sub[1])])
+                diff = np.nonzero(dev != mask)[0]
+                if diff.size:
+                    Emax = np.max(np.abs(mo.E))
+                    assert np.all(np.abs(dE[diff]) <= 2 * 2 * 2 * E_TOL * Emax), \
+                        f'sweep {sweep} subgrid {i}: decisions differ beyond tolerance'
+                    near += diff.size
+                assert int(dev.sum()) == len(got)
+                return dev
+            y0, x0 = divmod(int(o), sx)
+            if mo.occupation[y0, x0]:
+                mo.minimize_subgrid(int(o), sx, sy, ib, decide)
+            else:
+                assert n == 0
+        c = mp._read_counters()
+        assert int(c['switches']) == mo.switches and int(c['rng_call']) == mo.rng.call
+        assert np.array_equal(_np(mp.m), mo.m), f'sweep {sweep}'
+    assert rel_err(_np(mp.E), mo.E) < 2 * E_TOL
+    print(f'{name}: 3 sweeps, {near} near-threshold decisions')
+
+
+def _pinwheel(n, seed, **kw):
+    import hotspice_b200 as hs
+    return hs.ASI.IP_Pinwheel(300e-9, n, T=300, E_B=5e-20, moment=1e-15, pattern='random', seed=seed,
+                              energies=[hs.DipolarEnergy(cutoff_range=kw.pop('cutoff', 20 * 300e-9)),
+                                        hs.ZeemanEnergy(2e-4, 0.3)], **kw)
+
+
+@pytest.mark.parametrize('n,PBC', [(256, False), (200, True)])
+def test_relax_properties_large(n, PBC):
+    mm = _pinwheel(n, 5, PBC=PBC)
+    mm.relax()
+    n_max = int(np.sqrt(2) * n)
+    d = mm._dipolar()
+    E_inc = _np(d.E)
+    d.update(method='direct64')
+    assert rel_err(E_inc, _np(d.E)) < 2 * E_TOL
+    assert 1 <= mm.relax_sweeps <= n_max
+    # one more sweep: if it switches nothing, no magnet may gain by switching
+    dE = _np(mm.switch_energy())
+    occ = mm.occupation.astype(bool)
+    sw0 = mm.switches
+    mm._minimize_all()
+    if mm.switches == sw0:
+        assert np.all(dE[occ] >= -4 * E_TOL * np.max(np.abs(dE)))
+
+
+def test_minimize_properties():
+    mm = _pinwheel(48, 9)
+    mm.minimize()
+    dE = _np(mm.switch_energy())
+    kbt = 1.380649e-23 * 300
+    assert np.all(dE[mm.occupation.astype(bool)] >= -kbt * (1 + 1e-6))
+
+
+def test_relax_graph_equals_direct():
+    """The sweeps replayed from CUDA graphs equal the directly launched ones, bit for bit."""
+    import hotspice_b200 as hs
+    a = _pinwheel(64, 3, engine=hs.EngineConfig(use_graphs=False))
+    b = _pinwheel(64, 3, engine=hs.EngineConfig(use_graphs=True, graph_steps=4))
+    a.relax()
+    b.relax()
+    assert a.relax_sweeps == b.relax_sweeps
+    assert torch.equal(a._m_dev, b._m_dev)
+    assert torch.equal(a._dipolar()._E, b._dipolar()._E)
+    assert a._read_counters()['rng_call'] == b._read_counters()['rng_call']
+
+
+def test_minimize_refuses_barrier_mode():
+    mm = _pinwheel(16, 1)
+    with pytest.raises(NotImplementedError):
+        mm.minimize(ignore_barrier=False)
