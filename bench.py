@@ -380,6 +380,9 @@ def run_product(args):
     incremental = None
     if rank == 0 and args.incremental_n > 0:
         incremental = run_incremental(dev, n=args.incremental_n)
+    relax = None
+    if rank == 0 and args.relax_n > 0:
+        relax = run_relax(dev, n=args.relax_n, cpu_seconds=0.0 if args.no_cpu_baseline else 10.0)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -420,6 +423,8 @@ def run_product(args):
         line["full_recompute"] = recompute
     if incremental is not None:
         line["incremental_update"] = incremental
+    if relax is not None:
+        line["relax"] = relax
     if not args.no_cpu_baseline:
         v, secs, st, ni = oracle_sample(specs, seconds_per_instance=args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
@@ -575,6 +580,55 @@ def run_incremental(dev, n=2048, reps=20):
     return out
 
 
+def run_relax(dev, n=1024, cpu_n=128, cpu_seconds=10.0):
+    """relax() (f2): _minimize_all sweeps until the stop rule, on an IP_Pinwheel n x n from a
+    random start (dipolar cutoff 8.3a, Zeeman), all on the device. CPU baseline: whole
+    _minimize_all sweeps of the NumPy oracle (the reference's algorithm) on a cpu_n x cpu_n
+    lattice, as magnet-sweeps per second."""
+    import torch
+    import hotspice_b200 as hs
+    g = np.random.Generator(np.random.PCG64(SEED + 3))
+    m0 = g.integers(0, 2, size=(n, n)) * 2 - 1
+    mm = hs.ASI.IP_Pinwheel(A1, n, T=300.0, E_B=6e-20, moment=1e-15, pattern=m0,
+                            energies=[hs.DipolarEnergy(cutoff_range=8.3 * A1), hs.ZeemanEnergy(2e-4, 0.3)],
+                            seed=SEED, device=dev)
+    mm.relax()                        # warm-up: builds and caches the graphs
+    mm.m = m0
+    mm.update_energy()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sw0 = mm.switches
+    e0.record()
+    mm.relax()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    sweeps = mm.relax_sweeps
+    out = {"workload": f"relax() of IP_Pinwheel {n}x{n} ({mm.n} magnets), a=300nm, dipolar cutoff 8.3a, Zeeman 0.2 mT, "
+                       f"random start", "sweeps": sweeps, "switches": mm.switches - sw0, "ms": ms,
+           "ms_per_sweep": ms / max(sweeps, 1), "magnet_sweeps_per_s": mm.n * sweeps / (ms * 1e-3)}
+    del mm
+    torch.cuda.empty_cache()
+    # CPU: the oracle's _minimize_all on a smaller lattice (bounded sample)
+    from oracle import geometry as G
+    from oracle.hotspice_oracle import OracleDipolar, OracleMagnets, OracleZeeman
+    geo = G.ip_pinwheel(A1, cpu_n, cpu_n)
+    mc = g.integers(0, 2, size=(cpu_n, cpu_n)) * 2 - 1
+    mo = OracleMagnets(geo, mc, T=300.0, E_B=6e-20, moment=1e-15, seed=SEED,
+                       energies=[OracleDipolar(cutoff_range=8.3 * A1), OracleZeeman(2e-4, 0.3)])
+    t0 = time.perf_counter()
+    k = 0
+    while time.perf_counter() - t0 < cpu_seconds and k < 50:
+        mo.minimize_all()
+        k += 1
+    secs = time.perf_counter() - t0
+    out["cpu_baseline"] = {"value": mo.n * k / secs, "unit": "magnet-sweeps/s", "cores": 1, "kind": "port",
+                           "sample": f"{k} _minimize_all sweeps of IP_Pinwheel {cpu_n}x{cpu_n} with the NumPy oracle "
+                                     f"({secs:.1f} s)"}
+    out["gpu_over_cpu"] = out["magnet_sweeps_per_s"] / out["cpu_baseline"]["value"]
+    return out
+
+
 SERVED_WORKLOAD = ("served: the first {k} requests of a seeded Poisson arrival stream (mean 200/s); lattice uniform over "
                    "{{OOP_Square a=200nm, IP_Pinwheel a=300nm, IP_Kagome a=500nm, exchange-only square Ising J=1e-21 J "
                    "(Wolff)}}, n log-uniform in [64,1024], steps log-uniform in [1e3,1e5], T uniform in [200,400]K, Zeeman "
@@ -685,6 +739,8 @@ def main():
     ap.add_argument('--only-recompute', action='store_true', help='run only the full-recompute timing and print it')
     ap.add_argument('--incremental-n', type=int, default=2048, help='lattice side of the incremental-update timing (0: skip)')
     ap.add_argument('--only-incremental', action='store_true', help='run only the incremental-update timing and print it')
+    ap.add_argument('--relax-n', type=int, default=1024, help='lattice side of the relax() timing (0: skip)')
+    ap.add_argument('--only-relax', action='store_true', help='run only the relax() timing and print it')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)
@@ -693,6 +749,11 @@ def main():
         dev = torch.device('cuda', 0)
         torch.cuda.set_device(dev)
         print(json.dumps({"incremental_update": run_incremental(dev, n=args.incremental_n)}))
+    elif args.only_relax:
+        import torch
+        dev = torch.device('cuda', 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({"relax": run_relax(dev, n=args.relax_n)}))
     elif args.only_recompute:
         import torch
         dev = torch.device('cuda', 0)
