@@ -11,6 +11,7 @@ from .core import EngineConfig, Magnets, Scheme, SimParams, Unitcell, kB
 from .energies import DiMonopolarEnergy, DipolarEnergy, Energy, ExchangeEnergy, ZeemanEnergy
 from . import energies, utils
 from . import ASI
+from . import io
 
-__all__ = ['ASI', 'config', 'energies', 'utils', 'kB', 'SimParams', 'Magnets', 'Scheme', 'EngineConfig',
+__all__ = ['ASI', 'config', 'energies', 'io', 'utils', 'kB', 'SimParams', 'Magnets', 'Scheme', 'EngineConfig',
            'Unitcell', 'Energy', 'ZeemanEnergy', 'DipolarEnergy', 'DiMonopolarEnergy', 'ExchangeEnergy']

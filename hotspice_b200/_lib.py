@@ -98,6 +98,10 @@ SIGNATURES = {
     'hs_relax_check': (C.c_int, [C.POINTER(HsLattice), P, C.c_int32, P, C.c_int64, P]),
     'hs_minimize_begin': (C.c_int, [C.POINTER(HsLattice), P, C.c_int64, P]),
     'hs_minimize_step': (C.c_int, [C.POINTER(HsLattice), P, C.POINTER(HsSwitchList), C.c_double, P, C.c_int64, P]),
+    'hs_zeeman_set': (C.c_int, [C.c_int64, C.c_int32, P, P, P, C.c_double, C.c_double, P, P, P, P, P]),
+    'hs_progress_arm': (C.c_int, [P, C.c_int32, C.c_double, C.c_double, P]),
+    'hs_progress_disarm': (C.c_int, [P, P]),
+    'hs_region_readout': (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, P, P, P, P, P, P]),
     'hs_engine_run': (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, P, P]),
     'hs_engine_max_clusters': (C.c_int, [C.c_int32]),
     'hs_exchange_energy': (C.c_int, [C.POINTER(HsLattice), P, P, P]),

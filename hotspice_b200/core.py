@@ -992,6 +992,53 @@ class Magnets(ABC):
             self._set_control(progress=0, done=0, t_max=t_max)
         cache[1].launch(cache[2])
 
+    # ------------------------------------------------------------------ device-side stepping
+    def _moment64(self):
+        """FP64 device copy of the moment (the Zeeman factors are formed from it on the device)."""
+        c = getattr(self, '_mom64_cache', None)
+        if c is None or c[0] is not self._moment_np:
+            c = (self._moment_np, torch.as_tensor(self._moment_np, device=self.device, dtype=torch.float64).contiguous())
+            self._mom64_cache = c
+        return c[1]
+
+    def _orient64(self):
+        c = getattr(self, '_ori64_cache', None)
+        if c is None or c[0] is not self.orientation:
+            c = (self.orientation, torch.as_tensor(self.orientation, device=self.device, dtype=torch.float64).contiguous())
+            self._ori64_cache = c
+        return c[1]
+
+    def _progress_enqueue(self, t_max: float = 1, MCsteps_max: float = 4., **kwargs):
+        """progress(t_max, MCsteps_max) enqueued on the current stream with no host round trip:
+        hs_progress_arm sets the stop rule from the device counters, then one persistent engine
+        launch steps until it holds. Call :meth:`_progress_finish` after the last one (it ends
+        the armed state). Without the persistent engine this falls back to progress()."""
+        if not self.engine.persistent:
+            self.progress(t_max=t_max, MCsteps_max=MCsteps_max, **kwargs)
+            return
+        if self._T_zero:
+            raise RuntimeError('progress() with T=0 somewhere in the domain would never advance')
+        from .engine import BatchEngine
+        key = (self._version, tuple(sorted((k, float(v)) for k, v in kwargs.items())), self.engine.cluster_size)
+        c = getattr(self, '_pe_cache', None)
+        if c is None or c[0] != key:
+            eng = BatchEngine([self], cluster_size=self.engine.cluster_size or None)
+            c = (key, eng, eng._prepare([0], [dict(kwargs)]))
+            self._pe_cache = c
+        st = self._stream()
+        _lib.check(self._lib.hs_progress_arm(self._counters.data_ptr(), self.n, float(t_max), float(MCsteps_max), st),
+                   'hs_progress_arm')
+        c[1].launch(c[2])
+        self._ctl = None      # the device wrote t_max / progress / done: the host-side cache is stale
+
+    def _progress_finish(self):
+        """End device-armed progress() runs: plain steps run again; raises on a device status."""
+        _lib.check(self._lib.hs_progress_disarm(self._counters.data_ptr(), self._stream()), 'hs_progress_disarm')
+        self._ctl = None
+        st = int(self._read_counters()['status'])
+        if st:
+            raise RuntimeError(f'device step reported status {st} (HS_ST_* bits)')
+
     # ------------------------------------------------------------------ relaxation
     def _relax_args(self):
         L = self._lattice_struct()

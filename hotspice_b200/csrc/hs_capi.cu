@@ -255,6 +255,33 @@ int hs_minimize_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, 
     return hs_minimize_step_impl(*L, C, *sw, frac, scratch, scratch_bytes, (cudaStream_t)stream);
 }
 
+int hs_zeeman_set(int64_t n_cells, int32_t in_plane, const double *moment, const double *orient, const float *pattern,
+                  double magnitude, double angle, double *E_factor, double *E_factor_perp, float *zee, float *zee_perp,
+                  void *stream) {
+    if (n_cells <= 0 || !moment || !zee || (in_plane && !orient)) { hs_set_error("hs_zeeman_set: bad arguments"); return HS_EINVAL; }
+    return hs_zeeman_set_impl(n_cells, in_plane, moment, orient, pattern, magnitude, angle, E_factor, E_factor_perp, zee,
+                              zee_perp, (cudaStream_t)stream);
+}
+
+int hs_progress_arm(HsCounters *C, int32_t n_occ, double t_max, double MCsteps_max, void *stream) {
+    if (!C || n_occ <= 0) { hs_set_error("hs_progress_arm: bad arguments"); return HS_EINVAL; }
+    return hs_progress_arm_impl(C, n_occ, t_max, MCsteps_max, (cudaStream_t)stream);
+}
+
+int hs_progress_disarm(HsCounters *C, void *stream) {
+    if (!C) { hs_set_error("hs_progress_disarm: null counters"); return HS_EINVAL; }
+    return hs_progress_disarm_impl(C, (cudaStream_t)stream);
+}
+
+int hs_region_readout(const int8_t *m, int32_t nx, int32_t ny, int32_t n_regions, const int32_t *rects, const double *wx,
+                      const double *wy, const double *norm, double *out, void *stream) {
+    if (!m || nx <= 0 || ny <= 0 || n_regions <= 0 || !rects || !wx || !norm || !out) {
+        hs_set_error("hs_region_readout: bad arguments");
+        return HS_EINVAL;
+    }
+    return hs_region_readout_impl(m, nx, ny, n_regions, rects, wx, wy, norm, out, (cudaStream_t)stream);
+}
+
 int hs_engine_run(const HsInstance *insts, int32_t n_inst, int32_t cluster_size, int32_t n_clusters, int32_t *work,
                   void *stream) {
     if (!insts || !work || n_inst < 0 || n_clusters <= 0) { hs_set_error("hs_engine_run: bad arguments"); return HS_EINVAL; }

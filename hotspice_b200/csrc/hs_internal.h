@@ -41,6 +41,13 @@ int hs_minimize_begin_impl(const HsLattice &L, void *scratch, int64_t bytes, cud
 int hs_minimize_step_impl(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, double frac, void *scratch,
                           int64_t bytes, cudaStream_t st);
 
+int hs_zeeman_set_impl(int64_t n_cells, int in_plane, const double *moment, const double *orient, const float *pattern,
+                       double magnitude, double angle, double *ef, double *efp, float *ef32, float *efp32, cudaStream_t st);
+int hs_progress_arm_impl(HsCounters *C, int n_occ, double t_max, double mc_max, cudaStream_t st);
+int hs_progress_disarm_impl(HsCounters *C, cudaStream_t st);
+int hs_region_readout_impl(const int8_t *m, int nx, int ny, int R, const int32_t *rects, const double *wx,
+                           const double *wy, const double *norm, double *out, cudaStream_t st);
+
 int hs_launch_engine(const HsInstance *insts, int n_inst, int cluster_size, int n_clusters, int *work,
                      cudaStream_t st);
 int hs_engine_max_clusters_impl(int cluster_size);

@@ -75,6 +75,9 @@ class ZeemanEnergy(Energy):
         self.set_field(magnitude=self._magnitude, angle=self._angle)
 
     def set_field(self, magnitude=None, angle=None):
+        if magnitude is None:
+            self._resolve_lazy()
+        self._lazy = None
         if magnitude is not None:
             self._magnitude = magnitude
         if angle is not None:
@@ -122,8 +125,43 @@ class ZeemanEnergy(Energy):
     def E_tot(self):
         return float(torch.sum(self.E))
 
+    def set_field_device(self, magnitude: float, pattern: torch.Tensor | None = None, angle: float | None = None):
+        """set_field(magnitude * pattern, angle) computed on the device into the existing
+        buffers (hs_zeeman_set): stream-ordered, no host round trip, and the lattice struct and
+        captured graphs that point at the buffers stay valid. ``pattern``: an FP32 (ny, nx)
+        device tensor (None: uniform); ``angle`` None keeps the current (scalar) angle."""
+        mm = self.mm
+        if angle is not None:
+            self._angle = float(angle)
+        ang = self._angle
+        if mm.in_plane and not np.isscalar(ang):
+            a = np.asarray(ang, dtype=float)
+            if a.size and np.all(a == a.flat[0]):
+                ang = float(a.flat[0])
+            else:
+                raise NotImplementedError('set_field_device needs a uniform angle')
+        self._lazy = (float(magnitude), pattern)
+        _lib.check(mm._lib.hs_zeeman_set(mm.nx * mm.ny, int(mm.in_plane), mm._moment64().data_ptr(),
+                                         mm._orient64().data_ptr() if mm.in_plane else None,
+                                         pattern.data_ptr() if pattern is not None else None, float(magnitude),
+                                         float(ang) if mm.in_plane else 0.0, self.E_factor.data_ptr(),
+                                         self.E_factor_perp.data_ptr(), self._ef32.data_ptr(), self._efp32.data_ptr(),
+                                         mm._stream()), 'hs_zeeman_set')
+
+    def _resolve_lazy(self):
+        """Turn a magnitude set on the device back into the host-side value."""
+        lz = getattr(self, '_lazy', None)
+        if lz is not None:
+            self._lazy = None
+            scale, pat = lz
+            self._magnitude = scale if pat is None else pat.double().cpu().numpy() * scale
+
     @property
     def magnitude(self):
+        lz = getattr(self, '_lazy', None)
+        if lz is not None:
+            scale, pat = lz
+            return self.mm._field(scale if pat is None else pat.double().cpu().numpy() * scale)
         return self.mm._field(self._magnitude)
 
     @magnitude.setter

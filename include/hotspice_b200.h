@@ -21,6 +21,8 @@
  *   hs_minimize_all / hs_relax_check
  *                            Magnets._minimize_all / relax (hotspice/core.py:799-861)
  *   hs_minimize_step         one iteration of Magnets.minimize (hotspice/core.py:763-797)
+ *   hs_zeeman_set / hs_progress_arm / hs_region_readout
+ *                            the input / output steps of hotspice/io.py:193-500
  *   hs_exchange_energy       ExchangeEnergy.update (hotspice/energies.py:771-781)
  *   hs_philox_uniform        the variate stream that replaces numpy.random in the hot path
  */
@@ -254,6 +256,27 @@ int hs_minimize_begin(const HsLattice *L, void *scratch, int64_t scratch_bytes, 
  * and was not picked three times; else sets `done`. */
 int hs_minimize_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, double frac, void *scratch,
                      int64_t scratch_bytes, void *stream);
+
+/* ---- reservoir input / output stepping (hotspice/io.py:193-500) ------------------------------ */
+/* ZeemanEnergy.set_field (hotspice/energies.py:97-118) in place on the device: with
+ * B = magnitude * pattern[i] (pattern NULL: 1) at `angle`, E_factor = -moment (Bx ox + By oy) and
+ * E_factor_perp = -moment (By ox - Bx oy) in plane, E_factor = -moment B out of plane. moment and
+ * orient (ny, nx, 2) are FP64; E_factor / E_factor_perp (FP64, may be NULL) and zee / zee_perp
+ * (the FP32 copies HsLattice points at) are overwritten. */
+int hs_zeeman_set(int64_t n_cells, int32_t in_plane, const double *moment, const double *orient, const float *pattern,
+                  double magnitude, double angle, double *E_factor, double *E_factor_perp, float *zee, float *zee_perp,
+                  void *stream);
+/* Arms progress(t_max, MCsteps_max) (hotspice/core.py:736-760) from the device counters
+ * (t0 = t, mc0 = attempted / n_occ); a following hs_engine_run advances until the stop rule. */
+int hs_progress_arm(HsCounters *C, int32_t n_occ, double t_max, double MCsteps_max, void *stream);
+/* Ends a device-armed progress(): progress = 0, done = 0 (plain steps run again). */
+int hs_progress_disarm(HsCounters *C, void *stream);
+/* Coarse-grained readout (RegionalOutputReader / OOPSquareChessOutputReader.read_state,
+ * hotspice/io.py:362-380, 438-446): for region r with cell rectangle rects[4r..4r+3] =
+ * {y0, y1, x0, x1} (half-open, clipped to the lattice), out[r] = sum m * wx / norm[r] and, when
+ * wy is not NULL, out[n_regions + r] = sum m * wy / norm[r]. */
+int hs_region_readout(const int8_t *m, int32_t nx, int32_t ny, int32_t n_regions, const int32_t *rects, const double *wx,
+                      const double *wy, const double *norm, double *out, void *stream);
 
 /* ---- persistent multi-instance engine -------------------------------------------------------- */
 /* Advances n_inst instances (device array `insts`) in one launch of n_clusters thread-block

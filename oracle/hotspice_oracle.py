@@ -80,6 +80,15 @@ class OracleZeeman(OracleEnergy):
             self.E_factor = -mm.moment * mag
             self.E_factor_perp = np.zeros_like(mm.m)
 
+    def set_field(self, magnitude=None, angle=None):
+        """hotspice/energies.py:97-118."""
+        if magnitude is not None:
+            self.magnitude = magnitude
+        if angle is not None:
+            self.angle = angle
+        self._initialize()
+        self.update()
+
     def update(self):
         self.E = self.mm.m * self.E_factor
         if self.mm.USE_PERP_ENERGY:
@@ -493,6 +502,7 @@ class OracleMagnets:
         self.orientation = geom.orientation
         self.dx, self.dy = geom.dx, geom.dy
         self.x, self.y = geom.x, geom.y
+        self.geom_ixx, self.geom_iyy = np.meshgrid(np.arange(self.nx), np.arange(self.ny))
         self.x_min, self.x_max = float(self.x[0]), float(self.x[-1])
         self.y_min, self.y_max = float(self.y[0]), float(self.y[-1])
         with np.errstate(divide='ignore'):
@@ -1006,3 +1016,86 @@ def force_metropolis(mm: OracleMagnets, idx, accepted_mask, dt):
         mm.switches += sw.shape[1]
         mm.update_energy(sw)
     return sw
+
+
+# ----------------------------------------------------------------------------------------
+# Reservoir inputs and outputs (hotspice/io.py:193-500), the parts the fixtures exercise
+# ----------------------------------------------------------------------------------------
+def io_input(mm: OracleMagnets, kind, p, value):
+    """One Inputter.input_single call. kind / p: 'field' (FieldInputter, io.py:221-239,
+    constant magnitude), 'perp' (PerpFieldInputter, io.py:270-290), 'chess'
+    (OOPSquareChessFieldInputter, io.py:395-401), 'steps' (OOPSquareChessStepsInputter,
+    io.py:469-500)."""
+    Z = mm.get_energy('zeeman')
+    if kind == 'field':
+        if mm.in_plane:
+            Z.set_field(angle=p['angle'] % math.tau)
+        period = 1 / (1 + p['half_period'])
+        Z.set_field(magnitude=p['magnitude'] * value)
+        mm.progress(t_max=1 / p['frequency'] / (2 * period), MCsteps_max=p['n'] / (2 * period))
+        if not p['half_period']:
+            Z.set_field(magnitude=-p['magnitude'] * value)
+            mm.progress(t_max=.5 / p['frequency'], MCsteps_max=p['n'] / 2)
+    elif kind == 'perp':
+        angle = (p['angle'] % math.tau) + value * math.pi / 2
+        for mag in [p['magnitude'], -p['magnitude']]:
+            Z.set_field(magnitude=mag, angle=angle)
+            if p['relax']:
+                mm.minimize()
+            else:
+                mm.progress(t_max=0.5 / p['frequency'], MCsteps_max=p['n'])
+    elif kind == 'chess':
+        afm = (((mm.geom_ixx + mm.geom_iyy) % 2) * 2 - 1).astype(float)
+        Z.set_field(magnitude=afm * (2 * value - 1) * p['magnitude'])
+        mm.progress(t_max=1 / p['frequency'], MCsteps_max=p['n'])
+    elif kind == 'steps':
+        if p.get('binary'):
+            mag = (2 * value - 1) * p['magnitude']
+        else:
+            s_ = 0.5 - p['transition_range'] / 2
+            if value < s_:
+                mag = -p['magnitude'] + value * p['magnitude_range'] / s_
+            elif value > 1 - s_:
+                mag = p['magnitude'] + (value - 1) * p['magnitude_range'] / s_
+            else:
+                mag = 2 * (p['magnitude'] - p['magnitude_range']) / p['transition_range'] * (value - 0.5)
+        afm = ((mm.geom_ixx + mm.geom_iyy) % 2).astype(float)
+        Z.set_field(magnitude=afm * mag)
+        mm.progress(t_max=1 / p['frequency'], MCsteps_max=p['n'])
+        Z.set_field(magnitude=(afm - 1) * mag)
+        mm.progress(t_max=1 / p['frequency'], MCsteps_max=p['n'])
+    else:
+        raise ValueError(kind)
+
+
+def io_read(mm: OracleMagnets, kind, p):
+    """OutputReader.read_state: 'full' (io.py:328-332), 'regional' (io.py:346-379), 'chess'
+    (io.py:417-446)."""
+    if kind == 'full':
+        return mm.m[mm.nonzero].astype(float)
+    nxb, nyb = p['nx'], p['ny']
+    rx = np.tile(np.linspace(0, nxb * (1 - 1e-15), mm.nx, dtype=int), (mm.ny, 1))
+    ry = np.tile(np.linspace(0, nyb * (1 - 1e-15), mm.ny, dtype=int), (mm.nx, 1)).T
+    region = rx + nxb * ry
+    R = nxb * nyb
+    if kind == 'chess':
+        afm = ((mm.geom_ixx + mm.geom_iyy) % 2) * 2 - 1
+        masked = afm * mm.m
+        out = np.zeros(R)
+        for r in range(R):
+            out[r] = np.sum(masked[region == r]) / np.sum(mm.occupation[region == r])
+        return out
+    m = mm.m * mm.moment
+    out = np.zeros(2 * R if mm.in_plane else R)
+    norm = np.zeros(out.size)
+    for i in range(out.size):
+        sel = region == (i % R)
+        norm[i] = np.sum(mm.occupation[sel] * mm.moment[sel])
+    for r in range(R):
+        sel = region == r
+        if mm.in_plane:
+            out[r] = np.sum((m * mm.orientation[:, :, 0])[sel])
+            out[r + R] = np.sum((m * mm.orientation[:, :, 1])[sel])
+        else:
+            out[r] = np.sum(m[sel])
+    return out / norm

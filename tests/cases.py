@@ -71,6 +71,41 @@ def run_relaxation(mm, spec):
         mm.minimize(**spec['minimize'])
 
 
+def run_io_oracle(mo, spec):
+    """The oracle's input / readout loop of an 'io' scenario: one row of readouts per value."""
+    from oracle.hotspice_oracle import io_input, io_read
+    io = spec['io']
+    outs = []
+    for v in io['values']:
+        io_input(mo, io['inputter'], io['params'], v)
+        outs.append(io_read(mo, io['reader'], io['reader_params']))
+    return np.array(outs)
+
+
+def product_io_objects(mp, io):
+    """The product's Inputter / OutputReader of an 'io' scenario."""
+    from hotspice_b200 import io as hio
+    p = io['params']
+    kind = io['inputter']
+    if kind == 'field':
+        inp = hio.FieldInputter(hio.RandomScalarDatastream(), magnitude=p['magnitude'], angle=p['angle'], n=p['n'],
+                                sine=False, frequency=p['frequency'], half_period=p['half_period'])
+    elif kind == 'perp':
+        inp = hio.PerpFieldInputter(hio.RandomBinaryDatastream(), magnitude=p['magnitude'], angle=p['angle'], n=p['n'],
+                                    relax=p['relax'], frequency=p['frequency'])
+    elif kind == 'chess':
+        inp = hio.OOPSquareChessFieldInputter(hio.RandomBinaryDatastream(), magnitude=p['magnitude'], n=p['n'],
+                                              frequency=p['frequency'])
+    else:
+        ds = hio.RandomBinaryDatastream() if p.get('binary') else hio.RandomScalarDatastream()
+        inp = hio.OOPSquareChessStepsInputter(ds, magnitude=p['magnitude'], magnitude_range=p['magnitude_range'],
+                                              transition_range=p['transition_range'], n=p['n'], frequency=p['frequency'])
+    rp = io['reader_params']
+    rd = {'full': lambda: hio.FullOutputReader(mp), 'regional': lambda: hio.RegionalOutputReader(rp['nx'], rp['ny'], mp),
+          'chess': lambda: hio.OOPSquareChessOutputReader(rp['nx'], rp['ny'], mp)}[io['reader']]()
+    return inp, rd
+
+
 def dipolar_like(mm):
     """The DipolarEnergy or DiMonopolarEnergy of an instance (oracle or product), or None."""
     for name in ('dipolar', 'dimonopolar'):

@@ -59,6 +59,11 @@ def load_reference(ref_root):
     import hotspice.poisson  # noqa: F401
     import hotspice.core  # noqa: F401
     import hotspice.ASI  # noqa: F401
+    # hotspice/io.py imports show_m from the plotting module: an inert stand-in
+    pt = types.ModuleType('hotspice.plottools')
+    pt.show_m = lambda *a, **k: None
+    sys.modules['hotspice.plottools'] = pt
+    import hotspice.io  # noqa: F401
     return sys.modules['hotspice']
 
 
@@ -101,6 +106,32 @@ def _lattice(hs, spec):
     if kind == 'IP_Kagome':
         return hs.ASI.IP_Kagome(spec['a'], nx=spec['nx'], ny=spec['ny'], **kw)
     raise ValueError(kind)
+
+
+def io_objects(hs, io, mm):
+    """The reference Inputter / OutputReader of an 'io' scenario (hotspice/io.py)."""
+    hio = sys.modules['hotspice.io']
+    p = io['params']
+    kind = io['inputter']
+    if kind == 'field':
+        inp = hio.FieldInputter(hio.RandomScalarDatastream(), magnitude=p['magnitude'], angle=p['angle'], n=p['n'],
+                                sine=False, frequency=p['frequency'], half_period=p['half_period'])
+    elif kind == 'perp':
+        inp = hio.PerpFieldInputter(hio.RandomBinaryDatastream(), magnitude=p['magnitude'], angle=p['angle'], n=p['n'],
+                                    relax=p['relax'], frequency=p['frequency'])
+    elif kind == 'chess':
+        inp = hio.OOPSquareChessFieldInputter(hio.RandomBinaryDatastream(), magnitude=p['magnitude'], n=p['n'],
+                                              frequency=p['frequency'])
+    elif kind == 'steps':
+        ds = hio.RandomBinaryDatastream() if p.get('binary') else hio.RandomScalarDatastream()
+        inp = hio.OOPSquareChessStepsInputter(ds, magnitude=p['magnitude'], magnitude_range=p['magnitude_range'],
+                                              transition_range=p['transition_range'], n=p['n'], frequency=p['frequency'])
+    else:
+        raise ValueError(kind)
+    rp = io['reader_params']
+    rd = {'full': lambda: hio.FullOutputReader(mm), 'regional': lambda: hio.RegionalOutputReader(rp['nx'], rp['ny'], mm),
+          'chess': lambda: hio.OOPSquareChessOutputReader(rp['nx'], rp['ny'], mm)}[io['reader']]()
+    return inp, rd
 
 
 def run_spec(hs, spec):
@@ -163,6 +194,13 @@ def run_spec(hs, spec):
         mm.relax(**spec['relax'])
     if spec.get('minimize') is not None:
         mm.minimize(**spec['minimize'])
+    if spec.get('io') is not None:
+        inp, rd = io_objects(hs, spec['io'], mm)
+        outs = []
+        for v in spec['io']['values']:
+            inp.input(mm, values=[v])
+            outs.append(np.asarray(rd.read_state(mm), dtype=float).copy())
+        rec['io_outputs'] = np.array(outs)
     rec['final_counts'] = np.array([mm.switches, mm.attempted_switches, stream.call], dtype=np.int64)
     rec['m_final'] = mm.m.copy()
     rec['E_final'] = mm.E.copy()
@@ -245,6 +283,26 @@ SPECS = {
     'minimize_oop16': dict(BASE_OOP, nx=16, ny=16, seed=76, energies=[dict(type='dipolar'), dict(type='zeeman', B=3e-4)],
                            steps=0, minimize={}),
     'minimize_pin16': dict(BASE_PIN, nx=16, ny=16, seed=77, energies=[dict(type='dipolar')], steps=0, minimize={}),
+    # reservoir inputs and outputs (hotspice/io.py): field stimuli + progress()/minimize(), readouts
+    'io_chess_oop16': dict(BASE_OOP, nx=16, ny=16, seed=81, energies=[dict(type='dipolar'), dict(type='zeeman', B=0.0)], steps=0,
+                           io=dict(inputter='chess', params=dict(magnitude=4e-4, n=2, frequency=1.0), reader='chess',
+                                   reader_params=dict(nx=4, ny=4), values=[1, 0, 0, 1, 1, 0])),
+    'io_steps_oop12_metro': dict(BASE_OOP, nx=12, ny=12, seed=82, energies=[dict(type='dipolar'), dict(type='zeeman', B=0.0)],
+                                 steps=0, params=dict(UPDATE_SCHEME='Metropolis'),
+                                 io=dict(inputter='steps', params=dict(magnitude=6e-4, magnitude_range=2e-4, transition_range=0.4,
+                                                                       n=1.0, frequency=1.0),
+                                         reader='chess', reader_params=dict(nx=2, ny=3), values=[0.1, 0.45, 0.62, 0.95, 0.3])),
+    'io_field_pin16': dict(BASE_PIN, nx=16, ny=16, seed=83, energies=[dict(type='dipolar', cutoff=1.5e-6), dict(type='zeeman', B=0.0)],
+                           steps=0, io=dict(inputter='field', params=dict(magnitude=4e-3, angle=0.3, n=1.0, frequency=1.0,
+                                                                         half_period=True),
+                                            reader='regional', reader_params=dict(nx=4, ny=2), values=[0.3, -0.8, 0.1, 0.9, -0.55])),
+    'io_perp_pin12_relax': dict(BASE_PIN, nx=12, ny=12, seed=84, energies=[dict(type='dipolar'), dict(type='zeeman', B=0.0)], steps=0,
+                                io=dict(inputter='perp', params=dict(magnitude=3e-3, angle=0.2, n=2, relax=True, frequency=1.0),
+                                        reader='full', reader_params={}, values=[0, 1, 1, 0])),
+    'io_perp_pin12_progress': dict(BASE_PIN, nx=12, ny=12, seed=85, energies=[dict(type='dipolar'), dict(type='zeeman', B=0.0)],
+                                   steps=0, io=dict(inputter='perp', params=dict(magnitude=2e-3, angle=0.2, n=2, relax=False,
+                                                                                 frequency=1.0),
+                                                    reader='regional', reader_params=dict(nx=3, ny=3), values=[1, 0, 1])),
 }
 for name in ('metro_sq16_dimono_pbc', 'metro_pin32_grid', 'metro_pin24_pbc', 'metro_oop32_trunc_pbc', 'metro_oop30_trunc',
              'metro_oop16_time', 'metro_kagome_grid', 'metro_oop16_single'):

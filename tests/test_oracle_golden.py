@@ -5,7 +5,7 @@ counters, time and RNG call counts must agree exactly and energies to FP64 round
 import numpy as np
 import pytest
 
-from cases import build_oracle, dipolar_like, load_fixture, load_specs, rel_err, run_relaxation
+from cases import build_oracle, dipolar_like, load_fixture, load_specs, rel_err, run_io_oracle, run_relaxation
 from oracle.philox import PhiloxStream, philox4x32_10, uniform53
 
 SPECS = load_specs()
@@ -66,6 +66,8 @@ def test_oracle_matches_reference(name):
     assert np.array_equal(sw_y, fx['sw_y']) and np.array_equal(sw_x, fx['sw_x'])
     assert np.array_equal(sw_step, fx['sw_step'])
     run_relaxation(mm, spec)
+    if spec.get('io') is not None:
+        assert rel_err(run_io_oracle(mm, spec), fx['io_outputs']) < 1e-12
     if 'final_counts' in fx:
         assert [mm.switches, mm.attempted_switches, mm.rng.call] == fx['final_counts'].tolist()
     assert np.array_equal(mm.m, fx['m_final'])
