@@ -72,7 +72,7 @@ def test_set_field_device_equals_host(in_plane):
     if in_plane:
         assert rel_err(dev[1], host[1]) < 1e-15
     assert rel_err(dev[2], host[2]) < 1e-7
-    assert np.array_equal(_np(Z.magnitude), 2.5e-3 * _np(pat).astype(float))
+    assert np.array_equal(np.asarray(Z.magnitude), 2.5e-3 * _np(pat).astype(float))
 
 
 def test_large_reservoir_sequence():
