@@ -383,6 +383,9 @@ def run_product(args):
     relax = None
     if rank == 0 and args.relax_n > 0:
         relax = run_relax(dev, n=args.relax_n, cpu_seconds=0.0 if args.no_cpu_baseline else 10.0)
+    reservoir = None
+    if rank == 0 and args.reservoir_n > 0:
+        reservoir = run_reservoir(dev, n=args.reservoir_n, cpu_seconds=0.0 if args.no_cpu_baseline else 10.0)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -425,6 +428,8 @@ def run_product(args):
         line["incremental_update"] = incremental
     if relax is not None:
         line["relax"] = relax
+    if reservoir is not None:
+        line["reservoir"] = reservoir
     if not args.no_cpu_baseline:
         v, secs, st, ni = oracle_sample(specs, seconds_per_instance=args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
@@ -629,6 +634,75 @@ def run_relax(dev, n=1024, cpu_n=128, cpu_seconds=10.0):
     return out
 
 
+def run_reservoir(dev, n=256, inputs=100, cpu_n=64, cpu_seconds=10.0):
+    """Reservoir I/O stepping (f3): an OOP_Square n x n reservoir (dipolar cutoff 8.3a, Metropolis)
+    driven by a binary sequence through OOPSquareChessFieldInputter (1 MC step per input) and
+    read by OOPSquareChessOutputReader(8, 8) after every input. Timed three ways: run_sequence
+    (field, progress() and readout all enqueued on the device, one synchronisation), the
+    per-input public API (Inputter.input + read_state, synchronising per input), and the NumPy
+    oracle's restatement of the reference loop on a cpu_n x cpu_n lattice."""
+    import torch
+    import hotspice_b200 as hs
+    from hotspice_b200 import io as hio
+    vals = (np.random.Generator(np.random.PCG64(SEED + 5)).random(inputs) > 0.5).astype(int)
+
+    def make(nn, **kw):
+        return hs.ASI.OOP_Square(200e-9, nn, T=300, E_B=5e-20, moment=1.1e-15, pattern='random', seed=SEED, device=dev,
+                                 energies=[hs.DipolarEnergy(cutoff_range=8.3 * 200e-9), hs.ZeemanEnergy(0)],
+                                 params=hs.SimParams(UPDATE_SCHEME='Metropolis'), **kw)
+    inp = hio.OOPSquareChessFieldInputter(hio.RandomBinaryDatastream(), magnitude=8e-4, n=1, frequency=1)
+    out = {"workload": f"OOP_Square {n}x{n} reservoir, dipolar cutoff 8.3a, Metropolis grid, OOPSquareChessFieldInputter "
+                       f"(0.8 mT, 1 MC step per input), OOPSquareChessOutputReader 8x8, {inputs} binary inputs"}
+    a = make(n)
+    rd = hio.OOPSquareChessOutputReader(8, 8, a)
+    hio.run_sequence(a, inp, vals[:4], rd)             # warm-up (descriptors, graphs)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    att0 = a.attempted_switches
+    e0.record()
+    _, r = hio.run_sequence(a, inp, vals, rd)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - t0
+    mc = (a.attempted_switches - att0) / a.n
+    out["run_sequence"] = {"inputs_per_s": inputs / wall, "device_ms": e0.elapsed_time(e1), "wall_ms": wall * 1e3,
+                           "mc_steps": mc, "magnet_mcsteps_per_s": a.n * mc / wall}
+    b = make(n)
+    rb = hio.OOPSquareChessOutputReader(8, 8, b)
+    inp.input(b, values=vals[:4])
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for v in vals:
+        inp.input(b, values=[v])
+        rb.read_state(b)
+    torch.cuda.synchronize(dev)
+    wall_b = time.perf_counter() - t0
+    out["per_input_api"] = {"inputs_per_s": inputs / wall_b, "wall_ms": wall_b * 1e3}
+    out["sequence_over_api"] = wall_b / wall
+    del a, b
+    torch.cuda.empty_cache()
+    if cpu_seconds > 0:
+        from oracle import geometry as G
+        from oracle.hotspice_oracle import OracleDipolar, OracleMagnets, OracleZeeman, io_input, io_read
+        geo = G.oop_square(200e-9, cpu_n, cpu_n)
+        mc0 = np.random.Generator(np.random.PCG64(SEED)).integers(0, 2, size=(cpu_n, cpu_n)) * 2 - 1
+        mo = OracleMagnets(geo, mc0, T=300.0, E_B=5e-20, moment=1.1e-15, seed=SEED,
+                           energies=[OracleDipolar(cutoff_range=8.3 * 200e-9), OracleZeeman(0.0)],
+                           params=dict(UPDATE_SCHEME='Metropolis'))
+        t0 = time.perf_counter()
+        k = 0
+        while time.perf_counter() - t0 < cpu_seconds and k < inputs:
+            io_input(mo, 'chess', dict(magnitude=8e-4, n=1, frequency=1), int(vals[k]))
+            io_read(mo, 'chess', dict(nx=8, ny=8))
+            k += 1
+        secs = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": mo.n * mo.MCsteps / secs, "unit": "magnet-MCsteps/s", "cores": 1, "kind": "port",
+                               "sample": f"{k} inputs on OOP_Square {cpu_n}x{cpu_n} with the NumPy oracle ({secs:.1f} s)"}
+        out["gpu_over_cpu"] = out["run_sequence"]["magnet_mcsteps_per_s"] / out["cpu_baseline"]["value"]
+    return out
+
+
 SERVED_WORKLOAD = ("served: the first {k} requests of a seeded Poisson arrival stream (mean 200/s); lattice uniform over "
                    "{{OOP_Square a=200nm, IP_Pinwheel a=300nm, IP_Kagome a=500nm, exchange-only square Ising J=1e-21 J "
                    "(Wolff)}}, n log-uniform in [64,1024], steps log-uniform in [1e3,1e5], T uniform in [200,400]K, Zeeman "
@@ -741,6 +815,8 @@ def main():
     ap.add_argument('--only-incremental', action='store_true', help='run only the incremental-update timing and print it')
     ap.add_argument('--relax-n', type=int, default=1024, help='lattice side of the relax() timing (0: skip)')
     ap.add_argument('--only-relax', action='store_true', help='run only the relax() timing and print it')
+    ap.add_argument('--reservoir-n', type=int, default=256, help='lattice side of the reservoir I/O timing (0: skip)')
+    ap.add_argument('--only-reservoir', action='store_true', help='run only the reservoir I/O timing and print it')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)
@@ -749,6 +825,11 @@ def main():
         dev = torch.device('cuda', 0)
         torch.cuda.set_device(dev)
         print(json.dumps({"incremental_update": run_incremental(dev, n=args.incremental_n)}))
+    elif args.only_reservoir:
+        import torch
+        dev = torch.device('cuda', 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({"reservoir": run_reservoir(dev, n=args.reservoir_n)}))
     elif args.only_relax:
         import torch
         dev = torch.device('cuda', 0)

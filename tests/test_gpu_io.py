@@ -58,8 +58,8 @@ def test_public_api_equals_sequence(name):
 def test_set_field_device_equals_host(in_plane):
     import hotspice_b200 as hs
     if in_plane:
-        mm = hs.ASI.IP_Kagome(500e-9, 24, moment=np.linspace(1e-15, 2e-15, 24 * 24).reshape(24, 24),
-                              energies=[hs.ZeemanEnergy(1e-3, 0.4)])
+        mm = hs.ASI.IP_Kagome(500e-9, 24, energies=[hs.ZeemanEnergy(1e-3, 0.4)])
+        mm.moment = np.linspace(1e-15, 2e-15, mm.nx * mm.ny).reshape(mm.ny, mm.nx)
     else:
         mm = hs.ASI.OOP_Square(200e-9, 24, energies=[hs.ZeemanEnergy(1e-3)])
     Z = mm.get_energy('Zeeman')
