@@ -634,53 +634,78 @@ def run_relax(dev, n=1024, cpu_n=128, cpu_seconds=10.0):
     return out
 
 
-def run_reservoir(dev, n=256, inputs=100, cpu_n=64, cpu_seconds=10.0):
-    """Reservoir I/O stepping (f3): an OOP_Square n x n reservoir (dipolar cutoff 8.3a, Metropolis)
-    driven by a binary sequence through OOPSquareChessFieldInputter (1 MC step per input) and
-    read by OOPSquareChessOutputReader(8, 8) after every input. Timed three ways: run_sequence
-    (field, progress() and readout all enqueued on the device, one synchronisation), the
-    per-input public API (Inputter.input + read_state, synchronising per input), and the NumPy
-    oracle's restatement of the reference loop on a cpu_n x cpu_n lattice."""
+def run_reservoir(dev, n=256, inputs=20, batch=64, batch_n=128, cpu_n=64, cpu_seconds=10.0):
+    """Reservoir I/O stepping (f3): OOP_Square reservoirs (dipolar cutoff 8.3a, Metropolis grid)
+    driven by binary sequences through OOPSquareChessFieldInputter and read by
+    OOPSquareChessOutputReader(8, 8) after every input.
+    single:  one n x n reservoir, 1 MC step per input; run_sequence (field, progress() and
+             readout enqueued on the device, one synchronisation) against the per-input public
+             API (Inputter.input + read_state, synchronising per input);
+    batched: `batch` reservoirs of batch_n x batch_n, 0.25 MC steps per input, run_batch (one
+             persistent engine launch per input for all of them) against run_sequence of 4 of
+             them one after the other, scaled to the batch;
+    cpu:     the NumPy oracle's restatement of the reference loop on a cpu_n x cpu_n lattice."""
     import torch
     import hotspice_b200 as hs
     from hotspice_b200 import io as hio
-    vals = (np.random.Generator(np.random.PCG64(SEED + 5)).random(inputs) > 0.5).astype(int)
+    g = np.random.Generator(np.random.PCG64(SEED + 5))
 
-    def make(nn, **kw):
-        return hs.ASI.OOP_Square(200e-9, nn, T=300, E_B=5e-20, moment=1.1e-15, pattern='random', seed=SEED, device=dev,
+    def make(nn, seed=SEED):
+        return hs.ASI.OOP_Square(200e-9, nn, T=300, E_B=5e-20, moment=1.1e-15, pattern='random', seed=seed, device=dev,
                                  energies=[hs.DipolarEnergy(cutoff_range=8.3 * 200e-9), hs.ZeemanEnergy(0)],
-                                 params=hs.SimParams(UPDATE_SCHEME='Metropolis'), **kw)
+                                 params=hs.SimParams(UPDATE_SCHEME='Metropolis'))
+
+    def timed(fn):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize(dev)
+        return r, time.perf_counter() - t0
+    out = {"workload": f"OOP_Square reservoirs, dipolar cutoff 8.3a, Metropolis grid, OOPSquareChessFieldInputter 0.8 mT, "
+                       f"OOPSquareChessOutputReader 8x8; single {n}x{n} x {inputs} inputs of 1 MC step; batched "
+                       f"{batch} x {batch_n}x{batch_n} x {inputs} inputs of 0.25 MC step"}
+    vals = (g.random(inputs) > 0.5).astype(int)
     inp = hio.OOPSquareChessFieldInputter(hio.RandomBinaryDatastream(), magnitude=8e-4, n=1, frequency=1)
-    out = {"workload": f"OOP_Square {n}x{n} reservoir, dipolar cutoff 8.3a, Metropolis grid, OOPSquareChessFieldInputter "
-                       f"(0.8 mT, 1 MC step per input), OOPSquareChessOutputReader 8x8, {inputs} binary inputs"}
     a = make(n)
     rd = hio.OOPSquareChessOutputReader(8, 8, a)
-    hio.run_sequence(a, inp, vals[:4], rd)             # warm-up (descriptors, graphs)
-    torch.cuda.synchronize(dev)
-    t0 = time.perf_counter()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    hio.run_sequence(a, inp, vals[:2], rd)             # warm-up (descriptors)
     att0 = a.attempted_switches
-    e0.record()
-    _, r = hio.run_sequence(a, inp, vals, rd)
-    e1.record()
-    torch.cuda.synchronize(dev)
-    wall = time.perf_counter() - t0
+    _, wall = timed(lambda: hio.run_sequence(a, inp, vals, rd))
     mc = (a.attempted_switches - att0) / a.n
-    out["run_sequence"] = {"inputs_per_s": inputs / wall, "device_ms": e0.elapsed_time(e1), "wall_ms": wall * 1e3,
-                           "mc_steps": mc, "magnet_mcsteps_per_s": a.n * mc / wall}
     b = make(n)
     rb = hio.OOPSquareChessOutputReader(8, 8, b)
-    inp.input(b, values=vals[:4])
-    torch.cuda.synchronize(dev)
-    t0 = time.perf_counter()
-    for v in vals:
-        inp.input(b, values=[v])
-        rb.read_state(b)
-    torch.cuda.synchronize(dev)
-    wall_b = time.perf_counter() - t0
-    out["per_input_api"] = {"inputs_per_s": inputs / wall_b, "wall_ms": wall_b * 1e3}
-    out["sequence_over_api"] = wall_b / wall
+    inp.input(b, values=vals[:2])
+
+    def api():
+        for v in vals:
+            inp.input(b, values=[v])
+            rb.read_state(b)
+    _, wall_b = timed(api)
+    out["single"] = {"run_sequence_inputs_per_s": inputs / wall, "per_input_api_inputs_per_s": inputs / wall_b,
+                     "magnet_mcsteps_per_s": a.n * mc / wall}
     del a, b
+    # many reservoirs at once
+    inq = hio.OOPSquareChessFieldInputter(hio.RandomBinaryDatastream(), magnitude=8e-4, n=0.25, frequency=1)
+    bv = (g.random((batch, inputs)) > 0.5).astype(int)
+    mms = [make(batch_n, SEED + 1 + i) for i in range(batch)]
+    rds = [hio.OOPSquareChessOutputReader(8, 8, mm) for mm in mms]
+    hio.run_batch(mms, inq, bv[:, :1], rds)           # warm-up
+    att0 = sum(mm.attempted_switches for mm in mms)
+    _, wall_batch = timed(lambda: hio.run_batch(mms, inq, bv, rds))
+    mcs = sum(mm.attempted_switches for mm in mms) - att0
+    k = 4
+    seq = [make(batch_n, SEED + 1 + i) for i in range(k)]
+    for mm in seq:
+        hio.run_sequence(mm, inq, bv[0, :1], hio.OOPSquareChessOutputReader(8, 8, mm))
+    t_seq = 0.0
+    for i, mm in enumerate(seq):
+        _, w = timed(lambda: hio.run_sequence(mm, inq, bv[i], hio.OOPSquareChessOutputReader(8, 8, mm)))
+        t_seq += w
+    out["batched"] = {"reservoirs": batch, "wall_s": wall_batch, "reservoir_inputs_per_s": batch * inputs / wall_batch,
+                      "magnet_mcsteps_per_s": mcs / wall_batch,
+                      "sequential_wall_s_estimate": t_seq * batch / k,
+                      "batch_over_sequential": t_seq * batch / k / wall_batch}
+    del mms, seq
     torch.cuda.empty_cache()
     if cpu_seconds > 0:
         from oracle import geometry as G
@@ -699,7 +724,7 @@ def run_reservoir(dev, n=256, inputs=100, cpu_n=64, cpu_seconds=10.0):
         secs = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": mo.n * mo.MCsteps / secs, "unit": "magnet-MCsteps/s", "cores": 1, "kind": "port",
                                "sample": f"{k} inputs on OOP_Square {cpu_n}x{cpu_n} with the NumPy oracle ({secs:.1f} s)"}
-        out["gpu_over_cpu"] = out["run_sequence"]["magnet_mcsteps_per_s"] / out["cpu_baseline"]["value"]
+        out["batched_over_cpu"] = out["batched"]["magnet_mcsteps_per_s"] / out["cpu_baseline"]["value"]
     return out
 
 

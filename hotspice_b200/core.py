@@ -1025,10 +1025,14 @@ class Magnets(ABC):
             eng = BatchEngine([self], cluster_size=self.engine.cluster_size or None)
             c = (key, eng, eng._prepare([0], [dict(kwargs)]))
             self._pe_cache = c
-        st = self._stream()
-        _lib.check(self._lib.hs_progress_arm(self._counters.data_ptr(), self.n, float(t_max), float(MCsteps_max), st),
-                   'hs_progress_arm')
+        self._progress_arm(t_max, MCsteps_max)
         c[1].launch(c[2])
+
+    def _progress_arm(self, t_max: float, MCsteps_max: float):
+        """Arm progress(t_max, MCsteps_max) on the device (hs_progress_arm); the next engine
+        launch that runs this instance steps until the stop rule holds."""
+        _lib.check(self._lib.hs_progress_arm(self._counters.data_ptr(), self.n, float(t_max), float(MCsteps_max),
+                                             self._stream()), 'hs_progress_arm')
         self._ctl = None      # the device wrote t_max / progress / done: the host-side cache is stale
 
     def _progress_finish(self):

@@ -35,7 +35,8 @@ from .utils import lower_than
 __all__ = ['Datastream', 'ScalarDatastream', 'BinaryDatastream', 'IntegerDatastream', 'ConstantDatastream',
            'RandomBinaryDatastream', 'RandomIntegerDatastream', 'RandomScalarDatastream', 'Inputter', 'OutputReader',
            'FieldInputter', 'FieldInputterBinary', 'PerpFieldInputter', 'FullOutputReader', 'RegionalOutputReader',
-           'OOPSquareChessFieldInputter', 'OOPSquareChessOutputReader', 'OOPSquareChessStepsInputter', 'run_sequence']
+           'OOPSquareChessFieldInputter', 'OOPSquareChessOutputReader', 'OOPSquareChessStepsInputter', 'Stage',
+           'run_sequence', 'run_batch']
 
 
 # ------------------------------------------------------------------------------ datastreams
@@ -162,8 +163,29 @@ def _expand(inputter, values):
     return values
 
 
+class Stage:
+    """One field-then-progress step of an input: the Zeeman field magnitude * pattern (pattern
+    None: uniform) at ``angle`` (None: unchanged), then progress(t_max, MCsteps_max)."""
+    __slots__ = ('magnitude', 'pattern', 'angle', 't_max', 'mc_max')
+
+    def __init__(self, magnitude, pattern, angle, t_max, mc_max):
+        self.magnitude, self.pattern, self.angle, self.t_max, self.mc_max = magnitude, pattern, angle, t_max, mc_max
+
+
+def _run_stages(mm: Magnets, stages):
+    Zeeman = _zeeman(mm)
+    for st in stages:
+        Zeeman.set_field_device(st.magnitude, pattern=st.pattern, angle=st.angle)
+        mm._progress_enqueue(t_max=st.t_max, MCsteps_max=st.mc_max)
+
+
 class Inputter(ABC):
     """hotspice/io.py:73-106."""
+
+    def stages(self, mm: Magnets, value):
+        """The input of ``value`` as a list of :class:`Stage`, or None when it needs the host
+        between steps (then only input_single applies it)."""
+        return None
 
     def __init__(self, datastream: Datastream = None):
         self.datastream = ConstantDatastream(constant=1) if datastream is None else datastream
@@ -247,6 +269,16 @@ class FieldInputter(Inputter):
     def full_period(self):
         return not self.half_period
 
+    def stages(self, mm: Magnets, value):
+        if self.sine:
+            return None
+        angle = self.angle if mm.in_plane else None
+        period = 1 / (1 + self.half_period)
+        out = [Stage(self.magnitude * value, None, angle, 1 / self.frequency / (2 * period), self.n / (2 * period))]
+        if self.full_period:
+            out.append(Stage(-self.magnitude * value, None, None, .5 / self.frequency, self.n / 2))
+        return out
+
     def input_single(self, mm: Magnets, value: float | int):
         if self.sine and mm.params.UPDATE_SCHEME != Scheme.NEEL:
             raise AttributeError("Can not use temporal sine=True if UPDATE_SCHEME != Scheme.NEEL.")
@@ -262,11 +294,7 @@ class FieldInputter(Inputter):
                 Zeeman.set_field_device(self.magnitude * value * math.sin(progress * math.pi * 2 * period))
                 mm.update(t_max=min(1 - progress, 0.05) / self.frequency)
         else:
-            Zeeman.set_field_device(self.magnitude * value, angle=angle)
-            mm._progress_enqueue(t_max=1 / self.frequency / (2 * period), MCsteps_max=self.n / (2 * period))
-            if self.full_period:
-                Zeeman.set_field_device(-self.magnitude * value)
-                mm._progress_enqueue(t_max=.5 / self.frequency, MCsteps_max=self.n / 2)
+            _run_stages(mm, self.stages(mm, value))
 
 
 class FieldInputterBinary(FieldInputter):
@@ -275,6 +303,9 @@ class FieldInputterBinary(FieldInputter):
     def __init__(self, datastream: Datastream, magnitudes: tuple = (.8, 1), **kwargs):
         self.magnitude_ratio = magnitudes[0] / magnitudes[1]
         super().__init__(datastream, magnitude=magnitudes[1], half_period=False, **kwargs)
+
+    def stages(self, mm: Magnets, value):
+        return super().stages(mm, 1 if value else self.magnitude_ratio)
 
     def input_single(self, mm: Magnets, value: bool | int):
         super().input_single(mm, 1 if value else self.magnitude_ratio)
@@ -294,19 +325,24 @@ class PerpFieldInputter(FieldInputter):
         if not mm.in_plane:
             raise AttributeError("Can not use PerpFieldInputter on an out-of-plane ASI.")
 
+    def stages(self, mm: Magnets, value):
+        if self.relax:
+            return None
+        self._check(mm)
+        angle = self.angle + value * math.pi / 2
+        return [Stage(self.magnitude, None, angle, 0.5 / self.frequency, self.n),
+                Stage(-self.magnitude, None, angle, 0.5 / self.frequency, self.n)]
+
     def input_single(self, mm: Magnets, value: bool | int):
         self._check(mm)
-        Zeeman = _zeeman(mm)
-        angle = self.angle + value * math.pi / 2
         if self.relax:
+            Zeeman = _zeeman(mm)
+            angle = self.angle + value * math.pi / 2
             for mag in [self.magnitude, -self.magnitude]:
                 Zeeman.set_field_device(mag, angle=angle)
                 mm.minimize()
         else:
-            Zeeman.set_field_device(self.magnitude, angle=angle)
-            mm._progress_enqueue(t_max=0.5 / self.frequency, MCsteps_max=self.n)
-            Zeeman.set_field_device(-self.magnitude, angle=angle)
-            mm._progress_enqueue(t_max=0.5 / self.frequency, MCsteps_max=self.n)
+            _run_stages(mm, self.stages(mm, value))
 
     def input_single_generalized(self, mm: Magnets, value: bool | int):
         self._check(mm)
@@ -344,10 +380,11 @@ class OOPSquareChessFieldInputter(Inputter):
         self.n = n
         self.frequency = frequency
 
+    def stages(self, mm: OOP_Square, value):
+        return [Stage((2 * value - 1) * self.magnitude, _checkerboard(mm, 'pm'), None, 1 / self.frequency, self.n)]
+
     def input_single(self, mm: OOP_Square, value: bool | int):
-        Zeeman = _zeeman(mm)
-        Zeeman.set_field_device((2 * value - 1) * self.magnitude, pattern=_checkerboard(mm, 'pm'))
-        mm._progress_enqueue(t_max=1 / self.frequency, MCsteps_max=self.n)
+        _run_stages(mm, self.stages(mm, value))
 
 
 class OOPSquareChessStepsInputter(Inputter):
@@ -362,13 +399,13 @@ class OOPSquareChessStepsInputter(Inputter):
         self.frequency = frequency
         self.transform = self._get_transform_func()
 
-    def input_single(self, mm: OOP_Square, value: float | int | bool):
-        Zeeman = _zeeman(mm)
+    def stages(self, mm: OOP_Square, value):
         magnitude = self.transform(value)
-        Zeeman.set_field_device(magnitude, pattern=_checkerboard(mm, '01'))    # 0 / 1 checkerboard
-        mm._progress_enqueue(t_max=1 / self.frequency, MCsteps_max=self.n)
-        Zeeman.set_field_device(magnitude, pattern=_checkerboard(mm, 'm10'))   # -1 / 0, the other half
-        mm._progress_enqueue(t_max=1 / self.frequency, MCsteps_max=self.n)
+        return [Stage(magnitude, _checkerboard(mm, '01'), None, 1 / self.frequency, self.n),     # 0 / 1 checkerboard
+                Stage(magnitude, _checkerboard(mm, 'm10'), None, 1 / self.frequency, self.n)]   # -1 / 0, the other half
+
+    def input_single(self, mm: OOP_Square, value: float | int | bool):
+        _run_stages(mm, self.stages(mm, value))
 
     def _get_transform_func(self):
         if isinstance(self.datastream, (BinaryDatastream, IntegerDatastream)):
@@ -551,3 +588,52 @@ def run_sequence(mm: Magnets, inputter: Inputter, values=None, reader: OutputRea
             reader.read_into(mm, out[k])
     mm._progress_finish()
     return values, out
+
+
+def run_batch(mms, inputter: Inputter, values, readers=None):
+    """Drive several reservoirs at once: instance i receives the sequence ``values[i]`` (or
+    the shared 1-D ``values``) and is read by ``readers[i]`` after every input. Per input
+    stage the fields and progress() stop rules of all instances are set on the device, then
+    ONE persistent engine launch advances every instance until its own stop rule holds
+    (instances are independent: each result equals its :func:`run_sequence`). The inputter
+    must describe its inputs as stages (every input except the sinusoidal FieldInputter and
+    PerpFieldInputter with relax=True). Returns a list of (len, reader.n) float64 device
+    tensors (None without readers); synchronises once, at the end."""
+    from .engine import BatchEngine
+    mms = list(mms)
+    M = len(mms)
+    vals = np.asarray(values)
+    vals = np.broadcast_to(vals, (M, vals.size)) if vals.ndim <= 1 else vals
+    if vals.shape[0] != M:
+        raise ValueError(f'values has {vals.shape[0]} rows for {M} instances')
+    K = vals.shape[1]
+    for mm in mms:
+        _zeeman(mm)                     # before the launch descriptors are made
+    outs = None
+    if readers is not None:
+        if len(readers) != M:
+            raise ValueError('one reader per instance')
+        for mm, rd in zip(mms, readers):
+            if rd.mm is not mm:
+                rd.configure_for(mm)
+        outs = [torch.empty((K, rd.n), device=mm.device, dtype=torch.float64) for mm, rd in zip(mms, readers)]
+    eng = BatchEngine(mms)
+    prepared = eng._prepare([0] * M, [{} for _ in mms])
+    for k in range(K):
+        bits = [_expand(inputter, np.asarray([vals[i, k]])) for i in range(M)]
+        for b in range(len(bits[0])):
+            plans = [inputter.stages(mm, bits[i][b]) for i, mm in enumerate(mms)]
+            if any(p is None for p in plans):
+                raise NotImplementedError(f'{type(inputter).__name__} needs the host between steps: use run_sequence')
+            for j in range(len(plans[0])):
+                for mm, plan in zip(mms, plans):
+                    st = plan[j]
+                    mm.get_energy('Zeeman', verbose=False).set_field_device(st.magnitude, pattern=st.pattern, angle=st.angle)
+                    mm._progress_arm(t_max=st.t_max, MCsteps_max=st.mc_max)
+                eng.launch(prepared)
+        if outs is not None:
+            for i, (mm, rd) in enumerate(zip(mms, readers)):
+                rd.read_into(mm, outs[i][k])
+    for mm in mms:
+        mm._progress_finish()
+    return outs

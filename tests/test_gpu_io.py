@@ -99,3 +99,38 @@ def test_large_reservoir_sequence():
         inp.input(b, values=[v])
         rows.append(rd.read_state(b).clone())
     assert torch.equal(out, torch.stack(rows))
+
+
+@pytest.mark.parametrize('name', ['io_chess_oop16', 'io_steps_oop12_metro', 'io_field_pin16', 'io_perp_pin12_progress'])
+def test_batch_equals_sequences(name):
+    """run_batch (one engine launch per input stage for all instances) gives every instance
+    the result of its own run_sequence, bit for bit: different seeds and input values per
+    instance."""
+    from hotspice_b200 import io as hio
+    spec = SPECS[name]
+    base = np.asarray(spec['io']['values'])
+    vals = np.stack([base, base[::-1], np.roll(base, 1)])
+    seeds = [spec['seed'], spec['seed'] + 100, spec['seed'] + 200]
+    alone = []
+    for v, sd in zip(vals, seeds):
+        mm = build_product(name, seed=sd)
+        inp, rd = product_io_objects(mm, spec['io'])
+        _, out = hio.run_sequence(mm, inp, v, rd)
+        alone.append((out, mm._m_dev.clone(), mm._read_counters()))
+    mms = [build_product(name, seed=sd) for sd in seeds]
+    objs = [product_io_objects(mm, spec['io']) for mm in mms]
+    outs = hio.run_batch(mms, objs[0][0], vals, [o[1] for o in objs])
+    for i, mm in enumerate(mms):
+        assert torch.equal(outs[i], alone[i][0]), f'instance {i}: readouts differ'
+        assert torch.equal(mm._m_dev, alone[i][1])
+        c = mm._read_counters()
+        for k in ('switches', 'attempted', 'rng_call', 't'):
+            assert c[k] == alone[i][2][k], (i, k)
+
+
+def test_batch_refuses_host_inputs():
+    import hotspice_b200 as hs
+    from hotspice_b200 import io as hio
+    mm = hs.ASI.IP_Pinwheel(300e-9, 12, energies=[hs.DipolarEnergy(), hs.ZeemanEnergy(0)])
+    with pytest.raises(NotImplementedError):
+        hio.run_batch([mm], hio.PerpFieldInputter(hio.RandomBinaryDatastream(), relax=True), [0, 1])
