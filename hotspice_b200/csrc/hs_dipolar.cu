@@ -28,44 +28,10 @@ constexpr int UPD_SCAN = 2;                        // switches per lane per stag
 constexpr int UPD_ROUND = UPD_WARPS * 32 * UPD_SCAN;
 constexpr int UPD_LOC = 2048;                      // staged switches per pass
 
-// Index ranges of the switch list whose rows can reach tile rows [ty0, ty0 + UPD_TY): all of
-// it, or, when the list is sorted by row and row_start[y] (y = 0..ny) gives the first index of
-// row y, the rows within the largest window half-height (two ranges when that wraps around).
-// The ranges are in increasing index order, so the staged switches (and the summation order)
-// are the same as with a scan of the whole list.
-HS_DEV int upd_ranges(const HsLattice &L, const int32_t *row_start, int nsw, int ty0, int *ra, int *rb) {
-    ra[0] = 0; rb[0] = nsw;
-    if (!row_start) return 1;
-    const int H = max(L.dip_wy, L.trunc_size ? min(L.trunc_size, L.ny - 1) : L.ny - 1);
-    const bool wrap = L.pbc || L.dip_wrap;
-    int ylo = ty0 - H, yhi = ty0 + UPD_TY - 1 + H;
-    if (!wrap) {
-        ylo = max(ylo, 0);
-        yhi = min(yhi, L.ny - 1);
-        ra[0] = row_start[ylo];
-        rb[0] = row_start[yhi + 1];
-        return 1;
-    }
-    if (yhi - ylo + 1 >= L.ny) return 1;
-    if (ylo < 0) {             // rows [0, yhi] and [ylo + ny, ny - 1]
-        ra[0] = 0; rb[0] = row_start[yhi + 1];
-        ra[1] = row_start[ylo + L.ny]; rb[1] = nsw;
-        return 2;
-    }
-    if (yhi >= L.ny) {         // rows [0, yhi - ny] and [ylo, ny - 1]
-        ra[0] = 0; rb[0] = row_start[yhi - L.ny + 1];
-        ra[1] = row_start[ylo]; rb[1] = nsw;
-        return 2;
-    }
-    ra[0] = row_start[ylo];
-    rb[0] = row_start[yhi + 1];
-    return 1;
-}
-
 template <int VEC>
 __global__ void __launch_bounds__(32 * UPD_WARPS, 4)
 dip_update_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev, int n_host, int semantics,
-                  const HsCounters *C, const int32_t *row_start) {
+                  const HsCounters *C) {
     if (C && C->done) return;
     const int nsw = n_sw_dev ? *n_sw_dev : n_host;
     if (nsw <= 0) return;
@@ -73,8 +39,6 @@ dip_update_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev, int n_h
     const int tiles_x = (L.nx + TX - 1) / TX;
     const int ty0 = (blockIdx.x / tiles_x) * UPD_TY;
     const int tx0 = (blockIdx.x % tiles_x) * TX;
-    int ra[2], rb[2];
-    const int nr = upd_ranges(L, row_start, nsw, ty0, ra, rb);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int x0 = tx0 + lane * VEC;
 
@@ -91,19 +55,18 @@ dip_update_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev, int n_h
     // a one-switch update is update_single in the reference (hotspice/core.py:250-253)
     const bool flip_perp = !(L.dip_keep_perp_sign && nsw > 1);
     const bool vec_rows = VEC == 4 && x0 + 3 < L.nx && (L.nx & 3) == 0;
-    for (int g = 0; g < nr; ++g)
-    for (int base = ra[g], end = rb[g]; base < end;) {
-        // Stage, in list order, the switches of [base, end) whose window reaches this tile. All
+    for (int base = 0; base < nsw;) {
+        // Stage, in list order, the switches of [base, ...) whose window reaches this tile. All
         // warps scan: warp w takes the block [s + w 32 UPD_SCAN, ...) of each round, its hits are
         // compacted in order behind those of the warps before it.
         int n = 0, s = base;
-        while (s < end && n + UPD_ROUND <= UPD_LOC) {
+        while (s < nsw && n + UPD_ROUND <= UPD_LOC) {
             int ky[UPD_SCAN], kx[UPD_SCAN], kmode[UPD_SCAN];
             bool val[UPD_SCAN];
 #pragma unroll
             for (int u = 0; u < UPD_SCAN; ++u) {
                 const int k = s + (warp * UPD_SCAN + u) * 32 + lane;
-                val[u] = k < end;
+                val[u] = k < nsw;
                 ky[u] = val[u] ? sw.y[k] : 0;
                 kx[u] = val[u] ? sw.x[k] : 0;
                 kmode[u] = (val[u] && sw.mode) ? sw.mode[k] : 0;
@@ -311,19 +274,14 @@ __global__ void dip_full_direct_kernel(HsLattice L, int fp64, double *E64, doubl
 
 }  // namespace
 
-int hs_launch_dipolar_update_rows(const HsLattice &L, const HsSwitchList &sw, const int32_t *n_sw_dev, int n_host,
-                                  int semantics, const HsCounters *C, const int32_t *row_start, cudaStream_t st) {
+int hs_launch_dipolar_update(const HsLattice &L, const HsSwitchList &sw, const int32_t *n_sw_dev, int n_host,
+                             int semantics, const HsCounters *C, cudaStream_t st) {
     const bool vec = (L.nx % 4) == 0;
     const int TX = vec ? 128 : 32;
     const int tiles = ((L.nx + TX - 1) / TX) * ((L.ny + UPD_TY - 1) / UPD_TY);
-    if (vec) dip_update_kernel<4><<<tiles, 32 * UPD_WARPS, 0, st>>>(L, sw, n_sw_dev, n_host, semantics, C, row_start);
-    else dip_update_kernel<1><<<tiles, 32 * UPD_WARPS, 0, st>>>(L, sw, n_sw_dev, n_host, semantics, C, row_start);
+    if (vec) dip_update_kernel<4><<<tiles, 32 * UPD_WARPS, 0, st>>>(L, sw, n_sw_dev, n_host, semantics, C);
+    else dip_update_kernel<1><<<tiles, 32 * UPD_WARPS, 0, st>>>(L, sw, n_sw_dev, n_host, semantics, C);
     return hs_check_launch("dip_update_kernel");
-}
-
-int hs_launch_dipolar_update(const HsLattice &L, const HsSwitchList &sw, const int32_t *n_sw_dev, int n_host,
-                             int semantics, const HsCounters *C, cudaStream_t st) {
-    return hs_launch_dipolar_update_rows(L, sw, n_sw_dev, n_host, semantics, C, nullptr, st);
 }
 
 int hs_launch_dipolar_full_direct(const HsLattice &L, int fp64, double *E64, double *Ep64, cudaStream_t st) {

@@ -14,10 +14,6 @@ int hs_check_launch(const char *what);
 // launchers
 int hs_launch_dipolar_update(const HsLattice &L, const HsSwitchList &sw, const int32_t *n_sw_dev, int n_host,
                              int semantics, const HsCounters *C, cudaStream_t st);
-// The same for a switch list sorted by row, with row_start[y] (y = 0..ny) the first index of
-// row y: each tile scans only the rows its windows can come from.
-int hs_launch_dipolar_update_rows(const HsLattice &L, const HsSwitchList &sw, const int32_t *n_sw_dev, int n_host,
-                                  int semantics, const HsCounters *C, const int32_t *row_start, cudaStream_t st);
 int hs_launch_dipolar_full_direct(const HsLattice &L, int fp64, double *E64, double *Ep64, cudaStream_t st);
 int64_t hs_neel_scratch(const HsLattice &L);
 int hs_launch_neel(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, double attempt_freq,

@@ -13,9 +13,7 @@
 //     relax_apply_kernel   order-preserving compaction into the switch list, the flips, the
 //                          counters; the list's truncated-window flag follows
 //                          DipolarEnergy.update_multiple's per-sublattice rule
-//     row_start_kernel     first list index of every row (the list is in row-major order)
-//     dip_update_kernel    (hs_dipolar.cu) consumes the list; each tile scans only the rows
-//                          whose windows can reach it
+//     dip_update_kernel    (hs_dipolar.cu) consumes the list
 // relax() adds, after every sweep, its stop rule: nothing switched, the state equals the one
 // two sweeps before, or int(sqrt(nx^2 + ny^2)) sweeps (relax_compare_kernel, relax_end_kernel).
 // Every kernel reads the control state from device memory and returns at once when the stop
@@ -72,7 +70,6 @@ struct RelaxBufs {
     int8_t *snap;        // 2 N (relax) / visited N (minimize)
     int32_t *cells;      // N (minimize)
     int32_t *hist;       // MN_PASSES * MN_BINS (minimize)
-    int32_t *row_start;  // ny + 1: first switch-list index of every row (the lists here are row-sorted)
 };
 
 HS_DEV uint64_t u53_bits(uint64_t seed, uint64_t call, uint32_t e) {
@@ -539,18 +536,6 @@ __global__ void __launch_bounds__(RX_T) mn_mode_kernel(HsLattice L, const HsCoun
     }
 }
 
-// First index of every row in a switch list sorted by row (relax and minimize write theirs in
-// row-major order): row_start[r] = k for the rows r in (y[k-1], y[k]], with y[-1] = -1 and
-// y[n] = ny, so every row 0..ny is written exactly once.
-__global__ void __launch_bounds__(RX_T) row_start_kernel(HsSwitchList sw, const HsCounters *C, int ny, int32_t *row_start) {
-    const int n = C->n_sw;
-    for (int k = blockIdx.x * RX_T + threadIdx.x; k <= n; k += gridDim.x * RX_T) {
-        const int yk = k < n ? min(max(sw.y[k], 0), ny) : ny;
-        const int yp = k > 0 ? min(max(sw.y[k - 1], -1), ny) : -1;
-        for (int r = yp + 1; r <= yk; ++r) row_start[r] = k;
-    }
-}
-
 // ---------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------
@@ -574,7 +559,6 @@ int64_t layout(const HsLattice &L, char *base, RelaxBufs *B) {
     b.snap = reinterpret_cast<int8_t *>(take(2 * N));
     b.cells = reinterpret_cast<int32_t *>(take(4 * N));
     b.hist = reinterpret_cast<int32_t *>(take(4LL * MN_PASSES * MN_BINS));
-    b.row_start = reinterpret_cast<int32_t *>(take(4LL * (L.ny + 1)));
     if (B) *B = b;
     return off;
 }
@@ -649,10 +633,8 @@ int hs_relax_subset_impl(const HsLattice &L, HsCounters *C, const HsSwitchList &
     if ((rc = hs_check_launch("relax_decide_kernel"))) return rc;
     relax_apply_kernel<<<nblk, RX_T, 0, st>>>(L, C, B, sw, i, sx, sy, simultaneous, nblk);
     if ((rc = hs_check_launch("relax_apply_kernel"))) return rc;
-    if (!L.has_dipolar) return HS_OK;
-    row_start_kernel<<<std::max(1, std::min(nblk * RX_PER, 148 * 4)), RX_T, 0, st>>>(sw, C, L.ny, B.row_start);
-    if ((rc = hs_check_launch("row_start_kernel"))) return rc;
-    return hs_launch_dipolar_update_rows(L, sw, &C->n_sw, 0, HS_UPDATE_MULTIPLE, C, B.row_start, st);
+    if (L.has_dipolar) return hs_launch_dipolar_update(L, sw, &C->n_sw, 0, HS_UPDATE_MULTIPLE, C, st);
+    return HS_OK;
 }
 
 int hs_relax_check_impl(const HsLattice &L, HsCounters *C, int n_max, void *scratch, int64_t bytes, cudaStream_t st) {
@@ -708,8 +690,6 @@ int hs_minimize_step_impl(const HsLattice &L, HsCounters *C, const HsSwitchList 
     if ((rc = hs_check_launch("mn_select_write_kernel"))) return rc;
     mn_mode_kernel<<<std::min(nblk, 148), RX_T, 0, st>>>(L, C, B, sw);
     if ((rc = hs_check_launch("mn_mode_kernel"))) return rc;
-    if (!L.has_dipolar) return HS_OK;
-    row_start_kernel<<<std::max(1, std::min(nblk * RX_PER, 148 * 4)), RX_T, 0, st>>>(sw, C, L.ny, B.row_start);
-    if ((rc = hs_check_launch("row_start_kernel"))) return rc;
-    return hs_launch_dipolar_update_rows(L, sw, &C->n_sw, 0, HS_UPDATE_MULTIPLE, C, B.row_start, st);
+    if (L.has_dipolar) return hs_launch_dipolar_update(L, sw, &C->n_sw, 0, HS_UPDATE_MULTIPLE, C, st);
+    return HS_OK;
 }
