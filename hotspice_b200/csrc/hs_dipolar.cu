@@ -21,15 +21,29 @@
 
 namespace {
 
-constexpr int UPD_WARPS = 8;                       // warps per CTA
-constexpr int UPD_RPW = 2;                         // rows per warp
+// Tile shape and occupancy of the incremental update (compile-time; the defaults are the
+// measured best on B200 for the benchmarked windows).
+#ifndef HS_UPD_WARPS
+#define HS_UPD_WARPS 8
+#endif
+#ifndef HS_UPD_RPW
+#define HS_UPD_RPW 2
+#endif
+#ifndef HS_UPD_MIN_CTAS
+#define HS_UPD_MIN_CTAS 4
+#endif
+#ifndef HS_UPD_SCAN
+#define HS_UPD_SCAN 2
+#endif
+constexpr int UPD_WARPS = HS_UPD_WARPS;            // warps per CTA
+constexpr int UPD_RPW = HS_UPD_RPW;                // rows per warp
 constexpr int UPD_TY = UPD_WARPS * UPD_RPW;        // rows per tile
-constexpr int UPD_SCAN = 2;                        // switches per lane per staging round
+constexpr int UPD_SCAN = HS_UPD_SCAN;              // switches per lane per staging round
 constexpr int UPD_ROUND = UPD_WARPS * 32 * UPD_SCAN;
 constexpr int UPD_LOC = 2048;                      // staged switches per pass
 
 template <int VEC>
-__global__ void __launch_bounds__(32 * UPD_WARPS, 4)
+__global__ void __launch_bounds__(32 * UPD_WARPS, HS_UPD_MIN_CTAS)
 dip_update_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev, int n_host, int semantics,
                   const HsCounters *C) {
     if (C && C->done) return;
