@@ -18,6 +18,7 @@ HS_ST_SELECT_RETRY, HS_ST_SWITCH_OVERFLOW, HS_ST_POISSON_OVERFLOW, HS_ST_WOLFF_O
 HS_SAMPLE_SINGLE, HS_SAMPLE_GRID, HS_SAMPLE_POISSON = 0, 1, 2
 HS_BARRIER_SIMPLE, HS_BARRIER_PARABOLIC = 0, 1
 HS_UPDATE_SINGLE, HS_UPDATE_MULTIPLE = 0, 1
+HS_SEGMENT_MAX = 65536
 
 P = C.c_void_p
 
@@ -102,6 +103,7 @@ SIGNATURES = {
     'hs_progress_arm': (C.c_int, [P, C.c_int32, C.c_double, C.c_double, P]),
     'hs_progress_disarm': (C.c_int, [P, P]),
     'hs_region_readout': (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, P, P, P, P, P, P]),
+    'hs_segments_copy': (C.c_int, [P, P, C.c_int32, C.c_int32, P]),
     'hs_engine_run': (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, P, P]),
     'hs_engine_max_clusters': (C.c_int, [C.c_int32]),
     'hs_exchange_energy': (C.c_int, [C.POINTER(HsLattice), P, P, P]),

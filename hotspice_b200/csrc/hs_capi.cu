@@ -282,6 +282,12 @@ int hs_region_readout(const int8_t *m, int32_t nx, int32_t ny, int32_t n_regions
     return hs_region_readout_impl(m, nx, ny, n_regions, rects, wx, wy, norm, out, (cudaStream_t)stream);
 }
 
+int hs_segments_copy(void *staged, const HsSegment *segs, int32_t n, int32_t to_device, void *stream) {
+    if (n < 0 || (n > 0 && (!staged || !segs))) { hs_set_error("hs_segments_copy: bad arguments"); return HS_EINVAL; }
+    if (n == 0) return HS_OK;
+    return hs_segments_copy_impl(staged, segs, n, to_device ? 1 : 0, (cudaStream_t)stream);
+}
+
 int hs_engine_run(const HsInstance *insts, int32_t n_inst, int32_t cluster_size, int32_t n_clusters, int32_t *work,
                   void *stream) {
     if (!insts || !work || n_inst < 0 || n_clusters <= 0) { hs_set_error("hs_engine_run: bad arguments"); return HS_EINVAL; }

@@ -324,6 +324,110 @@ class BatchEngine:
         torch.cuda.current_stream(self.device).wait_stream(side)
         return CapturedRun(g, prepared, self)
 
+    # ---------------------------------------------------------------- packed state transfer
+    STATE_FIELDS = ('m', 'mm', 'C', 'E', 'Ep')
+
+    @staticmethod
+    def _field_tensor(mm: Magnets, f: str):
+        if f == 'm':
+            return mm._m_dev
+        if f == 'mm':
+            return mm._mm_dev
+        if f == 'C':
+            return mm._counters
+        d = mm._dipolar()
+        if d is None:
+            return None
+        return d._E if f == 'E' else d._Ep
+
+    def state_layout(self, fields=STATE_FIELDS):
+        """Layout of the packed state of ``fields`` ('m' int8 spins, 'mm' FP32 m * moment, 'C'
+        HsCounters, 'E' / 'Ep' FP64 dipolar energies): [(instance, field, offset, bytes)] with
+        every array at a 256-byte aligned offset, and the total size in bytes."""
+        out, off = [], 0
+        for i, mm in enumerate(self.magnets):
+            for f in fields:
+                t = self._field_tensor(mm, f)
+                if t is None:
+                    continue
+                nb = t.numel() * t.element_size()
+                out.append((i, f, off, nb))
+                off += -(-nb // 256) * 256
+        return out, off
+
+    def _segments(self, fields):
+        """Device table of HsSegment entries (at most HS_SEGMENT_MAX bytes each) for ``fields``,
+        cached on the arrays' addresses."""
+        lay, total = self.state_layout(fields)
+        ptrs = tuple(self._field_tensor(self.magnets[i], f).data_ptr() for i, f, _, _ in lay)
+        key = (tuple(fields), ptrs)
+        c = getattr(self, '_seg_cache', {}).get(key)
+        if c is None:
+            rows = []
+            for (i, f, off, nb), p in zip(lay, ptrs):
+                for k in range(0, nb, _lib.HS_SEGMENT_MAX):
+                    rows.append((off + k, p + k, min(_lib.HS_SEGMENT_MAX, nb - k)))
+            arr = np.array(rows, dtype=[('staged', '<i8'), ('device', '<u8'), ('bytes', '<i8')])
+            t = torch.from_numpy(arr.view(np.uint8).copy()).pin_memory().to(self.device, non_blocking=True)
+            c = (t, len(rows), total, lay)
+            if not hasattr(self, '_seg_cache'):
+                self._seg_cache = {}
+            self._seg_cache[key] = c
+        return c
+
+    def _staging(self, which, nbytes):
+        buf = getattr(self, '_stage_' + which, None)
+        if buf is None or buf.numel() < nbytes:
+            buf = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
+            setattr(self, '_stage_' + which, buf)
+        return buf
+
+    def _gather(self, fields, stream):
+        segs, n, total, _ = self._segments(fields)
+        stage = self._staging('out', total)
+        _lib.check(self.lib.hs_segments_copy(stage.data_ptr(), segs.data_ptr(), n, 0, stream), 'hs_segments_copy')
+        return stage, total
+
+    def pack_host(self, fields=STATE_FIELDS) -> torch.Tensor:
+        """The instances' current device state of ``fields`` packed (layout :meth:`state_layout`)
+        into a new pinned host buffer; synchronises."""
+        st = torch.cuda.current_stream(self.device)
+        stage, total = self._gather(fields, st.cuda_stream)
+        host = torch.empty(total, dtype=torch.uint8).pin_memory()
+        host.copy_(stage[:total], non_blocking=True)
+        st.synchronize()
+        return host
+
+    def run_from_host(self, steps, host_in: torch.Tensor, in_fields=STATE_FIELDS, host_out: torch.Tensor | None = None,
+                      out_fields=('m', 'C'), sizes=None, **kwargs):
+        """Load every instance's state from the packed pinned host buffer ``host_in`` (ONE host to
+        device copy and one scatter kernel, hs_segments_copy), run ``steps`` like :meth:`run`,
+        and gather ``out_fields`` into the pinned host buffer ``host_out`` (one gather kernel and
+        ONE device to host copy). Asynchronous: synchronise the stream before reading host_out.
+        The run controls (progress, done, t_max) come from the loaded counters; :meth:`run` writes
+        only the ones that differ from what it needs."""
+        st = torch.cuda.current_stream(self.device)
+        segs, n, total, lay = self._segments(in_fields)
+        if host_in.numel() < total:
+            raise ValueError(f'host_in holds {host_in.numel()} bytes, the layout needs {total}')
+        stage = self._staging('in', total)
+        stage[:total].copy_(host_in[:total], non_blocking=True)
+        _lib.check(self.lib.hs_segments_copy(stage.data_ptr(), segs.data_ptr(), n, 1, st.cuda_stream), 'hs_segments_copy')
+        if 'C' in in_fields:
+            raw = host_in.numpy()
+            for i, f, off, nb in lay:
+                if f == 'C':
+                    rec = np.frombuffer(raw[off:off + nb].tobytes(), dtype=_lib.COUNTERS_DTYPE)[0]
+                    self.magnets[i]._ctl = {'progress': int(rec['progress']), 'done': int(rec['done']),
+                                            't_max': float(rec['t_max'])}
+        prepared = self.run(steps, sizes=sizes, **kwargs)
+        if host_out is not None:
+            out_stage, out_total = self._gather(out_fields, st.cuda_stream)
+            if host_out.numel() < out_total:
+                raise ValueError(f'host_out holds {host_out.numel()} bytes, the layout needs {out_total}')
+            host_out[:out_total].copy_(out_stage[:out_total], non_blocking=True)
+        return prepared
+
     def progress(self, t_max=1.0, MCsteps_max=4.0, **kwargs):
         """The reference's progress() for every instance at once; returns [(dt, dMCsteps)]."""
         starts = []

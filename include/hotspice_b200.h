@@ -278,6 +278,22 @@ int hs_progress_disarm(HsCounters *C, void *stream);
 int hs_region_readout(const int8_t *m, int32_t nx, int32_t ny, int32_t n_regions, const int32_t *rects, const double *wx,
                       const double *wy, const double *norm, double *out, void *stream);
 
+/* ---- packed state transfer for batches (no reference counterpart: it replaces the per-array
+ * host<->device copies of a batch's start states and results) ---------------------------------- */
+/* One segment: `bytes` bytes at offset `staged` of a staging buffer <-> device address `device`.
+ * Segments of at most HS_SEGMENT_MAX bytes spread the copy over the SMs (one CTA per segment). */
+#define HS_SEGMENT_MAX 65536
+typedef struct HsSegment {
+    int64_t  staged;
+    uint64_t device;
+    int64_t  bytes;
+} HsSegment;
+/* Scatters the device-resident staging buffer `staged` into the segments' addresses
+ * (to_device = 1) or gathers them into it (to_device = 0); `segs` is a device array of n
+ * segments. With one host<->device copy of the staging buffer this moves a whole batch's state
+ * in two operations. */
+int hs_segments_copy(void *staged, const HsSegment *segs, int32_t n, int32_t to_device, void *stream);
+
 /* ---- persistent multi-instance engine -------------------------------------------------------- */
 /* Advances n_inst instances (device array `insts`) in one launch of n_clusters thread-block
  * clusters of `cluster_size` CTAs (1, 2, 4, 8 or 16). Each cluster claims instances from the
