@@ -404,7 +404,8 @@ HS_DEV WolffScratch wolff_scratch_of(const HsLattice &L, void *base) {
     S.cl_ep = reinterpret_cast<int32_t *>(p); p += hs_align_up_d(4 * N, 256);
     S.cl_layer = reinterpret_cast<int32_t *>(p); p += hs_align_up_d(4 * N, 256);
     S.list = reinterpret_cast<int32_t *>(p); p += hs_align_up_d(4 * N, 256);
-    S.cand = reinterpret_cast<int32_t *>(p);
+    S.cand = reinterpret_cast<int32_t *>(p); p += hs_align_up_d(4 * N, 256);
+    S.epoch = reinterpret_cast<int32_t *>(p);
     return S;
 }
 

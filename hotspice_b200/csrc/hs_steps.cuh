@@ -518,6 +518,8 @@ struct WolffScratch {
     int32_t *cl_layer; // layer in which it joined
     int32_t *list;     // cluster cells in BFS order (capacity N)
     int32_t *cand;     // frontier of the current layer (capacity N)
+    int32_t *epoch;    // last epoch used with these stamps; kept here, not in the counters, so that
+                       // restoring an earlier counter state never makes an old stamp current again
 };
 
 // One Wolff cluster step executed by one CTA.
@@ -531,7 +533,7 @@ HS_DEV void wolff_step_cta(const HsLattice &L, HsCounters *C, const HsSwitchList
     const int nx = L.nx, ny = L.ny;
     const int64_t N = (int64_t)nx * ny;
     uint64_t call = C->rng_call;
-    if (threadIdx.x == 0) { s_epoch = C->epoch + 1; C->epoch = s_epoch; }
+    if (threadIdx.x == 0) { s_epoch = *S.epoch + 1; *S.epoch = s_epoch; C->epoch = s_epoch; }
     // seed: _select_single (np.random.randint(n) -> nonzero index)
     const int seed = L.nonzero[(int)floor(hs_u53(L.seed, call, 0u) * L.n_occ)];
     call += 1;

@@ -25,7 +25,7 @@ __global__ void __launch_bounds__(WT) wolff_kernel(HsLattice L, HsCounters *C, H
 
 int64_t hs_wolff_scratch(const HsLattice &L) {
     const int64_t N = (int64_t)L.nx * L.ny;
-    return 5 * hs_align_up(4 * N, 256);
+    return 5 * hs_align_up(4 * N, 256) + 256;     // + the stamp epoch
 }
 
 int hs_launch_wolff(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, void *scratch, int64_t scratch_bytes,
@@ -45,7 +45,8 @@ int hs_launch_wolff(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, v
     S.cl_ep = reinterpret_cast<int32_t *>(p); p += hs_align_up(4 * N, 256);
     S.cl_layer = reinterpret_cast<int32_t *>(p); p += hs_align_up(4 * N, 256);
     S.list = reinterpret_cast<int32_t *>(p); p += hs_align_up(4 * N, 256);
-    S.cand = reinterpret_cast<int32_t *>(p);
+    S.cand = reinterpret_cast<int32_t *>(p); p += hs_align_up(4 * N, 256);
+    S.epoch = reinterpret_cast<int32_t *>(p);
     wolff_kernel<<<1, WT, 0, st>>>(L, C, sw, S);
     return hs_check_launch("wolff_kernel");
 }
