@@ -97,9 +97,10 @@ int hs_last_error(char *buf, int len) {
 }
 
 int hs_struct_sizes(int32_t *out, int n) {
-    const int32_t s[6] = {(int32_t)sizeof(HsLattice), (int32_t)sizeof(HsCounters), (int32_t)sizeof(HsSwitchList),
-                          (int32_t)sizeof(HsGridPlan), (int32_t)offsetof(HsLattice, nx), (int32_t)sizeof(HsInstance)};
-    for (int i = 0; i < n && i < 6; ++i) out[i] = s[i];
+    const int32_t s[7] = {(int32_t)sizeof(HsLattice), (int32_t)sizeof(HsCounters), (int32_t)sizeof(HsSwitchList),
+                          (int32_t)sizeof(HsGridPlan), (int32_t)offsetof(HsLattice, nx), (int32_t)sizeof(HsInstance),
+                          (int32_t)sizeof(HsSegment)};
+    for (int i = 0; i < n && i < 7; ++i) out[i] = s[i];
     return HS_OK;
 }
 

@@ -157,6 +157,21 @@ class CapturedRun:
         self.graph.replay()
 
 
+SEGMENT_DTYPE = np.dtype([('staged', '<i8'), ('device', '<u8'), ('bytes', '<i8')])   # HsSegment
+
+
+def segment_table(layout, ptrs, max_bytes=None) -> np.ndarray:
+    """HsSegment rows for a packed layout [(instance, field, staged offset, bytes)] and the
+    arrays' device addresses: every array split into pieces of at most ``max_bytes``
+    (HS_SEGMENT_MAX), each piece starting at the same offset into both sides."""
+    max_bytes = _lib.HS_SEGMENT_MAX if max_bytes is None else int(max_bytes)
+    rows = []
+    for (_, _, off, nb), p in zip(layout, ptrs):
+        for k in range(0, nb, max_bytes):
+            rows.append((off + k, p + k, min(max_bytes, nb - k)))
+    return np.array(rows, dtype=SEGMENT_DTYPE)
+
+
 class BatchEngine:
     """Advance several Magnets at once: ``run(steps)`` (fixed step budgets) or
     ``progress(t_max, MCsteps_max)`` (the reference's stop rule, per instance)."""
@@ -363,12 +378,8 @@ class BatchEngine:
         key = (tuple(fields), ptrs)
         c = getattr(self, '_seg_cache', {}).get(key)
         if c is None:
-            rows = []
-            for (i, f, off, nb), p in zip(lay, ptrs):
-                for k in range(0, nb, _lib.HS_SEGMENT_MAX):
-                    rows.append((off + k, p + k, min(_lib.HS_SEGMENT_MAX, nb - k)))
-            arr = np.array(rows, dtype=[('staged', '<i8'), ('device', '<u8'), ('bytes', '<i8')])
-            t = torch.from_numpy(arr.view(np.uint8).copy()).pin_memory().to(self.device, non_blocking=True)
+            rows = segment_table(lay, ptrs)
+            t = torch.from_numpy(rows.view(np.uint8).copy()).pin_memory().to(self.device, non_blocking=True)
             c = (t, len(rows), total, lay)
             if not hasattr(self, '_seg_cache'):
                 self._seg_cache = {}

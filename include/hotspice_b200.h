@@ -174,7 +174,9 @@ typedef struct HsInstance {
 /* ---- library ------------------------------------------------------------------------- */
 int hs_version(void);
 int hs_last_error(char *buf, int len);
-/* sizeof of the ABI structs, so bindings can check their mirrors */
+/* Sizes of the ABI structs, so bindings can check their mirrors; the first n of: sizeof
+ * HsLattice, HsCounters, HsSwitchList, HsGridPlan, offsetof(HsLattice, nx), HsInstance,
+ * HsSegment. */
 int hs_struct_sizes(int32_t *out, int n);
 
 /* n doubles u53 of Philox call `call` into out (device). */

@@ -137,3 +137,32 @@ def test_shard_requests_two_ranks_gloo():
     assert not (a & b)
     assert a | b == set(range(200))
     assert abs(len(a) - len(b)) < 100
+
+
+def test_segment_table_covers_packed_layout():
+    """The HsSegment table of the packed batch transfer: every array covered exactly once, pieces
+    of at most HS_SEGMENT_MAX bytes, staged and device sides advancing together, 16-byte
+    aligned piece starts when both bases are aligned (the kernel's vector path), and the
+    struct layout of the C header (24 bytes)."""
+    from hotspice_b200 import _lib
+    from hotspice_b200.engine import SEGMENT_DTYPE, segment_table
+    assert SEGMENT_DTYPE.itemsize == 24
+    import ctypes
+    sizes = (ctypes.c_int32 * 7)()
+    _lib.load().hs_struct_sizes(sizes, 7)
+    assert sizes[6] == SEGMENT_DTYPE.itemsize          # the library's sizeof(HsSegment)
+    sizes = [1, 15, 16, 1000, 65536, 65537, 300000]
+    layout, off = [], 0
+    for i, nb in enumerate(sizes):
+        layout.append((i, 'x', off, nb))
+        off += -(-nb // 256) * 256
+    ptrs = [0x7f0000000000 + 0x100000 * i for i in range(len(sizes))]
+    rows = segment_table(layout, ptrs)
+    assert np.all(rows['bytes'] > 0) and np.all(rows['bytes'] <= _lib.HS_SEGMENT_MAX)
+    for (i, _, o, nb), p in zip(layout, ptrs):
+        mine = rows[(rows['device'] >= p) & (rows['device'] < p + nb)]
+        assert int(mine['bytes'].sum()) == nb
+        assert np.all(mine['staged'] - o == mine['device'] - p)
+        assert np.all(mine['staged'] % 16 == 0) and np.all(mine['device'] % 16 == 0)
+    small = segment_table(layout, ptrs, max_bytes=4096)
+    assert int(small['bytes'].sum()) == sum(sizes) and np.all(small['bytes'] <= 4096)
