@@ -19,6 +19,13 @@ Deviations from the reference (deliberate, each checked by the tests):
   function written for cells, hotspice/core.py:564 -> hotspice/poisson.py:77,99, which
   always returns the single magnet (0,0)); ``poisson_compat=True`` reproduces the
   degenerate reference result.
+
+Restated only in part (each part pinned by reference fixtures):
+* ``minimize`` with ignore_barrier=True (with False the reference compares the
+  (barrier, barrier) tuple of E_barrier() against kBT and indexes the result as one array);
+* the reservoir inputs / outputs of hotspice/io.py used by the fixtures (``io_input``,
+  ``io_read``): constant-magnitude FieldInputter, PerpFieldInputter, the two checkerboard
+  inputters, and the full / regional / checkerboard readers.
 """
 from __future__ import annotations
 
