@@ -24,7 +24,7 @@ Restated only in part (each part pinned by reference fixtures):
 * ``minimize`` with ignore_barrier=True (with False the reference compares the
   (barrier, barrier) tuple of E_barrier() against kBT and indexes the result as one array);
 * the reservoir inputs / outputs of hotspice/io.py used by the fixtures (``io_input``,
-  ``io_read``): constant-magnitude FieldInputter, PerpFieldInputter, the two checkerboard
+  ``io_read``): FieldInputter, PerpFieldInputter, the two checkerboard
   inputters, and the full / regional / checkerboard readers.
 """
 from __future__ import annotations
@@ -1030,11 +1030,19 @@ def force_metropolis(mm: OracleMagnets, idx, accepted_mask, dt):
 # ----------------------------------------------------------------------------------------
 def io_input(mm: OracleMagnets, kind, p, value):
     """One Inputter.input_single call. kind / p: 'field' (FieldInputter, io.py:221-239,
-    constant magnitude), 'perp' (PerpFieldInputter, io.py:270-290), 'chess'
+    constant or sinusoidal magnitude), 'perp' (PerpFieldInputter, io.py:270-290), 'chess'
     (OOPSquareChessFieldInputter, io.py:395-401), 'steps' (OOPSquareChessStepsInputter,
     io.py:469-500)."""
     Z = mm.get_energy('zeeman')
-    if kind == 'field':
+    if kind == 'field' and p.get('sine'):
+        # io.py:228-233: the magnitude follows the sine, one update per field value
+        Z.set_field(angle=(p['angle'] % math.tau) if mm.in_plane else None)
+        mc0, t0 = mm.MCsteps, mm.t
+        period = 1 / (1 + p['half_period'])
+        while lower_than(progress := max((mm.MCsteps - mc0) / p['n'], (mm.t - t0) * p['frequency']), 1):
+            Z.set_field(magnitude=p['magnitude'] * value * math.sin(progress * math.pi * 2 * period))
+            mm.update(t_max=min(1 - progress, 0.05) / p['frequency'])
+    elif kind == 'field':
         if mm.in_plane:
             Z.set_field(angle=p['angle'] % math.tau)
         period = 1 / (1 + p['half_period'])

@@ -89,7 +89,7 @@ def product_io_objects(mp, io):
     kind = io['inputter']
     if kind == 'field':
         inp = hio.FieldInputter(hio.RandomScalarDatastream(), magnitude=p['magnitude'], angle=p['angle'], n=p['n'],
-                                sine=False, frequency=p['frequency'], half_period=p['half_period'])
+                                sine=p.get('sine', False), frequency=p['frequency'], half_period=p['half_period'])
     elif kind == 'perp':
         inp = hio.PerpFieldInputter(hio.RandomBinaryDatastream(), magnitude=p['magnitude'], angle=p['angle'], n=p['n'],
                                     relax=p['relax'], frequency=p['frequency'])

@@ -115,7 +115,7 @@ def io_objects(hs, io, mm):
     kind = io['inputter']
     if kind == 'field':
         inp = hio.FieldInputter(hio.RandomScalarDatastream(), magnitude=p['magnitude'], angle=p['angle'], n=p['n'],
-                                sine=False, frequency=p['frequency'], half_period=p['half_period'])
+                                sine=p.get('sine', False), frequency=p['frequency'], half_period=p['half_period'])
     elif kind == 'perp':
         inp = hio.PerpFieldInputter(hio.RandomBinaryDatastream(), magnitude=p['magnitude'], angle=p['angle'], n=p['n'],
                                     relax=p['relax'], frequency=p['frequency'])
@@ -296,6 +296,10 @@ SPECS = {
                            steps=0, io=dict(inputter='field', params=dict(magnitude=4e-3, angle=0.3, n=1.0, frequency=1.0,
                                                                          half_period=True),
                                             reader='regional', reader_params=dict(nx=4, ny=2), values=[0.3, -0.8, 0.1, 0.9, -0.55])),
+    'io_sine_oop12': dict(BASE_OOP, nx=12, ny=12, seed=86, energies=[dict(type='dipolar'), dict(type='zeeman', B=0.0)], steps=0,
+                          io=dict(inputter='field', params=dict(magnitude=1.5e-3, angle=0.0, n=0.5, frequency=2e3, half_period=True,
+                                                                sine=True),
+                                  reader='chess', reader_params=dict(nx=2, ny=2), values=[1.0, -0.6, 0.8])),
     'io_perp_pin12_relax': dict(BASE_PIN, nx=12, ny=12, seed=84, energies=[dict(type='dipolar'), dict(type='zeeman', B=0.0)], steps=0,
                                 io=dict(inputter='perp', params=dict(magnitude=3e-3, angle=0.2, n=2, relax=True, frequency=1.0),
                                         reader='full', reader_params={}, values=[0, 1, 1, 0])),
