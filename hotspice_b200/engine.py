@@ -409,21 +409,57 @@ class BatchEngine:
         st.synchronize()
         return host
 
-    def run_from_host(self, steps, host_in: torch.Tensor, in_fields=STATE_FIELDS, host_out: torch.Tensor | None = None,
-                      out_fields=('m', 'C'), sizes=None, **kwargs):
+    def upload(self, host_in: torch.Tensor, in_fields=STATE_FIELDS, slot: int = 0):
+        """Start the host to device copy of a packed state (pinned ``host_in``) into staging slot
+        ``slot`` on the engine's copy stream, so that it overlaps the launches running on the
+        compute stream; :meth:`run_from_host` with ``slot=`` then consumes it. A slot is reused
+        only after the scatter that read it has run."""
+        segs, n, total, lay = self._segments(in_fields)
+        if host_in.numel() < total:
+            raise ValueError(f'host_in holds {host_in.numel()} bytes, the layout needs {total}')
+        if not hasattr(self, '_copy_stream'):
+            self._copy_stream = torch.cuda.Stream(self.device)
+            self._slot_free, self._slot_ready, self._slot_host = {}, {}, {}
+        stage = self._staging(f'in{slot}', total)
+        cs = self._copy_stream
+        if slot in self._slot_free:
+            cs.wait_event(self._slot_free[slot])
+        with torch.cuda.stream(cs):
+            stage[:total].copy_(host_in[:total], non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(cs)
+        self._slot_ready[slot], self._slot_host[slot] = ev, host_in
+        return slot
+
+    def run_from_host(self, steps, host_in: torch.Tensor | None = None, in_fields=STATE_FIELDS,
+                      host_out: torch.Tensor | None = None, out_fields=('m', 'C'), sizes=None, slot: int | None = None,
+                      **kwargs):
         """Load every instance's state from the packed pinned host buffer ``host_in`` (ONE host to
         device copy and one scatter kernel, hs_segments_copy), run ``steps`` like :meth:`run`,
         and gather ``out_fields`` into the pinned host buffer ``host_out`` (one gather kernel and
         ONE device to host copy). Asynchronous: synchronise the stream before reading host_out.
+        With ``slot=`` the state was already sent by :meth:`upload` (the copy overlapped earlier
+        work) and ``host_in`` may be omitted.
         The run controls (progress, done, t_max) come from the loaded counters; :meth:`run` writes
         only the ones that differ from what it needs."""
         st = torch.cuda.current_stream(self.device)
         segs, n, total, lay = self._segments(in_fields)
-        if host_in.numel() < total:
-            raise ValueError(f'host_in holds {host_in.numel()} bytes, the layout needs {total}')
-        stage = self._staging('in', total)
-        stage[:total].copy_(host_in[:total], non_blocking=True)
+        if slot is None:
+            if host_in is None or host_in.numel() < total:
+                raise ValueError(f'host_in must hold the {total} bytes of the layout')
+            stage = self._staging('in', total)
+            stage[:total].copy_(host_in[:total], non_blocking=True)
+        else:
+            if slot not in getattr(self, '_slot_ready', {}):
+                raise ValueError(f'nothing was uploaded to slot {slot}')
+            st.wait_event(self._slot_ready.pop(slot))
+            host_in = self._slot_host.pop(slot)
+            stage = self._staging(f'in{slot}', total)
         _lib.check(self.lib.hs_segments_copy(stage.data_ptr(), segs.data_ptr(), n, 1, st.cuda_stream), 'hs_segments_copy')
+        if slot is not None:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            self._slot_free[slot] = ev
         if 'C' in in_fields:
             raw = host_in.numpy()
             for i, f, off, nb in lay:

@@ -128,9 +128,13 @@ def test_run_from_host_equals_per_array_loads():
         b[i]._ctl = None
     out_lay, out_total = ea.state_layout(('m', 'C'))
     host_out = torch.empty(out_total, dtype=torch.uint8).pin_memory()
-    for _ in range(2):                             # the same start state twice: identical results
-        ea.run_from_host(30, host_in, host_out=host_out)
-        torch.cuda.synchronize()
+    # the same start state twice: identical results; the second time through the overlapped
+    # upload slots
+    ea.run_from_host(30, host_in, host_out=host_out)
+    torch.cuda.synchronize()
+    ea.upload(host_in, slot=1)
+    ea.run_from_host(30, slot=1, host_out=host_out)
+    torch.cuda.synchronize()
     eb.run(30)
     torch.cuda.synchronize()
     for x, y in zip(a, b):
