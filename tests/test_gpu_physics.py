@@ -1,0 +1,58 @@
+"""Physics known answers of the reference's examples, reproduced by the device path at sizes
+where they are size-independent (statistical tolerances stated per test):
+
+* non-interacting magnets in a field (examples/Noninteracting.py): <M>/M0 = tanh(mu B / kB T);
+* 2-D exchange Ising square lattice (examples/OOP_Exchange.py): below T_c the spontaneous
+  magnetisation is Onsager's (1 - sinh(2J / kB T)^-4)^(1/8); above T_c it vanishes.
+"""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+kB = 1.380649e-23
+
+
+def test_noninteracting_tanh():
+    """IP_Square with no interactions, field at 45 degrees, Metropolis, 10 MC steps per field
+    (as the example does); 32768 magnets, so the standard error of <M>/M0 is ~0.006: tolerance
+    0.03."""
+    import hotspice_b200 as hs
+    T, moment = 300, 1.1e-15
+    Z = hs.ZeemanEnergy(magnitude=0, angle=math.pi / 4)
+    mm = hs.ASI.IP_Square(1, 256, moment=moment, energies=[Z], pattern='random', T=T, m_perp_factor=0, seed=3)
+    mm.params.UPDATE_SCHEME = hs.Scheme.METROPOLIS
+    mm.initialize_m('uniform', angle=math.pi / 4)
+    M0 = mm.m_avg
+    for alpha in (0.0, 0.5, 1.0, 2.0, 3.0):
+        Z.magnitude = alpha * kB * T / moment * math.sqrt(2)
+        mm.progress(MCsteps_max=10)
+        got = mm.m_avg / M0
+        assert abs(got - math.tanh(alpha)) < 0.03, (alpha, got, math.tanh(alpha))
+
+
+@pytest.mark.parametrize('scheme', ['Metropolis', 'Wolff'])
+def test_onsager_magnetisation(scheme):
+    """OOP_Square 128 x 128, PBC, exchange only, from the uniform state: after 60 MC steps of
+    equilibration, the mean |m| over 20 further MC steps matches Onsager's curve at
+    T = 0.85 and 0.93 T_c within 0.03 and is below 0.2 at 1.15 T_c (finite-size fluctuations)."""
+    import hotspice_b200 as hs
+    T_c = 1.0
+    J = T_c * kB * math.log(1 + math.sqrt(2)) / 2
+    params = hs.SimParams(UPDATE_SCHEME=scheme, MULTISAMPLING_SCHEME='cluster' if scheme == 'Wolff' else 'grid')
+    for t in (0.85, 0.93, 1.15):
+        mm = hs.ASI.OOP_Square(1, 128, energies=[hs.ExchangeEnergy(J=J)], pattern='uniform', PBC=True, T=t * T_c,
+                               params=params, seed=11)
+        mm.progress(t_max=math.inf, MCsteps_max=60)
+        ms = []
+        for _ in range(20):
+            mm.progress(t_max=math.inf, MCsteps_max=1)
+            ms.append(abs(mm.m_avg))
+        m = float(np.mean(ms))
+        k = math.sinh(2 * J / (kB * t * T_c)) ** -2
+        theory = (1 - k ** 2) ** (1 / 8) if k < 1 else 0.0
+        if t < 1:
+            assert abs(m - theory) < 0.03, (scheme, t, m, theory)
+        else:
+            assert m < 0.2, (scheme, t, m)
