@@ -32,11 +32,18 @@ def test_noninteracting_tanh():
         assert abs(got - math.tanh(alpha)) < 0.03, (alpha, got, math.tanh(alpha))
 
 
-@pytest.mark.parametrize('scheme', ['Metropolis', 'Wolff'])
+@pytest.mark.parametrize('scheme', ['Metropolis'])
 def test_onsager_magnetisation(scheme):
     """OOP_Square 128 x 128, PBC, exchange only, from the uniform state: after 60 MC steps of
     equilibration, the mean |m| over 20 further MC steps matches Onsager's curve at
-    T = 0.85 and 0.93 T_c within 0.03 and is below 0.2 at 1.15 T_c (finite-size fluctuations)."""
+    T = 0.85 and 0.93 T_c within 0.03 and is below 0.2 at 1.15 T_c (finite-size fluctuations).
+
+    Metropolis only, as in the reference's example. The reference's Wolff clusters
+    (hotspice/core.py:597-601) give each frontier cell a single attempt, with the number of
+    cluster neighbours it has when first reached; bonds to cells that join later are never
+    tried, so the clusters are smaller than Wolff's and the ordered phase is not stationary
+    (|m| decays to ~0.2 at 0.85 T_c on 32^2 in the oracle as well). The device path reproduces
+    those reference clusters exactly (test_gpu_parity.py), not Onsager."""
     import hotspice_b200 as hs
     T_c = 1.0
     J = T_c * kB * math.log(1 + math.sqrt(2)) / 2
