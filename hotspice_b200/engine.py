@@ -381,8 +381,8 @@ class BatchEngine:
             rows = segment_table(lay, ptrs)
             t = torch.from_numpy(rows.view(np.uint8).copy()).pin_memory().to(self.device, non_blocking=True)
             c = (t, len(rows), total, lay)
-            if not hasattr(self, '_seg_cache'):
-                self._seg_cache = {}
+            if not hasattr(self, '_seg_cache') or len(self._seg_cache) >= 8:
+                self._seg_cache = {}          # instance sets changed: drop the old tables
             self._seg_cache[key] = c
         return c
 

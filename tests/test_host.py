@@ -213,3 +213,25 @@ def test_truncated_window_sum_matches_convolve2d():
             crop = K[ny - 1 - ky:ny + ky, nx - 1 - kx:nx + kx]
             ref = signal.convolve2d(sf, crop, mode='same', boundary='wrap' if PBC else 'fill')
             assert np.allclose(got, ref, rtol=1e-12, atol=1e-12)
+
+
+def test_new_entry_points_reject_bad_arguments_without_a_launch():
+    """The relaxation, reservoir I/O and packed-transfer entry points validate their arguments on
+    the host and return HS_EINVAL before any launch (so this runs without a GPU)."""
+    import ctypes as C
+    from hotspice_b200 import _lib
+    lib = _lib.load()
+    L, sw = _lib.HsLattice(), _lib.HsSwitchList()
+    assert lib.hs_segments_copy(None, None, -1, 1, None) == _lib.HS_EINVAL
+    assert lib.hs_segments_copy(None, None, 0, 1, None) == _lib.HS_OK          # nothing to move
+    assert lib.hs_region_readout(None, 4, 4, 1, None, None, None, None, None, None) == _lib.HS_EINVAL
+    assert lib.hs_zeeman_set(0, 0, None, None, None, 1.0, 0.0, None, None, None, None, None) == _lib.HS_EINVAL
+    assert lib.hs_progress_arm(None, 1, 1.0, 1.0, None) == _lib.HS_EINVAL
+    assert lib.hs_progress_disarm(None, None) == _lib.HS_EINVAL
+    assert lib.hs_relax_scratch_bytes(C.byref(L)) == -1                          # empty lattice
+    assert lib.hs_minimize_step(C.byref(L), None, C.byref(sw), 0.3, None, 0, None) == _lib.HS_EINVAL
+    assert lib.hs_relax_check(C.byref(L), None, 1, None, 0, None) == _lib.HS_EINVAL
+    assert lib.hs_minimize_all(C.byref(L), None, C.byref(sw), 1, 0, None, 0, None) == _lib.HS_EINVAL
+    buf = C.create_string_buffer(256)
+    lib.hs_last_error(buf, 256)
+    assert buf.value                                                            # a message was left
