@@ -14,7 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, 'libhotspice_sm100.so')
 
 HS_OK, HS_EINVAL, HS_ENOMEM, HS_ETIMEDOUT, HS_ECUDA, HS_ERANGE = 0, -1, -2, -3, -4, -5
-HS_ST_SELECT_RETRY, HS_ST_SWITCH_OVERFLOW, HS_ST_POISSON_OVERFLOW, HS_ST_WOLFF_OVERFLOW = 1, 2, 4, 8
+HS_ST_SELECT_RETRY, HS_ST_SWITCH_OVERFLOW, HS_ST_POISSON_OVERFLOW, HS_ST_WOLFF_OVERFLOW, HS_ST_STEP_CAP = 1, 2, 4, 8, 16
+HS_PROGRESS_STEPS_MAX = 1 << 22
 HS_SAMPLE_SINGLE, HS_SAMPLE_GRID, HS_SAMPLE_POISSON = 0, 1, 2
 HS_BARRIER_SIMPLE, HS_BARRIER_PARABOLIC = 0, 1
 HS_UPDATE_SINGLE, HS_UPDATE_MULTIPLE = 0, 1

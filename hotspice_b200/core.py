@@ -102,6 +102,13 @@ class History:
         self.E.clear(); self.T.clear(); self.t.clear(); self.m.clear()
 
 
+def check_progress_limits(t_max, MCsteps_max):
+    """progress() stops when either limit is reached (hotspice/core.py:753-760); with both
+    infinite it would run forever, so that is refused."""
+    if not (float(t_max) < math.inf or float(MCsteps_max) < math.inf):
+        raise ValueError('progress() needs a finite t_max or MCsteps_max: with both infinite it never ends')
+
+
 def _ptr(t):
     return None if t is None else t.data_ptr()
 
@@ -897,6 +904,7 @@ class Magnets(ABC):
     def progress(self, t_max: float = 1, MCsteps_max: float = 4., stepwise: bool = False, **kwargs):
         """hotspice/core.py:736-760. Non-stepwise runs execute on the device in chunks of
         ``EngineConfig.graph_steps`` steps (CUDA-graph replays) and synchronise per chunk."""
+        check_progress_limits(t_max, MCsteps_max)
         if stepwise:
             return self._progress_stepwise(t_max=t_max, MCsteps_max=MCsteps_max, **kwargs)
         if self._T_zero:
@@ -1013,6 +1021,7 @@ class Magnets(ABC):
         hs_progress_arm sets the stop rule from the device counters, then one persistent engine
         launch steps until it holds. Call :meth:`_progress_finish` after the last one (it ends
         the armed state). Without the persistent engine this falls back to progress()."""
+        check_progress_limits(t_max, MCsteps_max)
         if not self.engine.persistent:
             self.progress(t_max=t_max, MCsteps_max=MCsteps_max, **kwargs)
             return

@@ -54,6 +54,35 @@ int check_lattice(const HsLattice *L, const char *who) {
 }
 }  // namespace
 
+int hs_check_metropolis_plan(const HsLattice *L, const HsGridPlan *P, const char *who) {
+    int rc = check_lattice(L, who);
+    if (rc) return rc;
+    if (!P) { hs_set_error("%s: null plan", who); return HS_EINVAL; }
+    if (P->sample_scheme == HS_SAMPLE_GRID && (!P->phase_off || !P->phase_yx || P->Rx < 1 || P->Ry < 1 || P->n_sc < 1)) {
+        hs_set_error("%s: bad grid plan", who); return HS_EINVAL;
+    }
+    if (P->sample_scheme == HS_SAMPLE_POISSON) {
+        if (!(P->r_cells >= 0.0) || !(P->r_cells < 1e9)) { hs_set_error("%s: bad Poisson radius", who); return HS_EINVAL; }
+        if (hs_poisson_grid_cells(*L, *P) > HS_POISSON_GRID_MAX) {
+            hs_set_error("%s: Poisson-disc background grid of %.0f cells exceeds %d", who, hs_poisson_grid_cells(*L, *P),
+                         HS_POISSON_GRID_MAX);
+            return HS_ERANGE;
+        }
+    }
+    if (P->sample_scheme != HS_SAMPLE_GRID && P->sample_scheme != HS_SAMPLE_POISSON && P->sample_scheme != HS_SAMPLE_SINGLE) {
+        hs_set_error("%s: unknown sample scheme %d", who, P->sample_scheme); return HS_EINVAL;
+    }
+    return HS_OK;
+}
+
+int hs_check_metropolis_args(const HsLattice *L, const HsCounters *C, const HsSwitchList *sw, const HsGridPlan *P,
+                             const char *who) {
+    int rc = hs_check_metropolis_plan(L, P, who);
+    if (rc) return rc;
+    if (!C || !sw) { hs_set_error("%s: null argument", who); return HS_EINVAL; }
+    return HS_OK;
+}
+
 void hs_set_error(const char *fmt, ...) {
     va_list ap;
     va_start(ap, fmt);
@@ -161,21 +190,15 @@ int hs_neel_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, doub
 }
 
 int64_t hs_metropolis_scratch_bytes(const HsLattice *L, const HsGridPlan *P) {
-    if (check_lattice(L, "hs_metropolis_scratch_bytes") || !P) return -1;
+    if (hs_check_metropolis_plan(L, P, "hs_metropolis_scratch_bytes")) return -1;
     return hs_metropolis_scratch(*L, *P);
 }
 
 int hs_metropolis_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, const HsGridPlan *P, void *scratch,
                        int64_t scratch_bytes, void *stream) {
-    int rc = check_lattice(L, "hs_metropolis_step");
+    int rc = hs_check_metropolis_args(L, C, sw, P, "hs_metropolis_step");
     if (rc) return rc;
-    if (!C || !sw || !P || !scratch) { hs_set_error("hs_metropolis_step: null argument"); return HS_EINVAL; }
-    if (P->sample_scheme == HS_SAMPLE_GRID && (!P->phase_off || !P->phase_yx || P->Rx < 1 || P->Ry < 1 || P->n_sc < 1)) {
-        hs_set_error("hs_metropolis_step: bad grid plan"); return HS_EINVAL;
-    }
-    if (P->sample_scheme == HS_SAMPLE_POISSON && !(P->r_cells >= 0.0)) {
-        hs_set_error("hs_metropolis_step: bad Poisson radius"); return HS_EINVAL;
-    }
+    if (!scratch) { hs_set_error("hs_metropolis_step: null scratch"); return HS_EINVAL; }
     return hs_launch_metropolis(*L, C, *sw, *P, scratch, scratch_bytes, (cudaStream_t)stream);
 }
 
@@ -266,6 +289,10 @@ int hs_zeeman_set(int64_t n_cells, int32_t in_plane, const double *moment, const
 
 int hs_progress_arm(HsCounters *C, int32_t n_occ, double t_max, double MCsteps_max, void *stream) {
     if (!C || n_occ <= 0) { hs_set_error("hs_progress_arm: bad arguments"); return HS_EINVAL; }
+    if (!(t_max < INFINITY) && !(MCsteps_max < INFINITY)) {
+        hs_set_error("hs_progress_arm: t_max and MCsteps_max are both infinite (the run would never end)");
+        return HS_EINVAL;
+    }
     return hs_progress_arm_impl(C, n_occ, t_max, MCsteps_max, (cudaStream_t)stream);
 }
 

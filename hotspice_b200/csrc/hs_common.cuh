@@ -47,6 +47,14 @@ HS_DEV float hs_log_exp1_f32(double u) {
     return logf(e1);
 }
 
+// Cells of the Poisson-disc background grid (hotspice/poisson.py:78-83 in cell units), as a
+// double so that no radius overflows it; the entry points refuse grids above HS_POISSON_GRID_MAX.
+constexpr int HS_POISSON_GRID_MAX = 1 << 28;
+HS_HD inline double hs_poisson_grid_cells(const HsLattice &L, const HsGridPlan &P) {
+    const double r = P.r_cells + 1.0, cs = r / sqrt(2.0);
+    return ceil(L.nx / cs) * ceil(L.ny / cs);
+}
+
 // ---------------------------------------------------------------------------------------
 // Lattice helpers
 // ---------------------------------------------------------------------------------------

@@ -453,11 +453,17 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
         }
         __syncthreads();
         const int scheme = s_I.scheme;
+        // progress() runs: at most `budget` steps in this launch; an unfinished run keeps done = 0
+        // and the next launch continues it, so every launch ends
+        const int64_t budget = I.steps > 0 ? I.steps : (int64_t)HS_PROGRESS_STEPS_MAX;
         for (int64_t st = 0;; ++st) {
             if (rank == 0 && threadIdx.x == 0) {
                 int go;
                 if (C->done) go = 0;
-                else if (C->progress) { go = hs_progress_continue(C, L.n_occ); if (!go) { C->done = 1; C->n_sw = 0; } }
+                else if (C->progress) {
+                    if (C->status || st >= budget) go = 0;   // a failed step, or the budget: not done
+                    else { go = hs_progress_continue(C, L.n_occ); if (!go) { C->done = 1; C->n_sw = 0; } }
+                }
                 else go = st < I.steps;
                 Sync<CS>::publish(&s_go, go);
                 Sync<CS>::publish(&s_call, (unsigned long long)C->rng_call);

@@ -19,6 +19,12 @@ int64_t hs_neel_scratch(const HsLattice &L);
 int hs_launch_neel(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, double attempt_freq,
                    void *scratch, int64_t scratch_bytes, cudaStream_t st);
 int64_t hs_metropolis_scratch(const HsLattice &L, const HsGridPlan &P);
+// Validation shared by every Metropolis entry point (hs_capi.cu): the lattice, the plan and,
+// for Poisson-disc plans, a finite radius and a background grid of at most HS_POISSON_GRID_MAX
+// cells; the second form also checks the counters and the switch list.
+int hs_check_metropolis_plan(const HsLattice *L, const HsGridPlan *P, const char *who);
+int hs_check_metropolis_args(const HsLattice *L, const HsCounters *C, const HsSwitchList *sw, const HsGridPlan *P,
+                             const char *who);
 int hs_launch_metropolis(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, const HsGridPlan &P,
                          void *scratch, int64_t scratch_bytes, cudaStream_t st);
 int64_t hs_wolff_scratch(const HsLattice &L);

@@ -9,6 +9,8 @@
 //                        copies the step kernels read), from magnitude * pattern and the angle
 //   progress_arm_kernel  t0 = t, mc0 = attempted / n, the limits, progress = 1, done = 0: the
 //                        persistent engine launch that follows runs until the stop rule holds
+//                        (or its step budget is used up, which the next arm / disarm reports
+//                        as HS_ST_STEP_CAP)
 //   region_sum_kernel    one CTA per output region (a rectangle of cells), FP64 tree sum of
 //                        m * weight, divided by the region's normalisation
 #include "hs_common.cuh"
@@ -42,6 +44,7 @@ __global__ void __launch_bounds__(IO_T) zeeman_field_kernel(int64_t N, int in_pl
 }
 
 __global__ void progress_arm_kernel(HsCounters *C, int n_occ, double t_max, double mc_max) {
+    if (C->progress && !C->done) C->status |= HS_ST_STEP_CAP;   // the previous armed run did not finish
     C->t0 = C->t;
     C->mc0 = (double)C->attempted / (double)n_occ;
     C->t_max = t_max;
@@ -51,6 +54,7 @@ __global__ void progress_arm_kernel(HsCounters *C, int n_occ, double t_max, doub
 }
 
 __global__ void progress_disarm_kernel(HsCounters *C) {
+    if (C->progress && !C->done) C->status |= HS_ST_STEP_CAP;
     C->progress = 0;
     C->done = 0;
 }

@@ -73,23 +73,60 @@ int hs_launch_metropolis(const HsLattice &L, HsCounters *C, const HsSwitchList &
 // Poisson-disc working arrays live in one fixed file-scope device array instead. The array
 // exists once per GPU that loads this library and stays allocated until the process exits.
 // The first call on a device, made with that device current, looks up the array's device
-// address with cudaGetSymbolAddress; make that first call before any stream capture. Every
-// call shares the array and it keeps the previous call's contents: the kernel rewrites
-// every entry it reads (nothing has to start at zero), and calls that overlap on the GPU
-// (other streams, other threads) race on it.
+// address with cudaGetSymbolAddress; make that first call before any stream capture. The
+// address is kept with the id of the device's context: after a cudaDeviceReset (a new
+// primary context) the next call looks it up again, so that call too must come before any
+// capture. Every call shares the array and it keeps the previous call's contents: the kernel
+// rewrites every entry it reads (nothing has to start at zero), and calls that overlap on the
+// GPU (other streams, other threads) race on it.
 // ---------------------------------------------------------------------------------------
+#include <cuda.h>   // types of the two driver entry points below (resolved at run time)
 #include <mutex>
 
 #define HS_NOALLOC_METRO_BYTES (4LL << 20)   // 4 MiB
 #define HS_NOALLOC_MAX_DEVICES 64
 
 static __device__ __align__(256) unsigned char g_hs_metro_scratch[HS_NOALLOC_METRO_BYTES];
-static void *g_hs_metro_scratch_ptr[HS_NOALLOC_MAX_DEVICES];
-static std::mutex g_hs_metro_scratch_mu;
+
+namespace {
+struct NoallocSlot { void *ptr; unsigned long long ctx_id; };
+NoallocSlot g_noalloc[HS_NOALLOC_MAX_DEVICES];
+std::mutex g_noalloc_mu;
+typedef CUresult (*PfnCtxGetCurrent)(CUcontext *);
+typedef CUresult (*PfnCtxGetId)(CUcontext, unsigned long long *);
+PfnCtxGetCurrent g_ctx_current = nullptr;
+PfnCtxGetId g_ctx_id = nullptr;
+
+// Id of the calling thread's current context (0 when there is none or it cannot be read).
+unsigned long long current_ctx_id() {
+    if (!g_ctx_current) {
+        cudaDriverEntryPointQueryResult q1, q2;
+        void *f1 = nullptr, *f2 = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess || !f1 || !f2)
+            return 0;
+        g_ctx_id = reinterpret_cast<PfnCtxGetId>(f2);
+        g_ctx_current = reinterpret_cast<PfnCtxGetCurrent>(f1);
+    }
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (g_ctx_current(&c) != CUDA_SUCCESS || !c || g_ctx_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+}  // namespace
 
 extern "C" int hs_metropolis_step_noalloc(const HsLattice *L, HsCounters *C, const HsSwitchList *sw,
                                           const HsGridPlan *P, void *stream) {
-    if (!L || !C || !sw || !P) { hs_set_error("hs_metropolis_step_noalloc: null argument"); return HS_EINVAL; }
+    // every argument check before anything is sized or looked up
+    int rc = hs_check_metropolis_args(L, C, sw, P, "hs_metropolis_step_noalloc");
+    if (rc) return rc;
+    const int64_t need = hs_metropolis_scratch(*L, *P);
+    if (need > HS_NOALLOC_METRO_BYTES) {
+        hs_set_error("hs_metropolis_step_noalloc: this selection plan needs %lld bytes of scratch, the fixed "
+                     "scratch holds %lld; use hs_metropolis_step with a caller-provided buffer",
+                     (long long)need, (long long)HS_NOALLOC_METRO_BYTES);
+        return HS_ERANGE;
+    }
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) { hs_set_error("hs_metropolis_step_noalloc: cudaGetDevice: %s", cudaGetErrorString(e)); return HS_ECUDA; }
@@ -99,24 +136,20 @@ extern "C" int hs_metropolis_step_noalloc(const HsLattice *L, HsCounters *C, con
     }
     void *ptr;
     {
-        std::lock_guard<std::mutex> lock(g_hs_metro_scratch_mu);
-        ptr = g_hs_metro_scratch_ptr[dev];
-        if (!ptr) {  // set-up: once per device, with that device current
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        NoallocSlot &slot = g_noalloc[dev];
+        const unsigned long long id = current_ctx_id();
+        if (!slot.ptr || id == 0 || id != slot.ctx_id) {  // set-up: once per device (and per context)
+            ptr = nullptr;
             e = cudaGetSymbolAddress(&ptr, g_hs_metro_scratch);
             if (e != cudaSuccess || !ptr) {
                 hs_set_error("hs_metropolis_step_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
                 return HS_ECUDA;
             }
-            g_hs_metro_scratch_ptr[dev] = ptr;
+            slot.ptr = ptr;
+            slot.ctx_id = current_ctx_id();   // the look-up made the device's context current
         }
-    }
-    if (L->nx <= 0 || L->ny <= 0) { hs_set_error("hs_metropolis_step_noalloc: bad lattice size"); return HS_EINVAL; }
-    const int64_t need = hs_metropolis_scratch(*L, *P);
-    if (need > HS_NOALLOC_METRO_BYTES) {
-        hs_set_error("hs_metropolis_step_noalloc: this selection plan needs %lld bytes of scratch, the fixed "
-                     "scratch holds %lld; use hs_metropolis_step with a caller-provided buffer",
-                     (long long)need, (long long)HS_NOALLOC_METRO_BYTES);
-        return HS_ERANGE;
+        ptr = slot.ptr;
     }
     return hs_metropolis_step(L, C, sw, P, ptr, HS_NOALLOC_METRO_BYTES, stream);
 }

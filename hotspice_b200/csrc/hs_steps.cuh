@@ -679,8 +679,8 @@ HS_HD inline void hs_metro_sizes(const HsLattice &L, const HsGridPlan &P, int &c
     cap = P.n_sc > 1 ? P.n_sc : 1;
     gsz = 0;
     if (P.sample_scheme == HS_SAMPLE_POISSON) {
-        const double r = P.r_cells + 1.0, cs = r / sqrt(2.0);
-        gsz = (int)(ceil(L.nx / cs) * ceil(L.ny / cs));
+        const double g = hs_poisson_grid_cells(L, P);
+        gsz = g <= (double)HS_POISSON_GRID_MAX ? (int)g : HS_POISSON_GRID_MAX;   // validated by the entry points
         cap = cap > gsz ? cap : gsz;
     }
 }

@@ -426,6 +426,9 @@ class BatchEngine:
             cs.wait_event(self._slot_free[slot])
         with torch.cuda.stream(cs):
             stage[:total].copy_(host_in[:total], non_blocking=True)
+        # the buffer belongs to the compute stream's pool but is written on the copy stream: if a
+        # larger layout replaces it, its memory must not be reused before this copy has run
+        stage.record_stream(cs)
         ev = torch.cuda.Event()
         ev.record(cs)
         self._slot_ready[slot], self._slot_host[slot] = ev, host_in
@@ -475,22 +478,39 @@ class BatchEngine:
             host_out[:out_total].copy_(out_stage[:out_total], non_blocking=True)
         return prepared
 
+    #: steps an instance makes per engine launch of progress(); an unfinished run is continued
+    #: by the next launch, so no launch runs unboundedly long
+    progress_launch_steps = 1 << 16
+
     def progress(self, t_max=1.0, MCsteps_max=4.0, **kwargs):
-        """The reference's progress() for every instance at once; returns [(dt, dMCsteps)]."""
+        """The reference's progress() for every instance at once; returns [(dt, dMCsteps)].
+        Runs engine launches of at most ``progress_launch_steps`` steps per instance until every
+        instance's stop rule holds."""
+        from .core import check_progress_limits
+        check_progress_limits(t_max, MCsteps_max)
         starts = []
         for mm in self.magnets:
             c = mm._read_counters()
             t0, mc0 = float(c['t']), float(c['attempted']) / mm.n
             mm._write_counters(t0=t0, mc0=mc0, t_max=float(t_max), mc_max=float(MCsteps_max), progress=1, done=0)
             starts.append((t0, mc0))
-        prepared = self._prepare([0] * len(self.magnets), [dict(kwargs) for _ in self.magnets])
-        self.launch(prepared)
+        budget = max(1, int(self.progress_launch_steps))
+        prepared = self._prepare([budget] * len(self.magnets), [dict(kwargs) for _ in self.magnets])
+        self.launches = 0
+        while True:
+            self.launch(prepared)
+            self.launches += 1
+            counters = [mm._read_counters() for mm in self.magnets]
+            for c in counters:
+                st = int(c['status'])
+                if st:
+                    for mm in self.magnets:
+                        mm._write_counters(progress=0, done=0)
+                    raise RuntimeError(f'device step reported status {st} (HS_ST_* bits)')
+            if all(int(c['done']) for c in counters):
+                break
         out = []
-        for mm, (t0, mc0) in zip(self.magnets, starts):
-            c = mm._read_counters()
-            st = int(c['status'])
-            if st:
-                raise RuntimeError(f'device step reported status {st} (HS_ST_* bits)')
+        for mm, c, (t0, mc0) in zip(self.magnets, counters, starts):
             mm._write_counters(progress=0, done=0)
             out.append((float(c['t']) - t0, float(c['attempted']) / mm.n - mc0))
         return out

@@ -49,6 +49,12 @@ extern "C" {
 #define HS_ST_SWITCH_OVERFLOW 2  /* more switches than the switch list holds               */
 #define HS_ST_POISSON_OVERFLOW 4 /* Poisson-disc grid/queue capacity exceeded              */
 #define HS_ST_WOLFF_OVERFLOW 8   /* Wolff frontier capacity exceeded                       */
+#define HS_ST_STEP_CAP       16  /* a device-armed progress() run used its whole per-launch step
+                                    budget before its stop rule held (set by the next
+                                    hs_progress_arm / hs_progress_disarm)                     */
+
+/* Per-launch step budget of a progress() run in hs_engine_run when HsInstance.steps is 0. */
+#define HS_PROGRESS_STEPS_MAX (1 << 22)
 
 /* update schemes / selection / barrier (SimParams values, hotspice/core.py:29-41) */
 #define HS_SCHEME_NEEL        0
@@ -165,7 +171,8 @@ typedef struct HsInstance {
     HsCounters  *C;             /* device counters of this instance                           */
     void        *scratch;       /* Metropolis or Wolff working arrays (see *_scratch_bytes)   */
     int64_t      scratch_bytes;
-    int64_t      steps;         /* steps to run when C->progress == 0                         */
+    int64_t      steps;         /* steps to run when C->progress == 0; when C->progress == 1,
+                                   the most steps this launch makes (0: HS_PROGRESS_STEPS_MAX) */
     double       attempt_freq;
     int32_t      scheme;        /* HS_SCHEME_*                                                */
     int32_t      pad;
@@ -269,9 +276,12 @@ int hs_zeeman_set(int64_t n_cells, int32_t in_plane, const double *moment, const
                   double magnitude, double angle, double *E_factor, double *E_factor_perp, float *zee, float *zee_perp,
                   void *stream);
 /* Arms progress(t_max, MCsteps_max) (hotspice/core.py:736-760) from the device counters
- * (t0 = t, mc0 = attempted / n_occ); a following hs_engine_run advances until the stop rule. */
+ * (t0 = t, mc0 = attempted / n_occ); a following hs_engine_run advances until the stop rule.
+ * At least one limit must be finite. If a previous armed run is still unfinished (it used its
+ * step budget), HS_ST_STEP_CAP is set in C->status first. */
 int hs_progress_arm(HsCounters *C, int32_t n_occ, double t_max, double MCsteps_max, void *stream);
-/* Ends a device-armed progress(): progress = 0, done = 0 (plain steps run again). */
+/* Ends a device-armed progress(): progress = 0, done = 0 (plain steps run again); sets
+ * HS_ST_STEP_CAP when the armed run had not finished. */
 int hs_progress_disarm(HsCounters *C, void *stream);
 /* Coarse-grained readout (RegionalOutputReader / OOPSquareChessOutputReader.read_state,
  * hotspice/io.py:362-380, 438-446): for region r with cell rectangle rects[4r..4r+3] =
@@ -299,9 +309,12 @@ int hs_segments_copy(void *staged, const HsSegment *segs, int32_t n, int32_t to_
 /* ---- persistent multi-instance engine -------------------------------------------------------- */
 /* Advances n_inst instances (device array `insts`) in one launch of n_clusters thread-block
  * clusters of `cluster_size` CTAs (1, 2, 4, 8 or 16). Each cluster claims instances from the
- * device counter `work` (reset by this call) and runs each instance's step budget, or until its
- * progress() stop rule holds when C->progress is set. Replaces repeated update() calls
- * (hotspice/core.py:604-622, 736-760) for many simulations at once. */
+ * device counter `work` (reset by this call) and runs each instance's step budget, or, when
+ * C->progress is set, until its progress() stop rule holds (C->done = 1), a step reports a
+ * status bit, or the launch's step budget (HsInstance.steps, else HS_PROGRESS_STEPS_MAX) is
+ * used up; then C->done stays 0 and a further launch continues the run. Every launch ends.
+ * Replaces repeated update() calls (hotspice/core.py:604-622, 736-760) for many simulations at
+ * once. */
 int hs_engine_run(const HsInstance *insts, int32_t n_inst, int32_t cluster_size, int32_t n_clusters,
                   int32_t *work, void *stream);
 /* Number of clusters of `cluster_size` CTAs that can be resident at once (occupancy query). */

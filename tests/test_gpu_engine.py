@@ -149,3 +149,49 @@ def test_run_from_host_equals_per_array_loads():
             assert all(np.array_equal(x[k], y[k]) for k in _lib.COUNTERS_DTYPE.names if k != 'epoch'), i
         else:
             assert np.array_equal(ho[off:off + nb], ref), (i, f)
+
+
+@pytest.mark.parametrize('name', ['progress_oop12', 'progress_pin16_metro'])
+def test_progress_launch_budget(name):
+    """A progress() launch ends after its step budget with done = 0 (every launch ends, however
+    far the stop rule is); BatchEngine.progress continues the run over further launches, and
+    the result equals a run made in one launch, bit for bit."""
+    import hotspice_b200 as hs
+    from hotspice_b200.engine import BatchEngine
+    spec = SPECS[name]
+    # one launch with a 5-step budget and a stop rule far away: exactly 5 steps, not done
+    c = build_product(name, engine=hs.EngineConfig(persistent=True, cluster_size=1))
+    c._write_counters(t0=0.0, mc0=0.0, t_max=1e30, mc_max=1e12, progress=1, done=0)
+    s0 = int(c._read_counters()['steps'])
+    eng = BatchEngine([c], cluster_size=1)
+    eng.launch(eng._prepare([5], [{}]))
+    r = c._read_counters()
+    assert int(r['steps']) - s0 == 5 and int(r['done']) == 0 and int(r['status']) == 0
+    c._write_counters(progress=0, done=0)
+    # the same progress() split into launches of 3 steps, and in one launch
+    a = build_product(name, engine=hs.EngineConfig(persistent=True, cluster_size=1))
+    b = build_product(name, engine=hs.EngineConfig(persistent=True, cluster_size=1))
+    ea, eb = BatchEngine([a], cluster_size=1), BatchEngine([b], cluster_size=1)
+    ea.progress_launch_steps = 3
+    ra = ea.progress(**spec['progress'])
+    rb = eb.progress(**spec['progress'])
+    assert ea.launches > 1 and eb.launches == 1
+    assert ra == rb
+    _assert_same(_state(a), _state(b), f'{name} budget 3 vs one launch')
+
+
+def test_armed_progress_that_hits_its_budget_is_reported():
+    """A device-armed progress() (hs_progress_arm + engine launch, as the reservoir I/O uses)
+    whose launch ends at its step budget is flagged HS_ST_STEP_CAP by the next disarm, so the
+    host raises instead of reading a truncated run."""
+    import hotspice_b200 as hs
+    from hotspice_b200 import _lib
+    from hotspice_b200.engine import BatchEngine
+    a = build_product('progress_oop12', engine=hs.EngineConfig(persistent=True, cluster_size=1))
+    a._progress_arm(t_max=1e30, MCsteps_max=1e12)
+    eng = BatchEngine([a], cluster_size=1)
+    eng.launch(eng._prepare([4], [{}]))
+    with pytest.raises(RuntimeError, match='status 16'):
+        a._progress_finish()
+    assert int(a._read_counters()['status']) & _lib.HS_ST_STEP_CAP
+    a._write_counters(status=0)

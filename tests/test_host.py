@@ -235,3 +235,57 @@ def test_new_entry_points_reject_bad_arguments_without_a_launch():
     buf = C.create_string_buffer(256)
     lib.hs_last_error(buf, 256)
     assert buf.value                                                            # a message was left
+
+
+def _host_only_lattice(nx=64, ny=64):
+    """An HsLattice whose checks pass on the host; its pointers are host buffers, so it may
+    only reach code that refuses it before any launch."""
+    import ctypes as C
+    from hotspice_b200 import _lib
+    keep = [C.create_string_buffer(16) for _ in range(5)]
+    L = _lib.HsLattice()
+    L.m, L.occ, L.mm, L.E_B, L.nonzero = (C.addressof(b) for b in keep)
+    L.nx, L.ny, L.ux, L.uy, L.n_occ, L.beta_uniform = nx, ny, 1, 1, nx * ny, 1e20
+    return L, keep
+
+
+def test_metropolis_entry_points_validate_before_any_cuda_call():
+    """hs_metropolis_step_noalloc checks the lattice, the plan and the Poisson radius before it
+    sizes anything or touches the device: a NaN radius, an unknown sampling scheme and a
+    Poisson grid beyond HS_POISSON_GRID_MAX are refused here, without a GPU."""
+    import ctypes as C
+    from hotspice_b200 import _lib
+    lib = _lib.load()
+    L, keep = _host_only_lattice()
+    Cn, sw = _lib.HsCounters(), _lib.HsSwitchList()
+    P = _lib.HsGridPlan()
+    P.sample_scheme, P.r_cells, P.n_sc = _lib.HS_SAMPLE_POISSON, float('nan'), 1
+    assert lib.hs_metropolis_step_noalloc(C.byref(L), C.byref(Cn), C.byref(sw), C.byref(P), None) == _lib.HS_EINVAL
+    assert 'Poisson radius' in _lib.last_error()
+    assert lib.hs_metropolis_scratch_bytes(C.byref(L), C.byref(P)) == -1
+    P.sample_scheme = 7
+    assert lib.hs_metropolis_step_noalloc(C.byref(L), C.byref(Cn), C.byref(sw), C.byref(P), None) == _lib.HS_EINVAL
+    assert 'sample scheme' in _lib.last_error()
+    # 40000^2 cells at radius 0: a background grid of ~3.2e9 cells (more than an int holds)
+    Lb, keepb = _host_only_lattice(40000, 40000)
+    P.sample_scheme, P.r_cells = _lib.HS_SAMPLE_POISSON, 0.0
+    assert lib.hs_metropolis_step_noalloc(C.byref(Lb), C.byref(Cn), C.byref(sw), C.byref(P), None) == _lib.HS_ERANGE
+    assert 'background grid' in _lib.last_error()
+    assert lib.hs_metropolis_step(C.byref(Lb), C.byref(Cn), C.byref(sw), C.byref(P), None, 0, None) == _lib.HS_ERANGE
+
+
+def test_progress_with_no_finite_limit_is_refused():
+    """progress() with t_max and MCsteps_max both infinite would never end: the C ABI and the
+    host-side check refuse it."""
+    import ctypes as C
+    import math
+    from hotspice_b200 import _lib
+    from hotspice_b200.core import check_progress_limits
+    lib = _lib.load()
+    Cn = _lib.HsCounters()
+    assert lib.hs_progress_arm(C.byref(Cn), 4, math.inf, math.inf, None) == _lib.HS_EINVAL
+    assert 'both infinite' in _lib.last_error()
+    with pytest.raises(ValueError):
+        check_progress_limits(math.inf, math.inf)
+    check_progress_limits(math.inf, 4.0)
+    check_progress_limits(1e-3, math.inf)
