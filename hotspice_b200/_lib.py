@@ -104,6 +104,7 @@ SIGNATURES = {
     'hs_progress_arm': (C.c_int, [P, C.c_int32, C.c_double, C.c_double, P]),
     'hs_progress_disarm': (C.c_int, [P, P]),
     'hs_region_readout': (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, P, P, P, P, P, P]),
+    'hs_square_vertex_counts': (C.c_int, [P, C.c_int32, C.c_int32, P, P]),
     'hs_segments_copy': (C.c_int, [P, P, C.c_int32, C.c_int32, P]),
     'hs_engine_run': (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, P, P]),
     'hs_engine_max_clusters': (C.c_int, [C.c_int32]),

@@ -296,6 +296,14 @@ int hs_progress_arm(HsCounters *C, int32_t n_occ, double t_max, double MCsteps_m
     return hs_progress_arm_impl(C, n_occ, t_max, MCsteps_max, (cudaStream_t)stream);
 }
 
+int hs_square_vertex_counts(const int8_t *m, int32_t nx, int32_t ny, int64_t *out, void *stream) {
+    if (!m || !out || nx < 2 || ny < 2 || (int64_t)nx * ny >= (1LL << 31)) {
+        hs_set_error("hs_square_vertex_counts: bad arguments (need m, out and a lattice of at least 2 x 2 cells)");
+        return HS_EINVAL;
+    }
+    return hs_square_vertex_counts_impl(m, nx, ny, out, (cudaStream_t)stream);
+}
+
 int hs_progress_disarm(HsCounters *C, void *stream) {
     if (!C) { hs_set_error("hs_progress_disarm: null counters"); return HS_EINVAL; }
     return hs_progress_disarm_impl(C, (cudaStream_t)stream);

@@ -54,6 +54,8 @@ int hs_progress_disarm_impl(HsCounters *C, cudaStream_t st);
 int hs_region_readout_impl(const int8_t *m, int nx, int ny, int R, const int32_t *rects, const double *wx,
                            const double *wy, const double *norm, double *out, cudaStream_t st);
 
+int hs_square_vertex_counts_impl(const int8_t *m, int nx, int ny, int64_t *out, cudaStream_t st);
+
 int hs_segments_copy_impl(void *staged, const HsSegment *segs, int n, int to_device, cudaStream_t st);
 
 int hs_launch_engine(const HsInstance *insts, int n_inst, int cluster_size, int n_clusters, int *work,

@@ -92,7 +92,44 @@ __global__ void __launch_bounds__(IO_T) region_sum_kernel(const int8_t *m, int n
     }
 }
 
+// Vertex types of in-plane square ASI (examples/IP_SquareVertices.py:19-35): a vertex is a
+// cell with even x and y; with its four neighbours (periodic wrap) N_in = up + left - right -
+// down and N_flower = up - left + right - down, the vertex is type 3 / 4 when |N_in| = 2 / 4,
+// else type 1 when |N_flower| = 4 and type 2 otherwise. Integer counts, one atomic per warp.
+__global__ void __launch_bounds__(IO_T) square_vertex_kernel(const int8_t *m, int nx, int ny, unsigned long long *out) {
+    const int vx = (nx + 1) / 2, vy = (ny + 1) / 2;
+    const int64_t nv = (int64_t)vx * vy;
+    unsigned c[4] = {0u, 0u, 0u, 0u};
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv; v += (int64_t)gridDim.x * blockDim.x) {
+        const int y = 2 * (int)(v / vx), x = 2 * (int)(v % vx);
+        const int yu = y == 0 ? ny - 1 : y - 1, yd = y + 1 == ny ? 0 : y + 1;
+        const int xl = x == 0 ? nx - 1 : x - 1, xr = x + 1 == nx ? 0 : x + 1;
+        const int up = m[(int64_t)yu * nx + x], down = m[(int64_t)yd * nx + x];
+        const int left = m[(int64_t)y * nx + xl], right = m[(int64_t)y * nx + xr];
+        const int n_in = abs(up + left - right - down), flower = abs(up - left + right - down);
+        const int t = n_in == 4 ? 3 : (n_in == 2 ? 2 : (n_in == 0 ? (flower == 4 ? 0 : 1) : -1));
+#pragma unroll
+        for (int k = 0; k < 4; ++k) c[k] += (t == k);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        unsigned s = c[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if ((threadIdx.x & 31) == 0 && s) atomicAdd(out + k, (unsigned long long)s);
+    }
+}
+
 }  // namespace
+
+int hs_square_vertex_counts_impl(const int8_t *m, int nx, int ny, int64_t *out, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(out, 0, 4 * sizeof(int64_t), st);
+    if (e != cudaSuccess) { hs_set_error("hs_square_vertex_counts: %s", cudaGetErrorString(e)); return HS_ECUDA; }
+    const int64_t nv = (int64_t)((nx + 1) / 2) * ((ny + 1) / 2);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((nv + IO_T - 1) / IO_T, 148 * 8));
+    square_vertex_kernel<<<grid, IO_T, 0, st>>>(m, nx, ny, reinterpret_cast<unsigned long long *>(out));
+    return hs_check_launch("square_vertex_kernel");
+}
 
 int hs_zeeman_set_impl(int64_t n_cells, int in_plane, const double *moment, const double *orient, const float *pattern,
                        double magnitude, double angle, double *ef, double *efp, float *ef32, float *efp32, cudaStream_t st) {

@@ -23,6 +23,7 @@
  *   hs_minimize_step         one iteration of Magnets.minimize (hotspice/core.py:763-797)
  *   hs_zeeman_set / hs_progress_arm / hs_region_readout
  *                            the input / output steps of hotspice/io.py:193-500
+ *   hs_square_vertex_counts  count_square_vertices (examples/IP_SquareVertices.py:19-35)
  *   hs_exchange_energy       ExchangeEnergy.update (hotspice/energies.py:771-781)
  *   hs_philox_uniform        the variate stream that replaces numpy.random in the hot path
  */
@@ -289,6 +290,12 @@ int hs_progress_disarm(HsCounters *C, void *stream);
  * wy is not NULL, out[n_regions + r] = sum m * wy / norm[r]. */
 int hs_region_readout(const int8_t *m, int32_t nx, int32_t ny, int32_t n_regions, const int32_t *rects, const double *wx,
                       const double *wy, const double *norm, double *out, void *stream);
+
+/* Vertex-type counts of an in-plane square ASI state (count_square_vertices,
+ * examples/IP_SquareVertices.py:19-35): vertices are the cells with even x and y, each with its
+ * four neighbouring magnets (periodic wrap); out[0..3] (device int64, overwritten) = the numbers
+ * of type 1 (flower), 2, 3 and 4 vertices. */
+int hs_square_vertex_counts(const int8_t *m, int32_t nx, int32_t ny, int64_t *out, void *stream);
 
 /* ---- packed state transfer for batches (no reference counterpart: it replaces the per-array
  * host<->device copies of a batch's start states and results) ---------------------------------- */

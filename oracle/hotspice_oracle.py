@@ -1114,3 +1114,28 @@ def io_read(mm: OracleMagnets, kind, p):
         else:
             out[r] = np.sum(m[sel])
     return out / norm
+
+
+# ----------------------------------------------------------------------------------------
+# Vertex statistics of in-plane square ASI (examples/IP_SquareVertices.py:19-35)
+# ----------------------------------------------------------------------------------------
+def square_vertex_counts(m):
+    """Counts (N1, N2, N3, N4) of the vertex types of an IP_Square state ``m`` (ny, nx):
+    vertices are the cells with even x and y, their four magnets the neighbours left, right,
+    above and below with periodic wrap (the reference's convolve2d(..., boundary='wrap')).
+    N_in = m[y-1, x] + m[y, x-1] - m[y, x+1] - m[y+1, x] counts in-pointing magnets; |N_in| = 2
+    is type 3, |N_in| = 4 type 4; with N_in = 0 the vertex is type 1 if
+    |m[y-1, x] - m[y, x-1] + m[y, x+1] - m[y+1, x]| = 4 (the flower state), else type 2."""
+    m = np.asarray(m, dtype=np.int64)
+    up, down = np.roll(m, 1, axis=0), np.roll(m, -1, axis=0)        # m[y-1, x], m[y+1, x]
+    left, right = np.roll(m, 1, axis=1), np.roll(m, -1, axis=1)     # m[y, x-1], m[y, x+1]
+    n_in = (up + left - right - down)[::2, ::2]
+    flower = (up - left + right - down)[::2, ::2]
+    a_in, a_fl = np.abs(n_in), np.abs(flower)
+    return (int(np.sum((a_in == 0) & (a_fl == 4))), int(np.sum((a_in == 0) & (a_fl != 4))),
+            int(np.sum(a_in == 2)), int(np.sum(a_in == 4)))
+
+
+def square_vertex_fractions(m):
+    c = np.asarray(square_vertex_counts(m), dtype=float)
+    return tuple(c / c.sum())

@@ -1,7 +1,8 @@
 """Generate golden fixtures by running the reference Hotspice NumPy path.
 
 Usage (only where the reference source tree is present):
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <reference checkout>   (or HOTSPICE_REFERENCE=<dir>)
+    python tests/golden/make_golden.py --ref <dir> --vertices        (only square_vertices.npz)
 
 The reference package is imported unmodified: ``hotspice/__init__.py`` (which pulls in the
 GUI and plotting modules) is bypassed by registering a bare package module, and the three
@@ -337,12 +338,60 @@ def hexagon_kat(hs):
     return out, -1e-7 * mom * mom / a ** 3 * (29 + 20 * np.sqrt(3) / 9)
 
 
+def reference_vertex_counter(ref_root):
+    """The reference's count_square_vertices (examples/IP_SquareVertices.py:19-35), taken from
+    the example file as written and executed unmodified (the example module itself imports
+    plotting packages, so only this function's source is compiled)."""
+    import ast
+    from scipy import signal
+    path = os.path.join(ref_root, 'examples', 'IP_SquareVertices.py')
+    src = open(path).read()
+    fn = next(n for n in ast.parse(src).body if isinstance(n, ast.FunctionDef) and n.name == 'count_square_vertices')
+    fn.returns = None
+    for a in fn.args.args:
+        a.annotation = None
+    mod = ast.Module(body=[fn], type_ignores=[])
+    env = {'np': np, 'signal': signal}
+    exec(compile(mod, path, 'exec'), env)
+    return env['count_square_vertices']
+
+
+def square_vertices(hs, ref_root):
+    """Vertex fractions of IP_Square states (random, ground state, and lightly annealed ones)
+    by the reference's own counting function."""
+    count = reference_vertex_counter(ref_root)
+    out = {}
+    cases = [(12, True, 'random', 1), (20, True, 'random', 2), (16, True, 'afm', 3), (18, False, 'random', 4),
+             (24, True, 'biased', 5)]
+    for k, (n, pbc, pattern, seed) in enumerate(cases):
+        mm = hs.ASI.IP_Square(1e-6, n, PBC=pbc, moment=3e-17, T=300, energies=[hs.energies.ZeemanEnergy()])
+        g = np.random.Generator(np.random.PCG64(seed))
+        if pattern == 'random':
+            mm.m = mm.occupation * (g.integers(0, 2, size=mm.m.shape) * 2 - 1)
+        elif pattern == 'biased':
+            mm.m = mm.occupation * np.where(g.random(mm.m.shape) < 0.8, 1, -1)
+        else:
+            mm.initialize_m('afm')
+        out[f'm_{k}'] = np.asarray(mm.m, dtype=np.int8)
+        out[f'pbc_{k}'] = np.asarray(pbc)
+        out[f'fractions_{k}'] = np.asarray(count(mm), dtype=float)
+    out['n_cases'] = np.asarray(len(cases))
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--ref', default='/root/reference')
+    ap.add_argument('--ref', default=os.environ.get('HOTSPICE_REFERENCE'),
+                    help='reference checkout (or set HOTSPICE_REFERENCE)')
     ap.add_argument('--only', default=None, help='comma-separated scenario names; merged into specs.json')
+    ap.add_argument('--vertices', action='store_true', help='write only square_vertices.npz')
     args = ap.parse_args()
+    if not args.ref:
+        ap.error('the reference checkout is required: --ref <dir> or HOTSPICE_REFERENCE=<dir>')
     hs = load_reference(args.ref)
+    if args.vertices:
+        np.savez_compressed(os.path.join(HERE, 'square_vertices.npz'), **square_vertices(hs, args.ref))
+        return
     only = set(args.only.split(',')) if args.only else None
     meta = {}
     for name, spec in SPECS.items():
@@ -375,6 +424,7 @@ def main():
         route_rng(mm, PhiloxStream(5))
         sel = [np.asarray(mm.select(r=mm.calc_r(0.05))) for _ in range(3)]
         np.savez_compressed(os.path.join(HERE, 'poisson_reference.npz'), selections=np.stack(sel))
+        np.savez_compressed(os.path.join(HERE, 'square_vertices.npz'), **square_vertices(hs, args.ref))
         with open(os.path.join(HERE, 'specs.json'), 'w') as f:
             json.dump(meta, f, indent=1, default=float)
 

@@ -3,7 +3,10 @@ where they are size-independent (statistical tolerances stated per test):
 
 * non-interacting magnets in a field (examples/Noninteracting.py): <M>/M0 = tanh(mu B / kB T);
 * 2-D exchange Ising square lattice (examples/OOP_Exchange.py): below T_c the spontaneous
-  magnetisation is Onsager's (1 - sinh(2J / kB T)^-4)^(1/8); above T_c it vanishes.
+  magnetisation is Onsager's (1 - sinh(2J / kB T)^-4)^(1/8); above T_c it vanishes;
+* vertex types of in-plane square ASI (examples/IP_SquareVertices.py): the device counts equal
+  the reference's, weakly coupled lattices approach the random fractions 1/8, 1/4, 1/2, 1/8
+  (:162), and coupled lattices give the oracle's fractions within error bars.
 """
 import math
 
@@ -63,3 +66,70 @@ def test_onsager_magnetisation(scheme):
             assert abs(m - theory) < 0.03, (scheme, t, m, theory)
         else:
             assert m < 0.2, (scheme, t, m)
+
+
+def test_square_vertex_counts_equal_reference():
+    """hs_square_vertex_counts on the reference's fixture states (examples/IP_SquareVertices.py:
+    19-35, run unmodified) and on odd-sized states against the oracle: integer counts, exact."""
+    import torch
+    import hotspice_b200 as hs
+    from cases import load_fixture
+    from oracle.hotspice_oracle import square_vertex_counts
+    z = load_fixture('square_vertices')
+    for k in range(int(z['n_cases'])):
+        m = z[f'm_{k}']
+        mm = hs.ASI.IP_Square(1e-6, m.shape[1], PBC=bool(z[f'pbc_{k}']), moment=3e-17, T=300,
+                              energies=[hs.ZeemanEnergy()], pattern='uniform', seed=k)
+        mm.m = m
+        assert hs.ASI.count_square_vertices(mm) == tuple(z[f'fractions_{k}']), k
+    for nx, ny, seed in ((15, 13, 1), (33, 64, 2), (201, 199, 3)):
+        g = np.random.Generator(np.random.PCG64(seed))
+        mm = hs.ASI.IP_Square(1e-6, nx=nx, ny=ny, moment=3e-17, T=300, energies=[hs.ZeemanEnergy()], seed=seed)
+        m = (g.integers(0, 2, size=(ny, nx)) * 2 - 1) * mm.occupation.astype(int)
+        mm.m = m
+        torch.cuda.synchronize()
+        assert hs.ASI.count_square_vertices(mm, counts=True) == square_vertex_counts(m), (nx, ny)
+
+
+def test_square_vertices_weak_coupling_limit():
+    """IP_Square at 3 um spacing (moment 3e-17: nearest-neighbour coupling ~0.01 kB T), Metropolis
+    from a random state: the vertex fractions are those of independent magnets, 1/8, 1/4, 1/2,
+    1/8 (examples/IP_SquareVertices.py:162). 256 x 256 cells = 16384 vertices, so the binomial
+    standard error is <= 0.004: tolerance 0.02 per type."""
+    import hotspice_b200 as hs
+    mm = hs.ASI.IP_Square(3e-6, 256, PBC=True, moment=3e-17, T=300, E_B=1.6e-18, m_perp_factor=0,
+                          energies=[hs.DipolarEnergy(), hs.ZeemanEnergy()], pattern='random', seed=21,
+                          params=hs.SimParams(UPDATE_SCHEME='Metropolis'))
+    mm.progress(t_max=math.inf, MCsteps_max=20)
+    f = hs.ASI.count_square_vertices(mm)
+    for got, want in zip(f, (1 / 8, 1 / 4, 1 / 2, 1 / 8)):
+        assert abs(got - want) < 0.02, (f, want)
+
+
+def test_square_vertices_coupled_match_oracle_statistics():
+    """IP_Square 48 x 48 at 500 nm spacing (strongly coupled: mostly type 1), Metropolis for 20
+    MC steps from random states: the mean vertex fractions over 8 device runs and over 8 oracle
+    runs with other seeds agree within 4 combined standard errors (+ 0.01)."""
+    import hotspice_b200 as hs
+    from oracle import geometry as G
+    from oracle.hotspice_oracle import OracleDipolar, OracleMagnets, square_vertex_fractions
+    a, n, runs = 500e-9, 48, 8
+    dev, ora = [], []
+    for k in range(runs):
+        mm = hs.ASI.IP_Square(a, n, PBC=True, moment=3e-17, T=300, E_B=1.6e-18, m_perp_factor=0,
+                              energies=[hs.DipolarEnergy()], pattern='random', seed=200 + k,
+                              params=hs.SimParams(UPDATE_SCHEME='Metropolis'))
+        mm.progress(t_max=math.inf, MCsteps_max=20, r=2 * a)
+        dev.append(hs.ASI.count_square_vertices(mm))
+        g = np.random.Generator(np.random.PCG64(300 + k))
+        mo = OracleMagnets(G.ip_square(a, n, n), g.integers(0, 2, size=(n, n)) * 2 - 1, T=300.0, E_B=1.6e-18,
+                           moment=3e-17, PBC=True, m_perp_factor=0, energies=[OracleDipolar()],
+                           params=dict(UPDATE_SCHEME='Metropolis'), seed=300 + k)
+        mo.progress(t_max=math.inf, MCsteps_max=20, r=2 * a)
+        ora.append(square_vertex_fractions(mo.m))
+    dev, ora = np.asarray(dev), np.asarray(ora)
+    se = np.sqrt(dev.var(axis=0, ddof=1) / runs + ora.var(axis=0, ddof=1) / runs)
+    diff = np.abs(dev.mean(axis=0) - ora.mean(axis=0))
+    print('device', dev.mean(axis=0), 'oracle', ora.mean(axis=0), 'se', se)
+    assert dev.mean(axis=0)[0] > 0.5            # ordered: mostly flower (type 1) vertices
+    assert np.all(diff <= 4 * se + 0.01), (dev.mean(axis=0), ora.mean(axis=0), se)

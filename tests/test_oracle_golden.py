@@ -137,3 +137,12 @@ def test_poisson_disc_cells_keeps_its_distance(w, h, r):
         d = np.minimum(d, np.array([w, h]) - d)
         d2 = (d ** 2).sum(-1) + np.eye(len(pts)) * 1e9
         assert d2.min() > (r + 1) ** 2
+
+
+def test_square_vertex_fractions_match_reference():
+    """The oracle's vertex counting equals the reference's count_square_vertices
+    (examples/IP_SquareVertices.py:19-35, run unmodified by make_golden.py)."""
+    from oracle.hotspice_oracle import square_vertex_fractions
+    z = load_fixture('square_vertices')
+    for k in range(int(z['n_cases'])):
+        assert np.allclose(square_vertex_fractions(z[f'm_{k}']), z[f'fractions_{k}'], rtol=0, atol=1e-15), k
