@@ -81,6 +81,7 @@ SIGNATURES = {
     'hs_dipolar_full_direct': (C.c_int, [C.POINTER(HsLattice), C.c_int32, P, P, P]),
     'hs_igemm_scratch_bytes': (C.c_int64, [C.POINTER(HsLattice), C.c_int32]),
     'hs_dipolar_full_igemm': (C.c_int, [C.POINTER(HsLattice), C.c_int32, P, C.c_int64, P]),
+    'hs_set_wait_limit': (C.c_int, [C.c_uint64]),
     'hs_neel_scratch_bytes': (C.c_int64, [C.POINTER(HsLattice)]),
     'hs_neel_step': (C.c_int, [C.POINTER(HsLattice), P, C.POINTER(HsSwitchList), C.c_double, P, C.c_int64, P]),
     'hs_metropolis_scratch_bytes': (C.c_int64, [C.POINTER(HsLattice), C.POINTER(HsGridPlan)]),

@@ -175,6 +175,8 @@ int hs_dipolar_full_igemm(const HsLattice *L, int32_t nsplit, void *scratch, int
     return hs_launch_igemm(*L, nsplit, scratch, scratch_bytes, (cudaStream_t)stream);
 }
 
+int hs_set_wait_limit(uint64_t ns) { return hs_set_wait_limit_impl(ns); }
+
 int64_t hs_neel_scratch_bytes(const HsLattice *L) {
     if (check_lattice(L, "hs_neel_scratch_bytes")) return -1;
     return hs_neel_scratch(*L);

@@ -237,6 +237,182 @@ dip_update_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev, int n_h
     }
 }
 
+// Persistent form of dip_update_kernel for lists of at most UPD_LOC switches: a CTA stages the
+// whole list in shared memory once and then walks tiles (tile = blockIdx.x, + gridDim.x, ...).
+// Inside a tile every warp works alone on its UPD_RPW rows, with no block barrier: it tests the
+// staged switches against its rows 32 at a time (ballot, in list order), prefetches its rows of
+// E, E_perp and m*moment into L2 as soon as one switch reaches them, adds the contributions of
+// the hits in list order, and writes E back. Per cell the arithmetic and the summation order are
+// those of dip_update_kernel, so both give the same bits.
+template <int VEC>
+__global__ void __launch_bounds__(32 * UPD_WARPS, HS_UPD_MIN_CTAS)
+dip_update_persist_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev, int n_host, int semantics,
+                          const HsCounters *C, int tiles) {
+    if (C && C->done) return;
+    const int nsw = n_sw_dev ? *n_sw_dev : n_host;
+    if (nsw <= 0 || nsw > UPD_LOC) return;   // the launcher sends longer lists to dip_update_kernel
+    constexpr int TX = 32 * VEC;
+    __shared__ SwInfo s_sw[UPD_LOC];
+    for (int k = threadIdx.x; k < nsw; k += blockDim.x) {
+        SwInfo w{sw.y[k], sw.x[k], sw.mode ? sw.mode[k] : 0, -1, 0.f};
+        w.sub = hs_sub(L, w.y, w.x);
+        if (w.sub >= 0) w.mm = L.mm[(int64_t)w.y * L.nx + w.x];
+        s_sw[k] = w;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tiles_x = (L.nx + TX - 1) / TX;
+    const float pref2 = (float)(2.0 * L.dip_pref);
+    const bool flip_perp = !(L.dip_keep_perp_sign && nsw > 1);
+    const int KW = 2 * L.dip_wx + 1, KH = 2 * L.dip_wy + 1;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int y0 = (tile / tiles_x) * UPD_TY + warp * UPD_RPW;   // this warp's first row
+        const int tx0 = (tile % tiles_x) * TX;
+        const int x0 = tx0 + lane * VEC;
+        if (y0 >= L.ny) continue;
+        const int nrows = min(UPD_RPW, L.ny - y0);
+        // does switch w reach this warp's rows (or, without a kernel, sit in them)?
+        auto hits = [&](const SwInfo &w) {
+            if (w.sub < 0)
+                return semantics == HS_UPDATE_MULTIPLE && w.y >= y0 && w.y < y0 + nrows && w.x >= tx0 && w.x < tx0 + TX;
+            int hy, wy_, hx, wx_;
+            hs_window(L, w.mode, true, hy, wy_);
+            hs_window(L, w.mode, false, hx, wx_);
+            return hs_axis_overlap(w.y, hy, wy_, L.ny, y0, nrows) && hs_axis_overlap(w.x, hx, wx_, L.nx, tx0, TX);
+        };
+        // pass 1: is the warp's strip touched at all? then prefetch its energies and sources
+        bool any = false;
+        for (int c = 0; c < nsw && !any; c += 32) {
+            const int k = c + lane;
+            any = __any_sync(0xffffffffu, k < nsw && hits(s_sw[k]));
+        }
+        if (!any) continue;   // warp-uniform
+        for (int r = 0; r < nrows; ++r) {
+            const int64_t i = (int64_t)(y0 + r) * L.nx + x0;
+            if (x0 < L.nx) {
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(L.E_dip + i));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(L.mm + i));
+                if (L.use_perp) asm volatile("prefetch.global.L2 [%0];" ::"l"(L.E_dip_perp + i));
+            }
+        }
+        // pass 2: contributions of the hits, in list order
+        float acc[UPD_RPW][VEC], accp[UPD_RPW][VEC];
+#pragma unroll
+        for (int r = 0; r < UPD_RPW; ++r)
+#pragma unroll
+            for (int v = 0; v < VEC; ++v) { acc[r][v] = 0.f; accp[r][v] = 0.f; }
+        unsigned touched = 0u, negate = 0u;   // bit r * VEC + v
+        for (int c = 0; c < nsw; c += 32) {
+            const int k = c + lane;
+            unsigned bal = __ballot_sync(0xffffffffu, k < nsw && hits(s_sw[k]));
+            while (bal) {
+                const int q = c + __ffs(bal) - 1;
+                bal &= bal - 1u;
+                const SwInfo w = s_sw[q];
+                if (w.sub >= 0 && !w.mode && !L.dip_wrap) {
+                    const int64_t kb = (int64_t)w.sub * KH * KW + (L.dip_wx - w.x);
+#pragma unroll
+                    for (int r = 0; r < UPD_RPW; ++r) {
+                        if (r >= nrows) continue;
+                        const int y = y0 + r;
+                        const int dy = y - w.y;
+                        const bool rowin = dy >= -L.dip_wy && dy <= L.dip_wy;
+                        const float *Kr = L.K + kb + (int64_t)(dy + L.dip_wy) * KW;
+                        const float *Kpr = L.use_perp ? L.Kpo + kb + (int64_t)(dy + L.dip_wy) * KW : nullptr;
+#pragma unroll
+                        for (int v = 0; v < VEC; ++v) {
+                            const int x = x0 + v;
+                            if (x >= L.nx) continue;
+                            touched |= 1u << (r * VEC + v);
+                            const int dx = x - w.x;
+                            if (rowin && dx >= -L.dip_wx && dx <= L.dip_wx) {
+                                acc[r][v] += w.mm * __ldg(Kr + x);
+                                if (L.use_perp) accp[r][v] += w.mm * __ldg(Kpr + x);
+                                if (dy == 0 && dx == 0) negate |= 1u << (r * VEC + v);
+                            }
+                        }
+                    }
+                    continue;
+                }
+#pragma unroll
+                for (int r = 0; r < UPD_RPW; ++r) {
+                    if (r >= nrows) continue;
+                    const int y = y0 + r;
+#pragma unroll
+                    for (int v = 0; v < VEC; ++v) {
+                        const int x = x0 + v;
+                        if (x >= L.nx) continue;
+                        if (w.sub >= 0) {
+                            float a = acc[r][v], ap = accp[r][v];
+                            hs_contrib(L, w, y, x, a, ap);
+                            acc[r][v] = a; accp[r][v] = ap;
+                        }
+                        touched |= 1u << (r * VEC + v);
+                        if (w.y == y && w.x == x) negate |= 1u << (r * VEC + v);
+                    }
+                }
+            }
+        }
+        const bool vec_rows = VEC == 4 && x0 + 3 < L.nx && (L.nx & 3) == 0;
+#pragma unroll
+        for (int r = 0; r < UPD_RPW; ++r) {
+            if (r >= nrows) continue;
+            const int64_t row = (int64_t)(y0 + r) * L.nx;
+            if (vec_rows) {
+                if (!((touched >> (r * VEC)) & 0xFu)) continue;
+                const float4 mm4 = *reinterpret_cast<const float4 *>(L.mm + row + x0);
+                const float mmv[4] = {mm4.x, mm4.y, mm4.z, mm4.w};
+                const double2 e01 = *reinterpret_cast<const double2 *>(L.E_dip + row + x0);
+                const double2 e23 = *reinterpret_cast<const double2 *>(L.E_dip + row + x0 + 2);
+                double ev[4] = {e01.x, e01.y, e23.x, e23.y};
+                double pv[4] = {0.0, 0.0, 0.0, 0.0};
+                if (L.use_perp) {
+                    const double2 p01 = *reinterpret_cast<const double2 *>(L.E_dip_perp + row + x0);
+                    const double2 p23 = *reinterpret_cast<const double2 *>(L.E_dip_perp + row + x0 + 2);
+                    pv[0] = p01.x; pv[1] = p01.y; pv[2] = p23.x; pv[3] = p23.y;
+                }
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const bool ng = (negate >> (r * VEC + v)) & 1u;
+                    if (semantics == HS_UPDATE_MULTIPLE) {
+                        if (ng) { ev[v] = -ev[v]; if (flip_perp) pv[v] = -pv[v]; }
+                        ev[v] += (double)(pref2 * (mmv[v] * acc[r][v]));
+                        pv[v] += (double)(pref2 * (mmv[v] * accp[r][v]));
+                    } else {
+                        ev[v] += (double)(pref2 * (mmv[v] * acc[r][v]));
+                        pv[v] += (double)(pref2 * (mmv[v] * accp[r][v]));
+                        if (ng) { ev[v] = -ev[v]; pv[v] = -pv[v]; }
+                    }
+                }
+                *reinterpret_cast<double2 *>(L.E_dip + row + x0) = make_double2(ev[0], ev[1]);
+                *reinterpret_cast<double2 *>(L.E_dip + row + x0 + 2) = make_double2(ev[2], ev[3]);
+                if (L.use_perp) {
+                    *reinterpret_cast<double2 *>(L.E_dip_perp + row + x0) = make_double2(pv[0], pv[1]);
+                    *reinterpret_cast<double2 *>(L.E_dip_perp + row + x0 + 2) = make_double2(pv[2], pv[3]);
+                }
+                continue;
+            }
+#pragma unroll
+            for (int v = 0; v < VEC; ++v) {
+                const int x = x0 + v;
+                if (x >= L.nx || !((touched >> (r * VEC + v)) & 1u)) continue;
+                const bool ng = (negate >> (r * VEC + v)) & 1u;
+                const float mmv = L.mm[row + x];
+                double e = L.E_dip[row + x];
+                if (semantics == HS_UPDATE_MULTIPLE) { if (ng) e = -e; e += (double)(pref2 * (mmv * acc[r][v])); }
+                else { e += (double)(pref2 * (mmv * acc[r][v])); if (ng) e = -e; }
+                L.E_dip[row + x] = e;
+                if (L.use_perp) {
+                    double p = L.E_dip_perp[row + x];
+                    if (semantics == HS_UPDATE_MULTIPLE) { if (ng && flip_perp) p = -p; p += (double)(pref2 * (mmv * accp[r][v])); }
+                    else { p += (double)(pref2 * (mmv * accp[r][v])); if (ng) p = -p; }
+                    L.E_dip_perp[row + x] = p;
+                }
+            }
+        }
+    }
+}
+
 // Direct-sum full recompute, one thread per target cell (hotspice/energies.py:290-308):
 //   E_i = pref * mu_i * m_i * sum_j K_{s(i)}(j - i) * mm_j,  E_perp with the perp-self kernel.
 template <typename Acc, bool FULLWIN>
@@ -288,11 +464,37 @@ __global__ void dip_full_direct_kernel(HsLattice L, int fp64, double *E64, doubl
 
 }  // namespace
 
+namespace {
+// resident CTAs of the persistent update kernel on this device (queried once per variant)
+template <int VEC>
+int persist_grid(int tiles) {
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0, sms = 148, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dip_update_persist_kernel<VEC>, 32 * UPD_WARPS, 0);
+        n = sms * std::max(per, 1);
+    }
+    return std::max(1, std::min(tiles, n));
+}
+}  // namespace
+
 int hs_launch_dipolar_update(const HsLattice &L, const HsSwitchList &sw, const int32_t *n_sw_dev, int n_host,
                              int semantics, const HsCounters *C, cudaStream_t st) {
     const bool vec = (L.nx % 4) == 0;
     const int TX = vec ? 128 : 32;
     const int tiles = ((L.nx + TX - 1) / TX) * ((L.ny + UPD_TY - 1) / UPD_TY);
+    // a list that fits the shared-memory staging goes to the persistent kernel (a device-side
+    // count is bounded by the list's capacity)
+    const int most = n_sw_dev ? sw.cap : n_host;
+    if (most <= UPD_LOC) {
+        if (vec) dip_update_persist_kernel<4><<<persist_grid<4>(tiles), 32 * UPD_WARPS, 0, st>>>(L, sw, n_sw_dev, n_host,
+                                                                                               semantics, C, tiles);
+        else dip_update_persist_kernel<1><<<persist_grid<1>(tiles), 32 * UPD_WARPS, 0, st>>>(L, sw, n_sw_dev, n_host,
+                                                                                           semantics, C, tiles);
+        return hs_check_launch("dip_update_persist_kernel");
+    }
     if (vec) dip_update_kernel<4><<<tiles, 32 * UPD_WARPS, 0, st>>>(L, sw, n_sw_dev, n_host, semantics, C);
     else dip_update_kernel<1><<<tiles, 32 * UPD_WARPS, 0, st>>>(L, sw, n_sw_dev, n_host, semantics, C);
     return hs_check_launch("dip_update_kernel");

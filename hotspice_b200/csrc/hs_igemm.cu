@@ -27,8 +27,10 @@
 // (deterministic).
 //
 // Warp roles (256 threads): warp 0 producer (bulk copies), warp 1 MMA issuer and TMEM owner,
-// warps 4-7 epilogue (TMEM lanes 0-127). Every mbarrier wait is bounded in time; on a timeout
-// the kernel records ST_TIMEOUT in its status word, lets its copies land and frees TMEM.
+// warps 4-7 epilogue (TMEM lanes 0-127). Every mbarrier wait is bounded in time (a pipeline
+// wait by hs_set_wait_limit, 4 s by default); on a timeout the kernel records ST_TIMEOUT in its
+// status word, lets its copies land and its MMAs finish (those waits keep the 4 s bound) and
+// frees TMEM.
 #include <cuda_bf16.h>
 
 #include "hs_common.cuh"
@@ -65,6 +67,7 @@ struct IgemmParams {
     int XT, KS, G;                 // column tiles, K-splits per tile, stages per accumulator chunk
     double *acc;                   // [KS][ny][P] FP64 partial sums (one slot per K-split)
     int *status;
+    unsigned long long wait_ns;    // limit of a pipeline wait (the drain after an abort keeps WAIT_NS)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -86,7 +89,8 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 
 // Parity wait bounded in wall time; returns false when it gave up or another thread aborted.
 // `backoff` makes an idle waiter sleep between polls so that it does not steal issue slots.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag, bool backoff = false) {
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
+                                          unsigned long long limit_ns = WAIT_NS, bool backoff = false) {
     const uint32_t a = smem_u32(bar);
     const unsigned long long t0 = globaltimer_ns();
     for (unsigned it = 0;; ++it) {
@@ -97,7 +101,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volati
         if (backoff) __nanosleep(500);
         if ((it & 255) == 255) {
             if (*abort_flag) return false;
-            if (globaltimer_ns() - t0 > WAIT_NS) { *abort_flag = 1; return false; }
+            if (globaltimer_ns() - t0 > limit_ns) { *abort_flag = 1; return false; }
         }
     }
 }
@@ -279,14 +283,14 @@ __global__ void __launch_bounds__(NT, 1) igemm_kernel(IgemmParams p) {
                 prev_band = S.band;
                 ++nb;
                 const int slot = nb & 1;
-                if (nb >= 2 && !mbar_wait(&bempty[slot], ((nb >> 1) - 1) & 1, abort_flag)) { --nb; break; }
+                if (nb >= 2 && !mbar_wait(&bempty[slot], ((nb >> 1) - 1) & 1, abort_flag, p.wait_ns)) { --nb; break; }
                 mbar_expect_tx(&bfull[slot], BAND_BYTES);
                 const __nv_bfloat16 *src = p.spins + ((size_t)(S.cc * 8) * p.rows + (S.row0 + PAD_LO)) * 8;
                 for (int j = 0; j < 8; ++j)
                     bulk_copy(bands + slot * BAND_BYTES + j * KGROUP_BYTES, src + (size_t)j * p.rows * 8, KGROUP_BYTES, &bfull[slot]);
             }
             const int u = t - t_begin, st = u % STAGES;
-            if (u >= STAGES && !mbar_wait(&empty[st], ((u / STAGES) - 1) & 1, abort_flag)) break;
+            if (u >= STAGES && !mbar_wait(&empty[st], ((u / STAGES) - 1) & 1, abort_flag, p.wait_ns)) break;
             unsigned char *sa = astage + st * STAGE_BYTES;
             mbar_expect_tx(&full[st], p.nsplit * A_BYTES);
             const int q0 = 8 * S.cc - w.x0 / 8 - p.qmin;
@@ -309,7 +313,7 @@ __global__ void __launch_bounds__(NT, 1) igemm_kernel(IgemmParams p) {
         StageIter it(t_begin, w, p.C);
         for (int lc = 0; lc < w.n_chunks && ok; ++lc) {
             const int b = lc & 1;
-            if (lc >= 2 && !mbar_wait(&acce[b], ((lc >> 1) - 1) & 1, abort_flag)) break;
+            if (lc >= 2 && !mbar_wait(&acce[b], ((lc >> 1) - 1) & 1, abort_flag, p.wait_ns)) break;
             asm volatile("tcgen05.fence::after_thread_sync;");
             const uint32_t d = tmem + (uint32_t)(b * BN);
             const int tb = t_begin + lc * p.G, te = min(t_end, tb + p.G);
@@ -319,11 +323,11 @@ __global__ void __launch_bounds__(NT, 1) igemm_kernel(IgemmParams p) {
                     if (nb >= 0) mma_commit(&bempty[nb & 1]);  // the previous band is free once its MMAs finish
                     prev_band = S.band;
                     ++nb;
-                    if (!mbar_wait(&bfull[nb & 1], (nb >> 1) & 1, abort_flag)) { ok = false; break; }
+                    if (!mbar_wait(&bfull[nb & 1], (nb >> 1) & 1, abort_flag, p.wait_ns)) { ok = false; break; }
                     asm volatile("tcgen05.fence::after_thread_sync;");
                 }
                 const int u = t - t_begin, st = u % STAGES;
-                if (!mbar_wait(&full[st], (u / STAGES) & 1, abort_flag)) { ok = false; break; }
+                if (!mbar_wait(&full[st], (u / STAGES) & 1, abort_flag, p.wait_ns)) { ok = false; break; }
                 asm volatile("tcgen05.fence::after_thread_sync;");
                 const uint32_t sa = smem_u32(astage + st * STAGE_BYTES);
                 const uint32_t sb = smem_u32(bands + (nb & 1) * BAND_BYTES) + (uint32_t)(S.off * 16);
@@ -351,7 +355,7 @@ __global__ void __launch_bounds__(NT, 1) igemm_kernel(IgemmParams p) {
         }
         for (int lc = 0; lc < w.n_chunks; ++lc) {
             const int b = lc & 1;
-            if (!mbar_wait(&accf[b], (lc >> 1) & 1, abort_flag, true)) break;
+            if (!mbar_wait(&accf[b], (lc >> 1) & 1, abort_flag, p.wait_ns, true)) break;
             asm volatile("tcgen05.fence::after_thread_sync;");
             for (int n0 = 0; n0 < BN; n0 += 32) {
                 uint32_t v[32];
@@ -541,6 +545,14 @@ int64_t hs_igemm_scratch(const HsLattice &L, int nsplit) {
     return layout_of(L, nsplit).total;
 }
 
+// Limit of one pipeline wait of the implicit GEMM (hs_set_wait_limit; WAIT_NS by default).
+static unsigned long long g_wait_ns = WAIT_NS;
+
+int hs_set_wait_limit_impl(unsigned long long ns) {
+    g_wait_ns = ns ? ns : WAIT_NS;
+    return HS_OK;
+}
+
 int hs_launch_igemm(const HsLattice &L, int nsplit, void *scratch, int64_t scratch_bytes, cudaStream_t st) {
     if (nsplit < 1 || nsplit > MAX_SPLIT) { hs_set_error("hs_dipolar_full_igemm: nsplit must be 1..3"); return HS_EINVAL; }
     if (!(L.dip_wy == L.ny - 1 && L.dip_wx == L.nx - 1 && !L.dip_wrap)) {
@@ -586,7 +598,8 @@ int hs_launch_igemm(const HsLattice &L, int nsplit, void *scratch, int64_t scrat
         }
         cudaMemsetAsync(out, 0, sizeof(double) * (size_t)L.nx * L.ny, st);
         for (int s = 0; s < L.n_sub; ++s) {
-            IgemmParams p{strips, spins, lo.qspan, lo.qmin, nsplit, s, lo.P, lo.C, L.nx, L.ny, lo.rows, lo.XT, lo.KS, lo.G, acc, status};
+            IgemmParams p{strips, spins, lo.qspan, lo.qmin, nsplit, s, lo.P, lo.C, L.nx, L.ny, lo.rows, lo.XT, lo.KS, lo.G, acc, status,
+                          g_wait_ns};
             igemm_kernel<<<grid, NT, SMEM_BYTES, st>>>(p);
             if ((rc = hs_check_launch("igemm_kernel"))) return rc;
             igemm_finalize_kernel<<<148 * 4, 256, 0, st>>>(acc, lo.KS, lo.P, L.nx, L.ny, L.ux, L.uy, L.sub_of, s, L.m, L.moment,

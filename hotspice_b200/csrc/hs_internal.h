@@ -35,6 +35,7 @@ int hs_launch_switch_energy(const HsLattice &L, float *dE, cudaStream_t st);
 int hs_launch_philox(uint64_t seed, uint64_t call, int32_t n, double *out, cudaStream_t st);
 int64_t hs_igemm_scratch(const HsLattice &L, int nsplit);
 int hs_launch_igemm(const HsLattice &L, int nsplit, void *scratch, int64_t scratch_bytes, cudaStream_t st);
+int hs_set_wait_limit_impl(unsigned long long ns);
 
 int64_t hs_relax_scratch(const HsLattice &L);
 int hs_relax_begin_impl(const HsLattice &L, void *scratch, int64_t bytes, cudaStream_t st);

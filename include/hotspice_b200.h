@@ -210,6 +210,12 @@ int hs_dipolar_full_direct(const HsLattice *L, int32_t fp64, double *E64, double
 int64_t hs_igemm_scratch_bytes(const HsLattice *L, int32_t nsplit);
 int hs_dipolar_full_igemm(const HsLattice *L, int32_t nsplit, void *scratch, int64_t scratch_bytes, void *stream);
 
+/* Limit, in ns of wall time, of one pipeline wait inside hs_dipolar_full_igemm (0: the default,
+ * 4 s). A wait that runs out sets bit 0 of the call's status word and the kernel ends cleanly (its
+ * copies land, its MMAs finish, TMEM is freed). No reference counterpart: a safety bound of this
+ * library, shortened only to test that path. Applies to later calls of this process. */
+int hs_set_wait_limit(uint64_t ns);
+
 /* ---- (c) Néel-Arrhenius step ------------------------------------------------------------- */
 int64_t hs_neel_scratch_bytes(const HsLattice *L);
 int hs_neel_step(const HsLattice *L, HsCounters *C, const HsSwitchList *sw, double attempt_freq,

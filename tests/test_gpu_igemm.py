@@ -111,3 +111,24 @@ def test_igemm_rejects_nonuniform_moment():
     mm.moment = mom
     with pytest.raises(ValueError):
         mm._dipolar().update(method='igemm')
+
+
+def test_igemm_wait_limit_runs_out_cleanly():
+    """A pipeline wait that runs out ends the recompute cleanly: with the limit shortened to 1 us
+    (hs_set_wait_limit) the epilogue's first wait for an accumulator chunk gives up, the call's
+    status word carries bit 0 (the host raises), the kernel's copies land, its MMAs finish and
+    TMEM is freed; with the default limit restored the next recompute on the same context is
+    correct."""
+    from hotspice_b200 import _lib
+    lib = _lib.load()
+    mm = _make('oop', 300, 270)
+    d = mm._dipolar()
+    try:
+        assert lib.hs_set_wait_limit(1000) == _lib.HS_OK
+        with pytest.raises(RuntimeError, match='status 1'):
+            d.update(method='igemm')
+    finally:
+        lib.hs_set_wait_limit(0)
+    torch.cuda.synchronize()
+    err, _ = _compare(mm, 3)
+    assert err <= TOL[3]
