@@ -459,6 +459,9 @@ def run_product(args):
     relax = None
     if rank == 0 and args.relax_n > 0:
         relax = run_relax(dev, n=args.relax_n, cpu_seconds=0.0 if args.no_cpu_baseline else 10.0)
+    c3 = None
+    if rank == 0 and args.c3_steps > 0:
+        c3 = run_c3(dev, n=args.c3_n, steps=args.c3_steps)
     reservoir = None
     if rank == 0 and args.reservoir_n > 0:
         reservoir = run_reservoir(dev, n=args.reservoir_n, cpu_seconds=0.0 if args.no_cpu_baseline else 10.0)
@@ -516,6 +519,8 @@ def run_product(args):
         line["relax"] = relax
     if reservoir is not None:
         line["reservoir"] = reservoir
+    if c3 is not None:
+        line["c3_poisson_resync"] = c3
     if not args.no_cpu_baseline:
         v, secs, st, ni = oracle_sample(specs, seconds_per_instance=args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
@@ -711,6 +716,63 @@ def run_incremental(dev, n=2048, reps=20):
                       "l2": "flushed (256 MB write) before every timed launch"}
     del mm, d, flush
     torch.cuda.empty_cache()
+    return out
+
+
+C3_WORKLOAD = ("OOP_Square {n}x{n} ({cells} magnets), a=200nm, moment=1.1e-15, E_B=5e-20 J, full uncut dipolar "
+               "kernel, random +-1 start, Metropolis with Poisson-disc multisampling (r = calc_r(0.05), cell units), "
+               "T = {temps} K, {steps} steps each, full recompute every {resync} steps as the tensor-core implicit GEMM "
+               "(3 BF16 splits, FP32 accumulation, FP64 near field and finalize)")
+
+
+def run_c3(dev, n=2048, steps=5000, resync=100, temps=(250.0, 300.0, 350.0)):
+    """The c3 workload: per temperature, `steps` Metropolis steps with Poisson-disc selection on
+    the full-kernel OOP square lattice, the energies recomputed by the tensor-core GEMM after
+    every `resync` steps. Reported per temperature: step time (Poisson sampling, acceptance and
+    the windowed update), recompute time, and the drift each resync removed (max |E_incremental
+    - E_recomputed| / max |E|)."""
+    import torch
+    import hotspice_b200 as hs
+    out = {"workload": C3_WORKLOAD.format(n=n, cells=n * n, temps='/'.join(f'{t:g}' for t in temps), steps=steps,
+                                          resync=resync), "temperatures": {}}
+    for T in temps:
+        mm = hs.ASI.OOP_Square(200e-9, n, T=T, E_B=5e-20, moment=1.1e-15, pattern='random', seed=SEED + int(T),
+                               energies=[hs.DipolarEnergy()], engine=hs.EngineConfig(recompute='igemm'),
+                               params=hs.SimParams(UPDATE_SCHEME='Metropolis', MULTISAMPLING_SCHEME='Poisson'),
+                               device=dev)
+        mm.run(10)            # warm-up: graphs, scratch
+        mm.resync_energies()
+        mm.check_resync()
+        torch.cuda.synchronize(dev)
+        a0 = mm.attempted_switches
+        run_ms, rec_ms, drifts = 0.0, 0.0, []
+        done = 0
+        while done < steps:
+            k = min(resync, steps - done)
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record()
+            mm.run(k)
+            e1.record()
+            drift = mm.resync_energies(measure=True) if k == resync else None
+            e2.record()
+            torch.cuda.synchronize(dev)
+            run_ms += e0.elapsed_time(e1)
+            if drift is not None:
+                rec_ms += e1.elapsed_time(e2)
+                drifts.append(drift)
+            done += k
+        mm.check_resync()
+        att = mm.attempted_switches - a0
+        out["temperatures"][f"{T:g}"] = {
+            "steps": steps, "attempts": att, "switches": mm.switches, "step_us": run_ms * 1e3 / steps,
+            "attempts_per_s": att / (run_ms * 1e-3), "recomputes": len(drifts),
+            "recompute_ms_mean": rec_ms / max(len(drifts), 1),
+            "attempts_per_s_with_recomputes": att / ((run_ms + rec_ms) * 1e-3),
+            "drift_before_resync_max": max(drifts) if drifts else None,
+            "drift_before_resync_median": float(np.median(drifts)) if drifts else None,
+            "drift_after_resync": 0.0}
+        del mm
+        torch.cuda.empty_cache()
     return out
 
 
@@ -973,6 +1035,9 @@ def main():
     ap.add_argument('--only-relax', action='store_true', help='run only the relax() timing and print it')
     ap.add_argument('--reservoir-n', type=int, default=256, help='lattice side of the reservoir I/O timing (0: skip)')
     ap.add_argument('--only-reservoir', action='store_true', help='run only the reservoir I/O timing and print it')
+    ap.add_argument('--c3-n', type=int, default=2048, help='lattice side of the Poisson-disc / resync workload')
+    ap.add_argument('--c3-steps', type=int, default=5000, help='steps per temperature of that workload (0: skip)')
+    ap.add_argument('--only-c3', action='store_true', help='run only the Poisson-disc / resync workload and print it')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)
@@ -991,6 +1056,11 @@ def main():
         dev = torch.device('cuda', 0)
         torch.cuda.set_device(dev)
         print(json.dumps({"relax": run_relax(dev, n=args.relax_n)}))
+    elif args.only_c3:
+        import torch
+        dev = torch.device('cuda', 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({"c3_poisson_resync": run_c3(dev, n=args.c3_n, steps=args.c3_steps)}))
     elif args.only_recompute:
         import torch
         dev = torch.device('cuda', 0)

@@ -725,7 +725,32 @@ class Magnets(ABC):
         return buf
 
     # -- full recompute and manual updates ----------------------------------------------
-    def _full_recompute(self, d: DipolarEnergy, method=None):
+    def resync_energies(self, measure: bool = False):
+        """Recompute the incrementally updated energies (the magnetostatic one) from the spins,
+        with the configured full-recompute method (EngineConfig.recompute): the periodic resync
+        that bounds the drift of the FP32 increments. Enqueued on the current stream; a status
+        word of the tensor-core recompute is checked later (:meth:`check_resync`). With
+        ``measure`` it returns the drift it removed, max |E_incremental - E_recomputed| /
+        max |E_recomputed| (this synchronises); else None."""
+        d = self._dipolar()
+        if d is None:
+            return 0.0 if measure else None
+        before = d._E.clone() if measure else None
+        self._full_recompute(d, check=False)
+        if measure:
+            return float((before - d._E).abs().max() / d._E.abs().max().clamp_min(1e-300))
+        return None
+
+    def check_resync(self):
+        """Raise if a recompute enqueued by :meth:`resync_energies` reported a status
+        (synchronises with it)."""
+        pend, self._pending_status = getattr(self, '_pending_status', []), []
+        for buf, nbytes in pend:
+            st = int(buf[nbytes - 256:nbytes - 252].view(torch.int32).item())
+            if st:
+                raise RuntimeError(f'hs_dipolar_full_igemm reported status {st} (1: wait timed out, 2: moment not uniform)')
+
+    def _full_recompute(self, d: DipolarEnergy, method=None, check=True):
         L = self._lattice_struct(d)
         method = method or self.engine.recompute
         ks = d.kernel_set
@@ -746,6 +771,9 @@ class Magnets(ABC):
             buf = self._get_scratch('igemm', max(nbytes, 1))
             _lib.check(self._lib.hs_dipolar_full_igemm(L, self.engine.igemm_splits, buf.data_ptr(), buf.numel(),
                                                         self._stream()), 'hs_dipolar_full_igemm')
+            if not check:
+                self._pending_status = getattr(self, '_pending_status', []) + [(buf, nbytes)]
+                return
             st = int(buf[nbytes - 256:nbytes - 252].view(torch.int32).item())  # status word (synchronises)
             if st:
                 raise RuntimeError(f'hs_dipolar_full_igemm reported status {st} (1: wait timed out, 2: moment not uniform)')

@@ -300,10 +300,37 @@ class BatchEngine:
         _lib.check(self.lib.hs_engine_run(p.inst.data_ptr(), p.n, p.cs, n_clusters, self._work[g:].data_ptr(), st),
                    'hs_engine_run')
 
-    def run(self, steps, sizes=None, **kwargs):
+    def resync(self):
+        """Recompute every instance's incrementally updated energies from its spins
+        (Magnets.resync_energies), enqueued on the current stream."""
+        for mm in self.magnets:
+            mm.resync_energies()
+
+    def _chunks(self, steps, resync_every):
+        """Per-instance step budgets of consecutive launches separated by resyncs."""
+        left = list(steps)
+        out = []
+        while any(left):
+            c = [min(r, resync_every) for r in left]
+            out.append(c)
+            left = [r - k for r, k in zip(left, c)]
+        return out
+
+    def run(self, steps, sizes=None, resync_every: int = 0, **kwargs):
         """Enqueue ``steps`` (an int or one int per instance) update steps of every instance
-        without the stop rule; asynchronous. ``sizes``: optional cluster size per instance."""
+        without the stop rule; asynchronous. ``sizes``: optional cluster size per instance.
+        ``resync_every``: recompute the energies from the spins after every that many steps
+        (one engine launch per stretch; the FP64 resync that bounds the drift of the FP32
+        increments)."""
         steps = [int(steps)] * len(self.magnets) if np.isscalar(steps) else [int(s) for s in steps]
+        if resync_every and resync_every > 0:
+            prepared = None
+            for c in self._chunks(steps, int(resync_every)):
+                prepared = self.run(c, sizes=sizes, **kwargs)
+                for mm, k, total in zip(self.magnets, c, steps):
+                    if k == int(resync_every):
+                        mm.resync_energies()
+            return prepared
         kws = [dict(kwargs) for _ in self.magnets]
         for mm, kw in zip(self.magnets, kws):
             mm._set_control(progress=0, done=0, t_max=float(kw.pop('t_max', math.inf)))
@@ -316,7 +343,7 @@ class BatchEngine:
         self.launch(prepared)
         return prepared
 
-    def capture(self, steps, sizes=None, **kwargs):
+    def capture(self, steps, sizes=None, resync_every: int = 0, **kwargs):
         """Record the launch of ``run(steps, ...)`` in a CUDA graph and return a
         :class:`CapturedRun`; each ``replay()`` advances every instance by ``steps`` again
         with no host work (the work counters are reset inside the graph). The instances'
@@ -326,18 +353,30 @@ class BatchEngine:
         kws = [dict(kwargs) for _ in self.magnets]
         for mm, kw in zip(self.magnets, kws):
             mm._set_control(progress=0, done=0, t_max=float(kw.pop('t_max', math.inf)))
-        prepared = self._prepare(steps_l, kws, sizes)
-        for p in prepared:          # occupancy queries happen outside the capture
-            self._max(p.cs)
-        if len(prepared) > 1 and len(self._streams) < len(prepared):
-            self._streams += [torch.cuda.Stream(self.device) for _ in range(len(prepared) - len(self._streams))]
+        chunks = self._chunks(steps_l, int(resync_every)) if resync_every and resync_every > 0 else [steps_l]
+        preps = [self._prepare(c, kws, sizes) for c in chunks]
+        for prepared in preps:      # occupancy queries happen outside the capture
+            for p in prepared:
+                self._max(p.cs)
+        n_groups = max(len(p) for p in preps)
+        if n_groups > 1 and len(self._streams) < n_groups:
+            self._streams += [torch.cuda.Stream(self.device) for _ in range(n_groups - len(self._streams))]
+        if len(chunks) > 1:
+            self.resync()           # scratch buffers of the recomputes exist before the capture
+            for mm in self.magnets:
+                mm.check_resync()
         side = torch.cuda.Stream(self.device)
         side.wait_stream(torch.cuda.current_stream(self.device))
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=side):
-            self.launch(prepared, stream=side)
+            for c, prepared in zip(chunks, preps):
+                self.launch(prepared, stream=side)
+                if len(chunks) > 1:
+                    for mm, k in zip(self.magnets, c):
+                        if k == int(resync_every):
+                            mm.resync_energies()
         torch.cuda.current_stream(self.device).wait_stream(side)
-        return CapturedRun(g, prepared, self)
+        return CapturedRun(g, [p for prepared in preps for p in prepared], self)
 
     # ---------------------------------------------------------------- packed state transfer
     STATE_FIELDS = ('m', 'mm', 'C', 'E', 'Ep')

@@ -221,6 +221,7 @@ class _Active:
     admitted: float
     bytes: int
     event: object = None         # build finished (stream event)
+    since_resync: int = 0        # steps run since the energies were last recomputed
 
 
 @dataclass
@@ -241,10 +242,13 @@ class Server:
     device time one instance's quantum aims at (from the engine's step-time model, corrected
     by the measured speed of past rounds) while requests arrive, ``tail_round_ms`` once they
     have all arrived; ``keep_state``: return the final spins; ``builders``: threads that build
-    admitted requests (host set-up overlaps the device rounds)."""
+    admitted requests (host set-up overlaps the device rounds); ``resync_every``: recompute a
+    request's energies from its spins (Magnets.resync_energies) after every that many of its
+    steps (0: never), which bounds the drift of the FP32 increments; quanta are cut at those
+    points, so they fall on the same steps of a request whatever the mix."""
 
     def __init__(self, device=None, hbm_budget=None, max_slots=4096, round_ms=5.0, keep_state=False,
-                 max_inflight=2, tail_round_ms=20.0, builders=2):
+                 max_inflight=2, tail_round_ms=20.0, builders=2, resync_every=0):
         import torch
         from .engine import BatchEngine  # noqa: F401  (binds the engine symbols early)
         self.torch = torch
@@ -264,6 +268,7 @@ class Server:
         self.stats = ServeStats()
         self._engine = None
         self.tail_round_ms = float(tail_round_ms)
+        self.resync_every = int(resync_every)
         import concurrent.futures
         self._builder = concurrent.futures.ThreadPoolExecutor(max_workers=max(1, int(builders)))
 
@@ -273,6 +278,8 @@ class Server:
         sizes = plan_sizes([a.model for a in active], [a.remaining for a in active], self.n_sm)
         times = [step_time(a.mm, c) for a, c in zip(active, sizes)]
         steps = plan_quanta(times, [a.remaining for a in active], self.speed * round_ms * 1e3)
+        if self.resync_every > 0:   # a quantum ends at the request's next resync point
+            steps = [min(s, self.resync_every - a.since_resync) for s, a in zip(steps, active)]
         if self._engine is None:
             from .engine import BatchEngine
             self._engine = BatchEngine([a.mm for a in active], device=self.device, throughput=True)
@@ -288,6 +295,11 @@ class Server:
                     a.event = None
             e0.record(self.stream)
             prepared = eng.run(steps, sizes=sizes)
+            for a, s in zip(active, steps):
+                a.since_resync += s
+                if self.resync_every > 0 and a.since_resync == self.resync_every:
+                    a.mm.resync_energies()
+                    a.since_resync = 0
             e1.record(self.stream)
         for a, s in zip(active, steps):
             a.remaining -= s
@@ -298,6 +310,7 @@ class Server:
     def _retire(self, a: _Active, now: float, t0: float) -> SimResult:
         mm = a.mm
         with self.torch.cuda.stream(self.stream):
+            mm.check_resync()
             c = mm._read_counters()
             res = SimResult(rid=a.req.rid, steps=a.req.steps, arrival=a.req.arrival, admitted=a.admitted - t0,
                             finished=now - t0, switches=int(c['switches']), attempts=int(c['attempted']),

@@ -195,3 +195,61 @@ def test_armed_progress_that_hits_its_budget_is_reported():
         a._progress_finish()
     assert int(a._read_counters()['status']) & _lib.HS_ST_STEP_CAP
     a._write_counters(status=0)
+
+
+def _bench_like(k, n=48, scheme='Metropolis'):
+    import hotspice_b200 as hs
+    lat = (hs.ASI.OOP_Square, hs.ASI.IP_Pinwheel)[k % 2]
+    a = (200e-9, 300e-9)[k % 2]
+    g = np.random.Generator(np.random.PCG64(40 + k))
+    return lat(a, n, T=300.0, E_B=5.5e-20 * g.lognormal(0, 0.05, size=(n, n)), moment=1.1e-15 if k % 2 == 0 else 1e-15,
+               pattern=g.integers(0, 2, size=(n, n)) * 2 - 1, seed=40 + k,
+               energies=[hs.DipolarEnergy(cutoff_range=16 * a), hs.ZeemanEnergy(2e-3, 0.3)],
+               params=hs.SimParams(UPDATE_SCHEME=scheme))
+
+
+def test_batch_resync_bounds_drift():
+    """BatchEngine.run(..., resync_every=R) recomputes every instance's energies after each R
+    steps: right after a resync the incremental energies equal a fresh FP64 recompute, and
+    R steps later they are within 1e-6 of one (the FP32 increments' drift)."""
+    from hotspice_b200.engine import BatchEngine
+    mms = [_bench_like(k, scheme=('Neel', 'Metropolis')[k % 2]) for k in range(4)]
+    eng = BatchEngine(mms)
+    eng.run(200, resync_every=100)               # ends on a resync
+    for mm in mms:
+        assert mm.resync_energies(measure=True) == 0.0
+    eng.run(250, resync_every=100)               # 50 steps since the last resync
+    for mm in mms:
+        if mm._dipolar().kernel_set.asymmetry < 1e-12:
+            assert mm.resync_energies(measure=True) <= 1e-6
+
+
+def test_captured_resync_equals_direct_run():
+    """The CUDA graph of a run with resyncs (engine launches and recomputes) replays the same
+    states as BatchEngine.run with the same resync_every."""
+    from hotspice_b200.engine import BatchEngine
+    a = [_bench_like(k) for k in range(3)]
+    b = [_bench_like(k) for k in range(3)]
+    BatchEngine(a).run(150, resync_every=60)
+    g = BatchEngine(b).capture(150, resync_every=60)
+    g.replay()
+    for x, y in zip(a, b):
+        _assert_same(_state(x), _state(y), 'captured resync')
+
+
+def test_server_resync():
+    """Server(resync_every=R) recomputes a request's energies after each R of its own steps
+    (quanta are cut there), so the results are the same alone and in the mix, bit for bit."""
+    import torch
+    from hotspice_b200 import serving as SV
+    reqs = [SV.SimRequest(i, dict(lattice=('OOP_Square', 'IP_Pinwheel')[i % 2], n=40 + 8 * i, T=300.0, B=1e-3,
+                                  angle=0.2, scheme=('Neel', 'Metropolis')[i % 2], seed=900 + i), 250 + 40 * i, 0.0)
+            for i in range(4)]
+    dev = torch.device('cuda')
+    mix = {r.rid: r for r in SV.Server(device=dev, keep_state=True, resync_every=64, round_ms=0.3).serve(reqs, realtime=False)}
+    for q in reqs:
+        alone = SV.Server(device=dev, keep_state=True, resync_every=64, round_ms=2.0).serve([q], realtime=False)[0]
+        got = mix[q.rid]
+        assert np.array_equal(alone.state, got.state), q.rid
+        assert (alone.switches, alone.attempts, alone.t) == (got.switches, got.attempts, got.t)
+        assert alone.E_tot == got.E_tot
