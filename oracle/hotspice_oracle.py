@@ -759,10 +759,14 @@ class OracleMagnets:
         return n
 
     def calc_r(self, Q):
-        """hotspice/core.py:720-733."""
-        r = (8e-7 * self.moment ** 2 / (Q * self.kBT)) ** (1 / 3)
-        r = np.clip(r, 0, (self.x_max - self.x_min) + (self.y_max - self.y_min))
-        return float(np.max(r))
+        """hotspice/core.py:720-733, cached per Q for the life of the instance like the
+        reference's lru_cache (a later change of T or moment does not change it there either)."""
+        cache = self.__dict__.setdefault('_calc_r_cache', {})
+        if Q not in cache:
+            r = (8e-7 * self.moment ** 2 / (Q * self.kBT)) ** (1 / 3)
+            r = np.clip(r, 0, (self.x_max - self.x_min) + (self.y_max - self.y_min))
+            cache[Q] = float(np.max(r))
+        return cache[Q]
 
     # -- selection -----------------------------------------------------------------------
     def select(self, **kw):
