@@ -411,9 +411,10 @@ HS_DEV WolffScratch wolff_scratch_of(const HsLattice &L, void *base) {
 
 template <int CS>
 __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsInstance *insts, int n_inst, int *work) {
-    __shared__ int s_inst, s_go, s_n1, s_y1, s_x1, s_nsw;
+    __shared__ int s_inst, s_n1, s_y1, s_x1, s_nsw;
+    __shared__ int s_go[2];                    // step st runs while s_go[st & 1] (double-buffered)
     __shared__ float s_mm1;
-    __shared__ unsigned long long s_call;
+    __shared__ unsigned long long s_call[2];   // Philox call of step st in s_call[st & 1]
     __shared__ __align__(16) HsCounters s_C;   // rank 0: the instance's counters for the whole run
     static_assert(sizeof(HsCounters) % 8 == 0, "HsCounters is copied in 8-byte words");
     __shared__ HsKeyIdx s_part[16];
@@ -456,25 +457,31 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
         // progress() runs: at most `budget` steps in this launch; an unfinished run keeps done = 0
         // and the next launch continues it, so every launch ends
         const int64_t budget = I.steps > 0 ? I.steps : (int64_t)HS_PROGRESS_STEPS_MAX;
-        for (int64_t st = 0;; ++st) {
-            if (rank == 0 && threadIdx.x == 0) {
-                int go;
-                if (C->done) go = 0;
-                else if (C->progress) {
-                    if (C->status || st >= budget) go = 0;   // a failed step, or the budget: not done
-                    else { go = hs_progress_continue(C, L.n_occ); if (!go) { C->done = 1; C->n_sw = 0; } }
-                }
-                else go = st < I.steps;
-                Sync<CS>::publish(&s_go, go);
-                Sync<CS>::publish(&s_call, (unsigned long long)C->rng_call);
+        // Whether step st runs, and its Philox call, are decided by rank 0's thread 0 as soon as
+        // the counters of step st - 1 are final (right after its decision phase) and published
+        // to every CTA in slot st & 1; the barriers that end step st - 1 make them visible, so a
+        // step needs no barrier of its own for this. Slot st & 1 was last read at the start of
+        // step st - 2, before that step's barriers, so the write cannot overtake a read.
+        auto decide_next = [&](int64_t next) {
+            int go;
+            if (C->done) go = 0;
+            else if (C->progress) {
+                if (C->status || next >= budget) go = 0;   // a failed step, or the budget: not done
+                else { go = hs_progress_continue(C, L.n_occ); if (!go) { C->done = 1; C->n_sw = 0; } }
             }
-            Sync<CS>::all();
-            if (!s_go) break;
+            else go = next < I.steps;
+            Sync<CS>::publish(&s_go[next & 1], go);
+            Sync<CS>::publish(&s_call[next & 1], (unsigned long long)C->rng_call);
+        };
+        if (rank == 0 && threadIdx.x == 0) decide_next(0);
+        Sync<CS>::all();
+        for (int64_t st = 0;; ++st) {
+            if (!s_go[st & 1]) break;
             if (scheme == HS_SCHEME_METROPOLIS) {
                 if (rank == 0) {
                     metro_step_cta(L, C, sw, P, metro_scratch_of(L, P, I.scratch));
                     __syncthreads();
-                    if (threadIdx.x == 0) Sync<CS>::publish(&s_nsw, C->n_sw);
+                    if (threadIdx.x == 0) { Sync<CS>::publish(&s_nsw, C->n_sw); decide_next(st + 1); }
                 }
                 Sync<CS>::all();
                 if (L.has_dipolar) {
@@ -484,7 +491,7 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
                 }
                 Sync<CS>::all();
             } else if (scheme == HS_SCHEME_NEEL) {
-                const uint64_t call = s_call;
+                const uint64_t call = s_call[st & 1];
                 const int64_t N = (int64_t)L.nx * L.ny;
                 const int64_t gt = (int64_t)rank * blockDim.x + threadIdx.x, gs = (int64_t)CS * blockDim.x;
                 const bool unif = L.beta_uniform > 0.0;
@@ -546,13 +553,18 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
                         Sync<CS>::publish(&s_x1, (int)(w.idx % L.nx));
                         Sync<CS>::publish(&s_mm1, L.mm[w.idx]);
                     }
+                    decide_next(st + 1);
                 }
                 Sync<CS>::all();
                 if (L.has_dipolar && s_n1 > 0)
                     update_one(L, s_y1, s_x1, s_mm1, rank * blockDim.x + threadIdx.x, CS * blockDim.x, cache);
                 Sync<CS>::all();
             } else {  // Wolff
-                if (rank == 0) wolff_step_cta(L, C, sw, wolff_scratch_of(L, I.scratch));
+                if (rank == 0) {
+                    wolff_step_cta(L, C, sw, wolff_scratch_of(L, I.scratch));
+                    __syncthreads();
+                    if (threadIdx.x == 0) decide_next(st + 1);
+                }
                 Sync<CS>::all();
             }
         }
