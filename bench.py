@@ -944,38 +944,70 @@ SERVED_WORKLOAD = ("served: the first {k} requests of a seeded Poisson arrival s
                    "0-5mT random angle, E_B lognormal(5.5e-20, 5%), dipolar cutoff 16a, Neel / Metropolis alternating")
 
 
-def run_served(dev, args, dist, rank, ws):
-    """Continuous batching against one-request-at-a-time solves on the same arrival stream."""
+OCCUPANCY = {'OOP_Square': 1.0, 'Ising_Square': 1.0, 'IP_Pinwheel': 0.5, 'IP_Kagome': 0.375}
+
+
+def modelled_alone_us(spec, steps):
+    """Modelled device time of a request run alone (engine step-time model at the cluster size
+    the engine gives a lone instance), from its spec without building it."""
+    from types import SimpleNamespace
+    from hotspice_b200 import engine as E
+    from hotspice_b200 import serving as SV
+    from hotspice_b200.core import Scheme
+    ny, nx = SV.geometry_shape(spec)
+    sch = Scheme.WOLFF if spec['lattice'] == 'Ising_Square' else \
+        (Scheme.NEEL if spec.get('scheme', 'Neel') == 'Neel' else Scheme.METROPOLIS)
+    fake = SimpleNamespace(nx=nx, ny=ny, n=int(nx * ny * OCCUPANCY[spec['lattice']]),
+                           params=SimpleNamespace(UPDATE_SCHEME=sch))
+    return steps * E.step_time(fake, E.cluster_size_for(fake))
+
+
+def run_served(dev, args, dist, rank, ws, sample=32):
+    """Continuous batching of the c5 Poisson stream (first `args.served` requests) against
+    one-request-at-a-time solves on the same arrivals. One at a time: a seeded sample of
+    `sample` requests is run to completion alone through Magnets.run (the lone-instance engine
+    launch), timed with CUDA events; the other requests' service times are the engine's step-time
+    model for a lone instance, scaled by the sample's measured / modelled ratio."""
     import torch
     from hotspice_b200 import serving as SV
     reqs = SV.request_stream(args.served, rate=200.0, seed=SEED)
     mine = SV.shard_requests(reqs, ws, rank) if ws > 1 else reqs
     srv = SV.Server(device=dev)
     torch.cuda.synchronize(dev)
+    torch.cuda.reset_peak_memory_stats(dev)
     if dist:
         dist.barrier()
     res = srv.serve(mine, realtime=True)
     torch.cuda.synchronize(dev)
-    # one-at-a-time solves: per-step time of each request alone (a 200-step sample through
-    # Magnets.run, the single-instance persistent launch), scaled to its step budget
-    svc = []
-    for r in mine:
+    peak_alloc = torch.cuda.max_memory_allocated(dev)
+    hist = np.asarray(srv.stats.history, dtype=float).reshape(-1, 3)   # (clock s, resident, round ms)
+    mid = hist[(hist[:, 0] > 0.25 * srv.stats.makespan) & (hist[:, 0] < 0.75 * srv.stats.makespan)]
+    steady = float(mid[:, 1].mean()) if len(mid) else None
+    # one at a time: a measured sample, the rest modelled and calibrated on it
+    g = np.random.Generator(np.random.PCG64(SEED + 11))
+    pick = sorted(g.choice(len(mine), size=min(sample, len(mine)), replace=False).tolist())
+    meas, model = {}, {}
+    for k in pick:
+        r = mine[k]
         mm = SV.build_magnets(r.spec, device=dev)
-        k = min(r.steps, 200)
-        mm.run(k)
+        mm.run(min(r.steps, 50))                     # warm-up: descriptors, graphs
         torch.cuda.synchronize(dev)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        mm.run(k)
+        mm.run(r.steps)
         e1.record()
         torch.cuda.synchronize(dev)
-        svc.append(e0.elapsed_time(e1) * 1e-3 / k * r.steps)
+        meas[k] = e0.elapsed_time(e1) * 1e-3
+        model[k] = modelled_alone_us(r.spec, r.steps) * 1e-6
         del mm
+    calib = sum(meas.values()) / sum(model.values())
+    svc = [meas[k] if k in meas else modelled_alone_us(r.spec, r.steps) * 1e-6 * calib for k, r in enumerate(mine)]
     seq_lat = SV.fifo_latencies([r.arrival for r in mine], svc)
     seq_end = max(a + l for a, l in zip([r.arrival for r in mine], seq_lat))
     mine_stats = dict(lat=[x.latency for x in res], att=sum(x.attempts for x in res), makespan=srv.stats.makespan,
                       seq_lat=list(seq_lat), seq_end=seq_end, rounds=srv.stats.rounds, max_active=srv.stats.max_active,
-                      peak=srv.stats.admitted_bytes_peak, budget=srv.hbm_budget)
+                      peak=srv.stats.admitted_bytes_peak, budget=srv.hbm_budget, steady=steady, calib=calib,
+                      sample_s=sum(meas.values()), peak_alloc=peak_alloc)
     allst = [mine_stats]
     if dist:
         allst = [None] * ws
@@ -989,14 +1021,20 @@ def run_served(dev, args, dist, rank, ws):
     seq_end = max(a['seq_end'] for a in allst)
     return {"workload": SERVED_WORKLOAD.format(k=args.served), "requests": int(lat.size),
             "value": att / makespan, "unit": UNIT, "makespan_s": makespan, "attempts": att,
+            "arrivals_span_s": float(max(r.arrival for r in reqs)),
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "mean_s": float(lat.mean()), "rounds": sum(a['rounds'] for a in allst),
             "max_resident": max(a['max_active'] for a in allst),
+            "steady_resident_mean": allst[0]['steady'],
             "hbm_budget_bytes": allst[0]['budget'], "peak_admitted_bytes": max(a['peak'] for a in allst),
+            "peak_allocated_bytes": max(a['peak_alloc'] for a in allst),
             "sequential": {"p50_s": float(np.percentile(seq, 50)), "p99_s": float(np.percentile(seq, 99)),
                            "makespan_s": seq_end, "value": att / seq_end,
-                           "form": "one request at a time, FIFO over the same arrivals; service time = steps x the "
-                                   "request's per-step time alone (200-step sample through Magnets.run)"},
+                           "sample": f"{len(pick)} requests run alone to completion ({allst[0]['sample_s']:.1f} s of "
+                                     f"device time); measured / modelled service time on them = {allst[0]['calib']:.3f}",
+                           "form": "one request at a time (Magnets.run, the lone-instance engine launch), FIFO over the "
+                                   "same arrivals; service times measured for the sample, modelled x the sample's "
+                                   "calibration for the rest"},
             "served_over_sequential": seq_end / makespan,
             "latency_clock": "host wall clock from each request's arrival to its result on the host"}
 
@@ -1045,7 +1083,8 @@ def main():
     ap.add_argument('--cpu-seconds', type=float, default=2.5)
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-single', action='store_true')
-    ap.add_argument('--served', type=int, default=64, help='requests of the served arrival stream (0: skip)')
+    ap.add_argument('--served', type=int, default=2000, help='requests of the served arrival stream (0: skip)')
+    ap.add_argument('--only-served', action='store_true', help='run only the served stream and print it')
     ap.add_argument('--recompute-n', type=int, default=2048, help='lattice side of the full-recompute timing (0: skip)')
     ap.add_argument('--only-recompute', action='store_true', help='run only the full-recompute timing and print it')
     ap.add_argument('--incremental-n', type=int, default=2048, help='lattice side of the incremental-update timing (0: skip)')
@@ -1075,6 +1114,11 @@ def main():
         dev = torch.device('cuda', 0)
         torch.cuda.set_device(dev)
         print(json.dumps({"relax": run_relax(dev, n=args.relax_n)}))
+    elif args.only_served:
+        import torch
+        dev = torch.device('cuda', 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({"served": run_served(dev, args, None, 0, 1)}))
     elif args.only_c3:
         import torch
         dev = torch.device('cuda', 0)

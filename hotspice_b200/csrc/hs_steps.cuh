@@ -269,7 +269,7 @@ HS_DEV bool metro_grid_fast(const HsLattice &L, HsCounters *C, const HsSwitchLis
     const bool mtime = P.metropolis_time != 0;
     const uint64_t call_time = call + 3;
     const uint64_t call_acc = mtime ? call + 4 : call + 3;
-    if (t < 256) s_bins[t] = 0;
+    for (int b = t; b < 256; b += blockDim.x) s_bins[b] = 0;
     int acc = 0;
     double tpart = 0.0;
     long long near = 0;
@@ -428,7 +428,7 @@ HS_DEV void metro_step_cta(const HsLattice &L, HsCounters *C, const HsSwitchList
     const bool mtime = P.metropolis_time != 0;
     const uint64_t call_time = call;
     const uint64_t call_acc = mtime ? call + 1 : call;
-    if (threadIdx.x < 256) s_bins[threadIdx.x] = 0;
+    for (int b = threadIdx.x; b < 256; b += blockDim.x) s_bins[b] = 0;
     double tpart = 0.0;
     long long near = 0;
     int acc_base = 0;
