@@ -209,18 +209,21 @@ def count_square_vertices(mm: Magnets, counts: bool = False):
     device (hs_square_vertex_counts): the counterpart of count_square_vertices in
     examples/IP_SquareVertices.py:19-35. Vertices are the cells with even x and y; their four
     magnets are the neighbours with periodic wrap. Type 1 is the flower state, 3 and 4 have two
-    and four magnets pointing in, 2 is the rest. ``counts=True`` returns the integer counts."""
+    and four magnets pointing in, 2 is the rest. Like the reference, the fractions require every
+    vertex to be of one of the four types (an odd lattice side wraps a vertex cell in as a
+    neighbour, which the reference's assertion refuses too). ``counts=True`` returns the four
+    integer counts as they are, without that check."""
     import torch
     from . import _lib
     out = torch.empty(4, dtype=torch.int64, device=mm.device)
     _lib.check(_lib.load().hs_square_vertex_counts(mm._m_dev.data_ptr(), mm.nx, mm.ny, out.data_ptr(), mm._stream()),
                'hs_square_vertex_counts')
     c = out.cpu().numpy()
+    if counts:
+        return tuple(int(v) for v in c)
     total = int(c.sum())
     if total != ((mm.nx + 1) // 2) * ((mm.ny + 1) // 2):
         raise RuntimeError(f'vertex counts {c.tolist()} do not add up to the number of vertices')
-    if counts:
-        return tuple(int(v) for v in c)
     return tuple(float(v) / total for v in c)
 
 

@@ -237,22 +237,37 @@ dip_update_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev, int n_h
     }
 }
 
-// Persistent form of dip_update_kernel for lists of at most UPD_LOC switches: a CTA stages the
-// whole list in shared memory once and then walks tiles (tile = blockIdx.x, + gridDim.x, ...).
-// Inside a tile every warp works alone on its UPD_RPW rows, with no block barrier: it tests the
-// staged switches against its rows 32 at a time (ballot, in list order), prefetches its rows of
-// E, E_perp and m*moment into L2 as soon as one switch reaches them, adds the contributions of
-// the hits in list order, and writes E back. Per cell the arithmetic and the summation order are
-// those of dip_update_kernel, so both give the same bits.
+// Persistent form of dip_update_kernel for lists of at most UPD_PLOC switches. A CTA stages the
+// whole list in dynamic shared memory once, then walks tiles (tile = blockIdx.x, + gridDim.x,
+// ...). For every tile the CTA builds the list of switches that reach it, in list order (each
+// thread tests a contiguous chunk of the list; one block scan places the hits), and it builds
+// the NEXT tile's list and prefetches that tile's rows of E, E_perp and m*moment into L2 while it
+// processes the current one, so the DRAM latency of a tile overlaps the work of the previous one.
+// Per cell the arithmetic and the summation order are those of dip_update_kernel, so both give
+// the same bits.
+constexpr int UPD_PLOC = 4096;
+
+struct PersistSmem {                // layout of the dynamic shared memory (n = list bound)
+    SwInfo *sw;                     // [n] the staged list
+    int16_t *hit[2];                // [n] each: hit lists of the current and the next tile
+    static int64_t bytes(int n) { return (int64_t)n * sizeof(SwInfo) + 2 * hs_align_up_d(2LL * n, 16) + 64; }
+};
+
 template <int VEC>
 __global__ void __launch_bounds__(32 * UPD_WARPS, HS_UPD_MIN_CTAS)
 dip_update_persist_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev, int n_host, int semantics,
-                          const HsCounters *C, int tiles) {
+                          const HsCounters *C, int tiles, int cap) {
     if (C && C->done) return;
     const int nsw = n_sw_dev ? *n_sw_dev : n_host;
-    if (nsw <= 0 || nsw > UPD_LOC) return;   // the launcher sends longer lists to dip_update_kernel
+    if (nsw <= 0 || nsw > cap) return;   // the launcher sends longer lists to dip_update_kernel
     constexpr int TX = 32 * VEC;
-    __shared__ SwInfo s_sw[UPD_LOC];
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    SwInfo *s_sw = reinterpret_cast<SwInfo *>(s_dyn);
+    int16_t *s_hit[2];
+    s_hit[0] = reinterpret_cast<int16_t *>(s_dyn + (int64_t)cap * sizeof(SwInfo));
+    s_hit[1] = s_hit[0] + hs_align_up_d(cap, 8);
+    __shared__ int s_tot[UPD_WARPS + 1];
+    __shared__ int s_nhit[2];
     for (int k = threadIdx.x; k < nsw; k += blockDim.x) {
         SwInfo w{sw.y[k], sw.x[k], sw.mode ? sw.mode[k] : 0, -1, 0.f};
         w.sub = hs_sub(L, w.y, w.x);
@@ -265,50 +280,77 @@ dip_update_persist_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev,
     const float pref2 = (float)(2.0 * L.dip_pref);
     const bool flip_perp = !(L.dip_keep_perp_sign && nsw > 1);
     const int KW = 2 * L.dip_wx + 1, KH = 2 * L.dip_wy + 1;
-    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const int y0 = (tile / tiles_x) * UPD_TY + warp * UPD_RPW;   // this warp's first row
-        const int tx0 = (tile % tiles_x) * TX;
-        const int x0 = tx0 + lane * VEC;
-        if (y0 >= L.ny) continue;
-        const int nrows = min(UPD_RPW, L.ny - y0);
-        // does switch w reach this warp's rows (or, without a kernel, sit in them)?
-        auto hits = [&](const SwInfo &w) {
-            if (w.sub < 0)
-                return semantics == HS_UPDATE_MULTIPLE && w.y >= y0 && w.y < y0 + nrows && w.x >= tx0 && w.x < tx0 + TX;
-            int hy, wy_, hx, wx_;
-            hs_window(L, w.mode, true, hy, wy_);
-            hs_window(L, w.mode, false, hx, wx_);
-            return hs_axis_overlap(w.y, hy, wy_, L.ny, y0, nrows) && hs_axis_overlap(w.x, hx, wx_, L.nx, tx0, TX);
-        };
-        // pass 1: is the warp's strip touched at all? then prefetch its energies and sources
-        bool any = false;
-        for (int c = 0; c < nsw && !any; c += 32) {
-            const int k = c + lane;
-            any = __any_sync(0xffffffffu, k < nsw && hits(s_sw[k]));
+    const int chunk = (nsw + blockDim.x - 1) / blockDim.x;   // switches tested by each thread
+
+    // the hits of `tile` in list order into s_hit[b], their count into s_nhit[b]; rows of a
+    // touched tile are prefetched into L2 (block-wide: every thread must call it)
+    auto build_hits = [&](int tile, int b) {
+        const int ty0 = (tile / tiles_x) * UPD_TY, tx0 = (tile % tiles_x) * TX;
+        const int k0 = min(nsw, (int)threadIdx.x * chunk), k1 = min(nsw, k0 + chunk);
+        unsigned mask = 0u;   // chunk <= 16 (UPD_PLOC / blockDim.x)
+        int cnt = 0;
+        for (int k = k0; k < k1; ++k) {
+            const SwInfo w = s_sw[k];
+            bool h;
+            if (w.sub < 0) {
+                h = semantics == HS_UPDATE_MULTIPLE && w.y >= ty0 && w.y < ty0 + UPD_TY && w.x >= tx0 && w.x < tx0 + TX;
+            } else {
+                int hy, wy_, hx, wx_;
+                hs_window(L, w.mode, true, hy, wy_);
+                hs_window(L, w.mode, false, hx, wx_);
+                h = hs_axis_overlap(w.y, hy, wy_, L.ny, ty0, UPD_TY) && hs_axis_overlap(w.x, hx, wx_, L.nx, tx0, TX);
+            }
+            if (h) { mask |= 1u << (k - k0); ++cnt; }
         }
-        if (!any) continue;   // warp-uniform
-        for (int r = 0; r < nrows; ++r) {
-            const int64_t i = (int64_t)(y0 + r) * L.nx + x0;
-            if (x0 < L.nx) {
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(L.E_dip + i));
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(L.mm + i));
-                if (L.use_perp) asm volatile("prefetch.global.L2 [%0];" ::"l"(L.E_dip_perp + i));
+        // exclusive block scan of the per-thread counts
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) { const int t = __shfl_up_sync(0xffffffffu, incl, o); if (lane >= o) incl += t; }
+        if (lane == 31) s_tot[warp] = incl;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int acc = 0;
+            for (int q = 0; q < UPD_WARPS; ++q) { const int v = s_tot[q]; s_tot[q] = acc; acc += v; }
+            s_nhit[b] = acc;
+        }
+        __syncthreads();
+        int pos = s_tot[warp] + incl - cnt;
+        for (int k = k0; mask; ++k, mask >>= 1)
+            if (mask & 1u) s_hit[b][pos++] = (int16_t)k;
+        if (s_nhit[b] > 0) {   // block-uniform: prefetch this warp's rows of the tile
+            for (int r = 0; r < UPD_RPW; ++r) {
+                const int y = ty0 + warp * UPD_RPW + r, x = tx0 + lane * VEC;
+                if (y < L.ny && x < L.nx) {
+                    const int64_t i = (int64_t)y * L.nx + x;
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(L.E_dip + i));
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(L.mm + i));
+                    if (L.use_perp) asm volatile("prefetch.global.L2 [%0];" ::"l"(L.E_dip_perp + i));
+                }
             }
         }
-        // pass 2: contributions of the hits, in list order
-        float acc[UPD_RPW][VEC], accp[UPD_RPW][VEC];
+    };
+
+    int tile = blockIdx.x, cur = 0;
+    if (tile < tiles) build_hits(tile, cur);
+    __syncthreads();
+    for (; tile < tiles; tile += gridDim.x, cur ^= 1) {
+        const int next = tile + gridDim.x;
+        if (next < tiles) build_hits(next, cur ^ 1);   // the next tile's list and its rows' prefetch
+        const int nhit = s_nhit[cur];
+        const int16_t *hl = s_hit[cur];
+        const int y0 = (tile / tiles_x) * UPD_TY + warp * UPD_RPW;
+        const int tx0 = (tile % tiles_x) * TX;
+        const int x0 = tx0 + lane * VEC;
+        if (nhit > 0 && y0 < L.ny) {
+            const int nrows = min(UPD_RPW, L.ny - y0);
+            float acc[UPD_RPW][VEC], accp[UPD_RPW][VEC];
 #pragma unroll
-        for (int r = 0; r < UPD_RPW; ++r)
+            for (int r = 0; r < UPD_RPW; ++r)
 #pragma unroll
-            for (int v = 0; v < VEC; ++v) { acc[r][v] = 0.f; accp[r][v] = 0.f; }
-        unsigned touched = 0u, negate = 0u;   // bit r * VEC + v
-        for (int c = 0; c < nsw; c += 32) {
-            const int k = c + lane;
-            unsigned bal = __ballot_sync(0xffffffffu, k < nsw && hits(s_sw[k]));
-            while (bal) {
-                const int q = c + __ffs(bal) - 1;
-                bal &= bal - 1u;
-                const SwInfo w = s_sw[q];
+                for (int v = 0; v < VEC; ++v) { acc[r][v] = 0.f; accp[r][v] = 0.f; }
+            unsigned touched = 0u, negate = 0u;   // bit r * VEC + v
+            for (int h = 0; h < nhit; ++h) {
+                const SwInfo w = s_sw[hl[h]];
                 if (w.sub >= 0 && !w.mode && !L.dip_wrap) {
                     const int64_t kb = (int64_t)w.sub * KH * KW + (L.dip_wx - w.x);
 #pragma unroll
@@ -352,64 +394,65 @@ dip_update_persist_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev,
                     }
                 }
             }
-        }
-        const bool vec_rows = VEC == 4 && x0 + 3 < L.nx && (L.nx & 3) == 0;
+            const bool vec_rows = VEC == 4 && x0 + 3 < L.nx && (L.nx & 3) == 0;
 #pragma unroll
-        for (int r = 0; r < UPD_RPW; ++r) {
-            if (r >= nrows) continue;
-            const int64_t row = (int64_t)(y0 + r) * L.nx;
-            if (vec_rows) {
-                if (!((touched >> (r * VEC)) & 0xFu)) continue;
-                const float4 mm4 = *reinterpret_cast<const float4 *>(L.mm + row + x0);
-                const float mmv[4] = {mm4.x, mm4.y, mm4.z, mm4.w};
-                const double2 e01 = *reinterpret_cast<const double2 *>(L.E_dip + row + x0);
-                const double2 e23 = *reinterpret_cast<const double2 *>(L.E_dip + row + x0 + 2);
-                double ev[4] = {e01.x, e01.y, e23.x, e23.y};
-                double pv[4] = {0.0, 0.0, 0.0, 0.0};
-                if (L.use_perp) {
-                    const double2 p01 = *reinterpret_cast<const double2 *>(L.E_dip_perp + row + x0);
-                    const double2 p23 = *reinterpret_cast<const double2 *>(L.E_dip_perp + row + x0 + 2);
-                    pv[0] = p01.x; pv[1] = p01.y; pv[2] = p23.x; pv[3] = p23.y;
+            for (int r = 0; r < UPD_RPW; ++r) {
+                if (r >= nrows) continue;
+                const int64_t row = (int64_t)(y0 + r) * L.nx;
+                if (vec_rows) {
+                    if (!((touched >> (r * VEC)) & 0xFu)) continue;
+                    const float4 mm4 = *reinterpret_cast<const float4 *>(L.mm + row + x0);
+                    const float mmv[4] = {mm4.x, mm4.y, mm4.z, mm4.w};
+                    const double2 e01 = *reinterpret_cast<const double2 *>(L.E_dip + row + x0);
+                    const double2 e23 = *reinterpret_cast<const double2 *>(L.E_dip + row + x0 + 2);
+                    double ev[4] = {e01.x, e01.y, e23.x, e23.y};
+                    double pv[4] = {0.0, 0.0, 0.0, 0.0};
+                    if (L.use_perp) {
+                        const double2 p01 = *reinterpret_cast<const double2 *>(L.E_dip_perp + row + x0);
+                        const double2 p23 = *reinterpret_cast<const double2 *>(L.E_dip_perp + row + x0 + 2);
+                        pv[0] = p01.x; pv[1] = p01.y; pv[2] = p23.x; pv[3] = p23.y;
+                    }
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) {
+                        const bool ng = (negate >> (r * VEC + v)) & 1u;
+                        if (semantics == HS_UPDATE_MULTIPLE) {
+                            if (ng) { ev[v] = -ev[v]; if (flip_perp) pv[v] = -pv[v]; }
+                            ev[v] += (double)(pref2 * (mmv[v] * acc[r][v]));
+                            pv[v] += (double)(pref2 * (mmv[v] * accp[r][v]));
+                        } else {
+                            ev[v] += (double)(pref2 * (mmv[v] * acc[r][v]));
+                            pv[v] += (double)(pref2 * (mmv[v] * accp[r][v]));
+                            if (ng) { ev[v] = -ev[v]; pv[v] = -pv[v]; }
+                        }
+                    }
+                    *reinterpret_cast<double2 *>(L.E_dip + row + x0) = make_double2(ev[0], ev[1]);
+                    *reinterpret_cast<double2 *>(L.E_dip + row + x0 + 2) = make_double2(ev[2], ev[3]);
+                    if (L.use_perp) {
+                        *reinterpret_cast<double2 *>(L.E_dip_perp + row + x0) = make_double2(pv[0], pv[1]);
+                        *reinterpret_cast<double2 *>(L.E_dip_perp + row + x0 + 2) = make_double2(pv[2], pv[3]);
+                    }
+                    continue;
                 }
 #pragma unroll
-                for (int v = 0; v < 4; ++v) {
+                for (int v = 0; v < VEC; ++v) {
+                    const int x = x0 + v;
+                    if (x >= L.nx || !((touched >> (r * VEC + v)) & 1u)) continue;
                     const bool ng = (negate >> (r * VEC + v)) & 1u;
-                    if (semantics == HS_UPDATE_MULTIPLE) {
-                        if (ng) { ev[v] = -ev[v]; if (flip_perp) pv[v] = -pv[v]; }
-                        ev[v] += (double)(pref2 * (mmv[v] * acc[r][v]));
-                        pv[v] += (double)(pref2 * (mmv[v] * accp[r][v]));
-                    } else {
-                        ev[v] += (double)(pref2 * (mmv[v] * acc[r][v]));
-                        pv[v] += (double)(pref2 * (mmv[v] * accp[r][v]));
-                        if (ng) { ev[v] = -ev[v]; pv[v] = -pv[v]; }
+                    const float mmv = L.mm[row + x];
+                    double e = L.E_dip[row + x];
+                    if (semantics == HS_UPDATE_MULTIPLE) { if (ng) e = -e; e += (double)(pref2 * (mmv * acc[r][v])); }
+                    else { e += (double)(pref2 * (mmv * acc[r][v])); if (ng) e = -e; }
+                    L.E_dip[row + x] = e;
+                    if (L.use_perp) {
+                        double p = L.E_dip_perp[row + x];
+                        if (semantics == HS_UPDATE_MULTIPLE) { if (ng && flip_perp) p = -p; p += (double)(pref2 * (mmv * accp[r][v])); }
+                        else { p += (double)(pref2 * (mmv * accp[r][v])); if (ng) p = -p; }
+                        L.E_dip_perp[row + x] = p;
                     }
                 }
-                *reinterpret_cast<double2 *>(L.E_dip + row + x0) = make_double2(ev[0], ev[1]);
-                *reinterpret_cast<double2 *>(L.E_dip + row + x0 + 2) = make_double2(ev[2], ev[3]);
-                if (L.use_perp) {
-                    *reinterpret_cast<double2 *>(L.E_dip_perp + row + x0) = make_double2(pv[0], pv[1]);
-                    *reinterpret_cast<double2 *>(L.E_dip_perp + row + x0 + 2) = make_double2(pv[2], pv[3]);
-                }
-                continue;
-            }
-#pragma unroll
-            for (int v = 0; v < VEC; ++v) {
-                const int x = x0 + v;
-                if (x >= L.nx || !((touched >> (r * VEC + v)) & 1u)) continue;
-                const bool ng = (negate >> (r * VEC + v)) & 1u;
-                const float mmv = L.mm[row + x];
-                double e = L.E_dip[row + x];
-                if (semantics == HS_UPDATE_MULTIPLE) { if (ng) e = -e; e += (double)(pref2 * (mmv * acc[r][v])); }
-                else { e += (double)(pref2 * (mmv * acc[r][v])); if (ng) e = -e; }
-                L.E_dip[row + x] = e;
-                if (L.use_perp) {
-                    double p = L.E_dip_perp[row + x];
-                    if (semantics == HS_UPDATE_MULTIPLE) { if (ng && flip_perp) p = -p; p += (double)(pref2 * (mmv * accp[r][v])); }
-                    else { p += (double)(pref2 * (mmv * accp[r][v])); if (ng) p = -p; }
-                    L.E_dip_perp[row + x] = p;
-                }
             }
         }
+        __syncthreads();   // s_hit[cur] is rebuilt two tiles on; s_nhit[cur ^ 1] is read next
     }
 }
 
@@ -465,18 +508,30 @@ __global__ void dip_full_direct_kernel(HsLattice L, int fp64, double *E64, doubl
 }  // namespace
 
 namespace {
-// resident CTAs of the persistent update kernel on this device (queried once per variant)
+// resident CTAs of the persistent update kernel with `smem` bytes of dynamic shared memory
 template <int VEC>
-int persist_grid(int tiles) {
-    static int n = 0;
-    if (n == 0) {
-        int dev = 0, sms = 148, per = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dip_update_persist_kernel<VEC>, 32 * UPD_WARPS, 0);
-        n = sms * std::max(per, 1);
+int persist_grid(int tiles, int64_t smem) {
+    int dev = 0, sms = 148, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dip_update_persist_kernel<VEC>, 32 * UPD_WARPS, (size_t)smem);
+    return std::max(1, std::min(tiles, sms * std::max(per, 1)));
+}
+
+template <int VEC>
+int launch_persist(const HsLattice &L, const HsSwitchList &sw, const int32_t *n_sw_dev, int n_host, int semantics,
+                   const HsCounters *C, int tiles, int cap, cudaStream_t st) {
+    const int64_t smem = PersistSmem::bytes(cap);
+    static int64_t granted = 0;   // dynamic shared memory opted in so far for this variant
+    if (smem > 48 * 1024 && smem > granted) {
+        cudaError_t e = cudaFuncSetAttribute(dip_update_persist_kernel<VEC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) { hs_set_error("dip_update_persist_kernel: %s", cudaGetErrorString(e)); return HS_ECUDA; }
+        granted = smem;
     }
-    return std::max(1, std::min(tiles, n));
+    dip_update_persist_kernel<VEC><<<persist_grid<VEC>(tiles, smem), 32 * UPD_WARPS, (size_t)smem, st>>>(
+        L, sw, n_sw_dev, n_host, semantics, C, tiles, cap);
+    return hs_check_launch("dip_update_persist_kernel");
 }
 }  // namespace
 
@@ -488,12 +543,10 @@ int hs_launch_dipolar_update(const HsLattice &L, const HsSwitchList &sw, const i
     // a list that fits the shared-memory staging goes to the persistent kernel (a device-side
     // count is bounded by the list's capacity)
     const int most = n_sw_dev ? sw.cap : n_host;
-    if (most <= UPD_LOC) {
-        if (vec) dip_update_persist_kernel<4><<<persist_grid<4>(tiles), 32 * UPD_WARPS, 0, st>>>(L, sw, n_sw_dev, n_host,
-                                                                                               semantics, C, tiles);
-        else dip_update_persist_kernel<1><<<persist_grid<1>(tiles), 32 * UPD_WARPS, 0, st>>>(L, sw, n_sw_dev, n_host,
-                                                                                           semantics, C, tiles);
-        return hs_check_launch("dip_update_persist_kernel");
+    if (most <= UPD_PLOC && tiles <= 1 << 20) {
+        const int cap = std::max(most, 1);
+        return vec ? launch_persist<4>(L, sw, n_sw_dev, n_host, semantics, C, tiles, cap, st)
+                   : launch_persist<1>(L, sw, n_sw_dev, n_host, semantics, C, tiles, cap, st);
     }
     if (vec) dip_update_kernel<4><<<tiles, 32 * UPD_WARPS, 0, st>>>(L, sw, n_sw_dev, n_host, semantics, C);
     else dip_update_kernel<1><<<tiles, 32 * UPD_WARPS, 0, st>>>(L, sw, n_sw_dev, n_host, semantics, C);

@@ -32,7 +32,7 @@ namespace {
 #define HS_ENGINE_THREADS 512
 #endif
 constexpr int ENG_NT = HS_ENGINE_THREADS;   // threads per CTA
-constexpr int ENG_MIN_CTAS = ENG_NT <= 256 ? 2 : 1;  // resident CTAs per SM the registers are budgeted for
+constexpr int ENG_MIN_CTAS = 65536 / (ENG_NT * 128);  // resident CTAs per SM at 128 registers a thread
 constexpr int ENG_SWCAP = 512;  // switches staged per CTA in shared memory
 
 struct SwX {                    // staged switch with its window footprint

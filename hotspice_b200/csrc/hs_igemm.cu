@@ -99,7 +99,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volati
                      : "=r"(ok) : "r"(a), "r"(parity) : "memory");
         if (ok) return true;
         if (backoff) __nanosleep(500);
-        if ((it & 255) == 255) {
+        // the clock is read every 256 polls, or on every poll when the limit was shortened
+        if ((it & 255) == 255 || limit_ns < WAIT_NS) {
             if (*abort_flag) return false;
             if (globaltimer_ns() - t0 > limit_ns) { *abort_flag = 1; return false; }
         }

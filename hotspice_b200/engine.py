@@ -106,14 +106,16 @@ def lpt_makespan(durations, n_workers):
     return max(heap)
 
 
-def plan_uniform_size(models, steps, n_sm, sizes=CLUSTER_SIZES):
+def plan_uniform_size(models, steps, n_sm, sizes=CLUSTER_SIZES, workers=None):
     """One cluster size for a whole launch: the size whose longest-first schedule of the
-    modelled run times over the clusters that fit (SM count / size) finishes first. One
-    size per launch keeps clusters of different shapes from fragmenting the GPCs."""
+    modelled run times over the clusters that fit (``workers[cs]``, the resident clusters of
+    that size, else SM count / size) finishes first. One size per launch keeps clusters of
+    different shapes from fragmenting the GPCs."""
     t = _t
     best, best_t = 1, math.inf
     for cs in sizes:
-        mk = lpt_makespan([st * t(m, cs) for m, st in zip(models, steps)], n_sm // cs)
+        nw = workers[cs] if workers else n_sm // cs
+        mk = lpt_makespan([st * t(m, cs) for m, st in zip(models, steps)], nw)
         if mk < best_t * 0.97:
             best, best_t = cs, mk
     return best
@@ -250,7 +252,8 @@ class BatchEngine:
         """Cluster sizes for throughput mode: one size for the launch (:func:`plan_uniform_size`
         over the modelled step times)."""
         n_sm = torch.cuda.get_device_properties(self.device).multi_processor_count
-        cs = plan_uniform_size([step_model(mm) for mm in self.magnets], [max(1, st) for st in steps], n_sm)
+        cs = plan_uniform_size([step_model(mm) for mm in self.magnets], [max(1, st) for st in steps], n_sm,
+                               workers={c: self._max(c) for c in CLUSTER_SIZES})
         return [cs] * len(self.magnets)
 
     def _prepare(self, steps, kws, sizes=None):

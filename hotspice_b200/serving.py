@@ -253,6 +253,8 @@ class Server:
         from .engine import BatchEngine  # noqa: F401  (binds the engine symbols early)
         self.torch = torch
         self.device = torch.device(device) if device is not None else torch.device('cuda', torch.cuda.current_device())
+        if self.device.index is None:
+            self.device = torch.device(self.device.type, torch.cuda.current_device())
         if hbm_budget is None:
             free, _ = torch.cuda.mem_get_info(self.device)
             hbm_budget = free // 2
