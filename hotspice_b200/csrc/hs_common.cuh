@@ -20,8 +20,10 @@ struct HsU4 { uint32_t x, y, z, w; };
 HS_DEV HsU4 hs_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1) {
 #pragma unroll
     for (int r = 0; r < 10; ++r) {
-        const uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
-        const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+        // one 32 x 32 -> 64-bit product per word gives both halves
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        const uint32_t lo0 = (uint32_t)p0, hi0 = (uint32_t)(p0 >> 32);
+        const uint32_t lo1 = (uint32_t)p1, hi1 = (uint32_t)(p1 >> 32);
         const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
         c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
         k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
@@ -29,12 +31,21 @@ HS_DEV HsU4 hs_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32
     return HsU4{c0, c1, c2, c3};
 }
 
-HS_DEV double hs_u53(uint64_t seed, uint64_t call, uint32_t element) {
-    HsU4 w = hs_philox(element, (uint32_t)call, (uint32_t)(call >> 32), 0u,
-                       (uint32_t)seed, (uint32_t)(seed >> 32));
+HS_DEV double hs_u53_of(HsU4 w) {
     const double hi = (double)(w.x >> 5), lo = (double)(w.y >> 6);
     return (hi * 67108864.0 + lo) * (1.0 / 9007199254740992.0);
 }
+
+HS_DEV HsU4 hs_philox_at(uint64_t seed, uint64_t call, uint32_t element) {
+    return hs_philox(element, (uint32_t)call, (uint32_t)(call >> 32), 0u, (uint32_t)seed, (uint32_t)(seed >> 32));
+}
+
+HS_DEV double hs_u53(uint64_t seed, uint64_t call, uint32_t element) {
+    return hs_u53_of(hs_philox_at(seed, call, element));
+}
+
+// A float lower bound of u53 from the first word alone: (w0 >> 8) 2^-24 <= (w0 >> 5) 2^-27 <= u53.
+HS_DEV float hs_u24_low(HsU4 w) { return (float)(w.x >> 8) * 5.9604644775390625e-08f; }
 
 // Exponential variate E1 = -log1p(-u), accurate for small u and for u near 1.
 HS_DEV double hs_exp1_f64(double u) { return -log1p(-u); }
@@ -183,8 +194,9 @@ HS_DEV bool hs_progress_continue(const HsCounters *C, int n_occ) {
     return hs_lower_than(dt, C->t_max) && hs_lower_than(dmc, C->mc_max);
 }
 
-// Arg-min helpers: smaller key wins, ties go to the smaller index (numpy nanargmin).
-struct HsKeyIdx { double key; int idx; };
+// Arg-min helpers: smaller key wins, ties go to the smaller index (numpy nanargmin). A Néel
+// candidate also carries its two barriers, so the step's decision needs no reload of them.
+struct HsKeyIdx { double key; int idx; double b1, b2; };
 HS_DEV HsKeyIdx hs_kmin(HsKeyIdx a, HsKeyIdx b) {
     if (b.idx < 0) return a;
     if (a.idx < 0) return b;
@@ -197,6 +209,8 @@ HS_DEV HsKeyIdx hs_warp_kmin(HsKeyIdx v) {
         HsKeyIdx w;
         w.key = __shfl_xor_sync(0xffffffffu, v.key, o);
         w.idx = __shfl_xor_sync(0xffffffffu, v.idx, o);
+        w.b1 = __shfl_xor_sync(0xffffffffu, v.b1, o);
+        w.b2 = __shfl_xor_sync(0xffffffffu, v.b2, o);
         v = hs_kmin(v, w);
     }
     return v;

@@ -281,6 +281,7 @@ HS_DEV void update_one(const HsLattice &L, int sy, int sx, float smm, int t0, in
         float kv[U], kp[U], mv[U], zf[U], zp[U], eb[U];
         double ev[U], pv[U];
         int8_t oc[U], ms[U];
+        bool live[U];   // in the window and on a unit-cell site that holds magnets
 #pragma unroll
         for (int k = 0; k < U; ++k) {
             const int c = base + k * nt;
@@ -290,10 +291,13 @@ HS_DEV void update_one(const HsLattice &L, int sy, int sx, float smm, int t0, in
             if (col >= L.nx) col -= L.nx;
             rw[k] = row; cl[k] = col;
             idx[k] = row * L.nx + col;
+            // a site without a kernel never holds a magnet: its energy stays 0 (the reference adds
+            // m * ... = 0 there) and the Néel scan never reads its cache entry
+            live[k] = c < total && hs_sub(L, row, col) >= 0;
         }
 #pragma unroll
         for (int k = 0; k < U; ++k) {
-            const bool v = base + k * nt < total;
+            const bool v = live[k];
             const int i = idx[k];
             kv[k] = v ? hs_kval(L, L.K, sub, rw[k] - sy, cl[k] - sx) : 0.f;
             kp[k] = (v && two) ? hs_kval(L, L.Kpo, sub, rw[k] - sy, cl[k] - sx) : 0.f;
@@ -310,7 +314,7 @@ HS_DEV void update_one(const HsLattice &L, int sy, int sx, float smm, int t0, in
         }
 #pragma unroll
         for (int k = 0; k < U; ++k) {
-            if (base + k * nt >= total) continue;
+            if (!live[k]) continue;
             const int i = idx[k];
             float acc = 0.f, accp = 0.f;
             acc += smm * kv[k];

@@ -114,6 +114,8 @@ neel_scan_kernel(HsLattice L, HsCounters *C, HsSwitchList sw, double attempt_fre
         HsKeyIdx p;
         p.key = __ldcg(&S->part[b].key);
         p.idx = __ldcg(&S->part[b].idx);
+        p.b1 = __ldcg(&S->part[b].b1);
+        p.b2 = __ldcg(&S->part[b].b2);
         w = hs_kmin(w, p);
     }
     __syncthreads();

@@ -327,6 +327,103 @@ HS_DEV bool metro_grid_fast(const HsLattice &L, HsCounters *C, const HsSwitchLis
     return true;
 }
 
+// The same step as metro_grid_fast when every supercell fits one warp (n_sc <= 32), executed
+// by a single warp with ballots instead of block scans: candidates, acceptances and switch
+// list in the same order, the per-sublattice switch counts by __match_any_sync, the
+// METROPOLIS_TIME sum by the same xor-shuffle tree (the other warps held only zeros), so the
+// results are identical. Returns false, without side effects, when the step needs the rare
+// branches (the general path then runs it from the same call).
+HS_DEV bool metro_grid_warp(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, const HsGridPlan &P,
+                            uint64_t call) {
+    const int lane = threadIdx.x & 31;
+    int ox, oy;
+    if (L.pbc) {
+        ox = (int)floor(hs_u53(L.seed, call, 0u) * L.nx);
+        oy = (int)floor(hs_u53(L.seed, call + 1, 0u) * L.ny);
+    } else {
+        ox = -P.Rx + (int)floor(hs_u53(L.seed, call, 0u) * (2.0 * P.Rx));
+        oy = -P.Ry + (int)floor(hs_u53(L.seed, call + 1, 0u) * (2.0 * P.Ry));
+    }
+    if (P.Rx == L.nx) ox = 0;
+    if (P.Ry == L.ny) oy = 0;
+    const int phase = pymod(oy, L.uy) * L.ux + pymod(ox, L.ux);
+    const int off = P.phase_off[phase], len = P.phase_off[phase + 1] - off;
+    if (len <= 0) return false;
+    const int nscx = (min(P.snx, L.nx) + 1) / 2;
+    int ok = 0, valid = 0, x = 0, y = 0;
+    if (lane < P.n_sc) {
+        const int pick = (int)floor(hs_u53(L.seed, call + 2, (uint32_t)lane) * len);
+        const int yx = __ldg(P.phase_yx + off + pick);
+        x = 2 * (lane % nscx) * P.Rx + (yx & 0xffff);
+        y = 2 * (lane / nscx) * P.Ry + (yx >> 16);
+        if (L.pbc) {
+            ok = x < max(P.Rx, L.nx - P.Rx) && y < max(P.Ry, L.ny - P.Ry);
+            x = (x + ox) % L.nx; y = (y + oy) % L.ny;
+        } else {
+            x += ox; y += oy;
+            ok = x >= 0 && x < L.nx && y >= 0 && y < L.ny;
+        }
+        valid = ok && L.occ[(int64_t)y * L.nx + x] != 0;
+    }
+    const unsigned below = (1u << lane) - 1u;
+    const unsigned okb = __ballot_sync(0xffffffffu, ok), vb = __ballot_sync(0xffffffffu, valid);
+    const int k = __popc(vb);
+    if (okb == 0u || k == 0) return false;   // warp-uniform
+    const int r = __popc(vb & below);
+    const bool mtime = P.metropolis_time != 0;
+    const uint64_t call_time = call + 3;
+    const uint64_t call_acc = mtime ? call + 4 : call + 3;
+    int acc = 0;
+    double tpart = 0.0;
+    int near = 0;
+    if (valid) {
+        const int64_t i = (int64_t)y * L.nx + x;
+        double E, Ep;
+        hs_energy_at(L, y, x, E, Ep);
+        const double beta = hs_beta(L, i);
+        const double p = fmin(fmax(exp(2.0 * E * beta), 1e-10), 1e10);
+        if (mtime) {
+            double b1, b2;
+            hs_barriers(L, y, x, b1, b2);
+            const double u = hs_u53(L.seed, call_time, (uint32_t)r);
+            tpart = -log(u) / P.attempt_freq / (double)L.n_occ * exp(fmin(b1, b2) * beta);
+        }
+        const double u = hs_u53(L.seed, call_acc, (uint32_t)r);
+        acc = u < p;
+        if (fabs(u - p) <= p * beta * 2e-6 * fabs(E) && p < 1e10 && p > 1e-10) near = 1;
+    }
+    const unsigned accb = __ballot_sync(0xffffffffu, acc);
+    const int nacc = __popc(accb), pa = __popc(accb & below);
+    const int bin = (x % L.ux) + (y % L.uy) * L.ux;
+    const unsigned same = __match_any_sync(0xffffffffu, acc ? bin : -1);
+    if (acc) {
+        const int64_t i = (int64_t)y * L.nx + x;
+        L.m[i] = (int8_t)(-L.m[i]);
+        L.mm[i] = -L.mm[i];
+        if (pa < sw.cap) {
+            sw.y[pa] = y; sw.x[pa] = x;
+            if (sw.mode) sw.mode[pa] = __popc(same & accb) > L.trunc_cutoff ? 1 : 0;
+        }
+    }
+    if (mtime) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) tpart += __shfl_xor_sync(0xffffffffu, tpart, o);
+    }
+    const int nnear = __popc(__ballot_sync(0xffffffffu, near));
+    if (lane == 0) {
+        if (nnear) C->near_threshold += nnear;
+        if (mtime) C->t += tpart;
+        const int ncap = min(nacc, sw.cap);
+        C->attempted += k;
+        C->switches += ncap;
+        C->rng_call = call_acc + 1;
+        C->n_sw = ncap;
+        C->steps += 1;
+        if (nacc > sw.cap) C->status |= HS_ST_SWITCH_OVERFLOW;
+    }
+    return true;
+}
+
 // One Metropolis step executed by one CTA (selection, acceptance, flips, switch list).
 HS_DEV void metro_step_cta(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, const HsGridPlan &P,
                            const MetroScratch &S) {
@@ -342,8 +439,18 @@ HS_DEV void metro_step_cta(const HsLattice &L, HsCounters *C, const HsSwitchList
         return;
     }
     uint64_t call = C->rng_call;
-    if (P.sample_scheme == HS_SAMPLE_GRID && P.n_sc <= (int)blockDim.x && L.ux * L.uy <= 256 &&
-        metro_grid_fast(L, C, sw, P, call))
+    if (P.sample_scheme == HS_SAMPLE_GRID && P.n_sc <= 32) {
+        __shared__ int s_done;
+        if (threadIdx.x < 32) {
+            const bool d = metro_grid_warp(L, C, sw, P, call);
+            if (threadIdx.x == 0) s_done = d;
+        }
+        __syncthreads();
+        const int d = s_done;
+        __syncthreads();   // s_done is rewritten by the next step
+        if (d) return;
+    } else if (P.sample_scheme == HS_SAMPLE_GRID && P.n_sc <= (int)blockDim.x && L.ux * L.uy <= 256 &&
+               metro_grid_fast(L, C, sw, P, call))
         return;
     if (threadIdx.x == 0) s_status = 0;
     int k = 0;
@@ -642,8 +749,8 @@ HS_DEV void neel_finalize(const HsLattice &L, HsCounters *C, const HsSwitchList 
     }
     const int64_t i = w.idx;
     const int y = (int)(i / L.nx), x = (int)(i % L.nx);
-    double b1, b2;
-    hs_barriers(L, y, x, b1, b2);
+    // the barriers the scan computed for this cell (the same operations as hs_barriers)
+    const double b1 = w.b1, b2 = w.b2;
     const double beta = hs_beta(L, i);
     const double e1 = hs_exp1_f64(hs_u53(L.seed, call, (uint32_t)i));
     double time;
@@ -720,7 +827,7 @@ HS_DEV void hs_barriers_from(const HsLattice &L, double E, double Ep, double EB,
 // Néel barrier cache (engine only): per cell s = b_low * beta (uniform beta), rounded down to
 // float, +inf for an empty cell. It lives in the Néel scratch at this offset and is valid only
 // inside one engine launch (built by the launch's first step, refreshed by the window update).
-constexpr int64_t HS_NEEL_CACHE_OFFSET = 32768;
+constexpr int64_t HS_NEEL_CACHE_OFFSET = 65536;
 HS_DEV float neel_cache_value(const HsLattice &L, double E, double Ep, double EB) {
     double b1, b2;
     hs_barriers_from(L, E, Ep, EB, b1, b2);
@@ -794,7 +901,7 @@ HS_DEV HsKeyIdx neel_scan_range(const HsLattice &L, int64_t start64, int64_t str
                 const double bm = fmin(b1, b2), dd = fabs(b1 - b2);
                 key = le1 + (bm - bmin) * beta - (double)log1pf(expf((float)(-dd * beta)));
             }
-            best = hs_kmin(best, HsKeyIdx{key, ci[k]});
+            best = hs_kmin(best, HsKeyIdx{key, ci[k], b1, b2});
         }
     }
     return best;
@@ -814,7 +921,7 @@ HS_DEV HsKeyIdx neel_scan_cached(const HsLattice &L, const float *cache, int64_t
     for (int base = start; base < M; base += stride * NEEL_UNR) {
         int ci[NEEL_UNR];
         float sc[NEEL_UNR];
-        double u[NEEL_UNR];
+        HsU4 wv[NEEL_UNR];
 #pragma unroll
         for (int k = 0; k < NEEL_UNR; ++k) {
             const int j = base + k * stride;
@@ -823,12 +930,14 @@ HS_DEV HsKeyIdx neel_scan_cached(const HsLattice &L, const float *cache, int64_t
 #pragma unroll
         for (int k = 0; k < NEEL_UNR; ++k) sc[k] = base + k * stride < M ? __ldcg(cache + ci[k]) : INFINITY;
 #pragma unroll
-        for (int k = 0; k < NEEL_UNR; ++k) u[k] = hs_u53(L.seed, call, (uint32_t)ci[k]);
+        for (int k = 0; k < NEEL_UNR; ++k) wv[k] = hs_philox_at(L.seed, call, (uint32_t)ci[k]);
 #pragma unroll
         for (int k = 0; k < NEEL_UNR; ++k) {
             if (sc[k] == INFINITY) continue;
-            const double lbk = (double)__logf((float)u[k]) + (double)sc[k] - slack;
+            // bound from the first Philox word (below u53): the FP64 variate only for admitted cells
+            const double lbk = (double)__logf(hs_u24_low(wv[k])) + (double)sc[k] - slack;
             if (best.idx >= 0 && lbk > best.key) continue;
+            const double uk = hs_u53_of(wv[k]);
             const int i = ci[k];
             double E = L.has_dipolar ? __ldcg(L.E_dip + i) : 0.0;
             double Ep = (L.has_dipolar && two) ? __ldcg(L.E_dip_perp + i) : 0.0;
@@ -836,14 +945,14 @@ HS_DEV HsKeyIdx neel_scan_cached(const HsLattice &L, const float *cache, int64_t
             if (L.zee) { E += (double)mv * (double)__ldg(L.zee + i); if (two) Ep += (double)mv * (double)__ldg(L.zee_perp + i); }
             double b1, b2;
             hs_barriers_from(L, E, Ep, (double)__ldg(L.E_B + i), b1, b2);
-            const double le1 = (double)hs_log_exp1_f32(u[k]);
+            const double le1 = (double)hs_log_exp1_f32(uk);
             double key;
             if (!two) key = le1 + b1 * beta;
             else {
                 const double bm = fmin(b1, b2), dd = fabs(b1 - b2);
                 key = le1 + bm * beta - (double)log1pf(expf((float)(-dd * beta)));
             }
-            best = hs_kmin(best, HsKeyIdx{key, i});
+            best = hs_kmin(best, HsKeyIdx{key, i, b1, b2});
         }
     }
     return best;
