@@ -238,11 +238,11 @@ dip_update_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev, int n_h
 }
 
 // Persistent form of dip_update_kernel for lists of at most UPD_PLOC switches. A CTA stages the
-// whole list in dynamic shared memory once, then walks tiles (tile = blockIdx.x, + gridDim.x,
+// whole list in dynamic shared memory once, issues bulk L2 prefetches of the rows of every one
+// of its tiles that a switch reaches, then walks those tiles (tile = blockIdx.x, + gridDim.x,
 // ...). For every tile the CTA builds the list of switches that reach it, in list order (each
-// thread tests a contiguous chunk of the list; one block scan places the hits), and it builds
-// the NEXT tile's list and prefetches that tile's rows of E, E_perp and m*moment into L2 while it
-// processes the current one, so the DRAM latency of a tile overlaps the work of the previous one.
+// thread tests a contiguous chunk of the list; one block scan places the hits), the next
+// tile's list while it processes the current one.
 // Per cell the arithmetic and the summation order are those of dip_update_kernel, so both give
 // the same bits.
 constexpr int UPD_PLOC = 4096;
@@ -268,11 +268,28 @@ dip_update_persist_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev,
     s_hit[1] = s_hit[0] + hs_align_up_d(cap, 8);
     __shared__ int s_tot[UPD_WARPS + 1];
     __shared__ int s_nhit[2];
-    for (int k = threadIdx.x; k < nsw; k += blockDim.x) {
-        SwInfo w{sw.y[k], sw.x[k], sw.mode ? sw.mode[k] : 0, -1, 0.f};
-        w.sub = hs_sub(L, w.y, w.x);
-        if (w.sub >= 0) w.mm = L.mm[(int64_t)w.y * L.nx + w.x];
-        s_sw[k] = w;
+    {   // stage the list; the loads of 8 entries per thread are issued before any is used
+        constexpr int SU = 8;
+        for (int k0 = threadIdx.x; k0 < nsw; k0 += SU * blockDim.x) {
+            int yy[SU], xx[SU], md[SU], sb[SU];
+            float mv[SU];
+#pragma unroll
+            for (int j = 0; j < SU; ++j) {
+                const int k = k0 + j * blockDim.x;
+                const bool v = k < nsw;
+                yy[j] = v ? sw.y[k] : 0;
+                xx[j] = v ? sw.x[k] : 0;
+                md[j] = (v && sw.mode) ? sw.mode[k] : 0;
+            }
+#pragma unroll
+            for (int j = 0; j < SU; ++j) {
+                sb[j] = k0 + j * blockDim.x < nsw ? hs_sub(L, yy[j], xx[j]) : -1;
+                mv[j] = sb[j] >= 0 ? L.mm[(int64_t)yy[j] * L.nx + xx[j]] : 0.f;
+            }
+#pragma unroll
+            for (int j = 0; j < SU; ++j)
+                if (k0 + j * blockDim.x < nsw) s_sw[k0 + j * blockDim.x] = SwInfo{yy[j], xx[j], md[j], sb[j], mv[j]};
+        }
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -282,26 +299,48 @@ dip_update_persist_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev,
     const int KW = 2 * L.dip_wx + 1, KH = 2 * L.dip_wy + 1;
     const int chunk = (nsw + blockDim.x - 1) / blockDim.x;   // switches tested by each thread
 
-    // the hits of `tile` in list order into s_hit[b], their count into s_nhit[b]; rows of a
-    // touched tile are prefetched into L2 (block-wide: every thread must call it)
+    // does switch w reach (or, without a kernel, sit in) the tile at (ty0, tx0)?
+    auto hits_tile = [&](const SwInfo &w, int ty0, int tx0) {
+        if (w.sub < 0)
+            return semantics == HS_UPDATE_MULTIPLE && w.y >= ty0 && w.y < ty0 + UPD_TY && w.x >= tx0 && w.x < tx0 + TX;
+        int hy, wy_, hx, wx_;
+        hs_window(L, w.mode, true, hy, wy_);
+        hs_window(L, w.mode, false, hx, wx_);
+        return hs_axis_overlap(w.y, hy, wy_, L.ny, ty0, UPD_TY) && hs_axis_overlap(w.x, hx, wx_, L.nx, tx0, TX);
+    };
+
+    // Every tile of this CTA that a switch reaches has its rows of E, E_perp and m*moment
+    // prefetched into L2 now, by bulk prefetches (one per row and array), so the DRAM reads of
+    // all of the CTA's tiles stream while it works through them.
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int ty0 = (tile / tiles_x) * UPD_TY, tx0 = (tile % tiles_x) * TX;
+        const int k0 = min(nsw, (int)threadIdx.x * chunk), k1 = min(nsw, k0 + chunk);
+        bool any = false;
+        for (int k = k0; k < k1 && !any; ++k) any = hits_tile(s_sw[k], ty0, tx0);
+        if (__syncthreads_or(any)) {
+            const int cols = min(TX, L.nx - tx0);
+            const int r = threadIdx.x / 3, a = threadIdx.x % 3;    // 16 rows x 3 arrays
+            const int y = ty0 + r;
+            if (r < UPD_TY && y < L.ny && (a < 2 || L.use_perp)) {
+                const int64_t i = (int64_t)y * L.nx + tx0;
+                const void *src = a == 0 ? (const void *)(L.E_dip + i) : a == 1 ? (const void *)(L.mm + i)
+                                                                                : (const void *)(L.E_dip_perp + i);
+                const uint32_t bytes = (uint32_t)(cols * (a == 1 ? 4 : 8)) & ~15u;   // whole 16-byte units only
+                if (bytes > 0 && (reinterpret_cast<uintptr_t>(src) & 15u) == 0)
+                    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+            }
+        }
+    }
+
+    // the hits of `tile` in list order into s_hit[b], their count into s_nhit[b] (block-wide:
+    // every thread must call it)
     auto build_hits = [&](int tile, int b) {
         const int ty0 = (tile / tiles_x) * UPD_TY, tx0 = (tile % tiles_x) * TX;
         const int k0 = min(nsw, (int)threadIdx.x * chunk), k1 = min(nsw, k0 + chunk);
         unsigned mask = 0u;   // chunk <= 16 (UPD_PLOC / blockDim.x)
         int cnt = 0;
-        for (int k = k0; k < k1; ++k) {
-            const SwInfo w = s_sw[k];
-            bool h;
-            if (w.sub < 0) {
-                h = semantics == HS_UPDATE_MULTIPLE && w.y >= ty0 && w.y < ty0 + UPD_TY && w.x >= tx0 && w.x < tx0 + TX;
-            } else {
-                int hy, wy_, hx, wx_;
-                hs_window(L, w.mode, true, hy, wy_);
-                hs_window(L, w.mode, false, hx, wx_);
-                h = hs_axis_overlap(w.y, hy, wy_, L.ny, ty0, UPD_TY) && hs_axis_overlap(w.x, hx, wx_, L.nx, tx0, TX);
-            }
-            if (h) { mask |= 1u << (k - k0); ++cnt; }
-        }
+        for (int k = k0; k < k1; ++k)
+            if (hits_tile(s_sw[k], ty0, tx0)) { mask |= 1u << (k - k0); ++cnt; }
         // exclusive block scan of the per-thread counts
         int incl = cnt;
 #pragma unroll
@@ -317,17 +356,6 @@ dip_update_persist_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev,
         int pos = s_tot[warp] + incl - cnt;
         for (int k = k0; mask; ++k, mask >>= 1)
             if (mask & 1u) s_hit[b][pos++] = (int16_t)k;
-        if (s_nhit[b] > 0) {   // block-uniform: prefetch this warp's rows of the tile
-            for (int r = 0; r < UPD_RPW; ++r) {
-                const int y = ty0 + warp * UPD_RPW + r, x = tx0 + lane * VEC;
-                if (y < L.ny && x < L.nx) {
-                    const int64_t i = (int64_t)y * L.nx + x;
-                    asm volatile("prefetch.global.L2 [%0];" ::"l"(L.E_dip + i));
-                    asm volatile("prefetch.global.L2 [%0];" ::"l"(L.mm + i));
-                    if (L.use_perp) asm volatile("prefetch.global.L2 [%0];" ::"l"(L.E_dip_perp + i));
-                }
-            }
-        }
     };
 
     int tile = blockIdx.x, cur = 0;

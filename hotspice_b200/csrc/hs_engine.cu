@@ -31,8 +31,11 @@ namespace {
 #ifndef HS_ENGINE_THREADS
 #define HS_ENGINE_THREADS 512
 #endif
+#ifndef HS_ENGINE_REGS
+#define HS_ENGINE_REGS 128
+#endif
 constexpr int ENG_NT = HS_ENGINE_THREADS;   // threads per CTA
-constexpr int ENG_MIN_CTAS = 65536 / (ENG_NT * 128);  // resident CTAs per SM at 128 registers a thread
+constexpr int ENG_MIN_CTAS = 65536 / (ENG_NT * HS_ENGINE_REGS);  // resident CTAs per SM at that register budget
 constexpr int ENG_SWCAP = 512;  // switches staged per CTA in shared memory
 
 struct SwX {                    // staged switch with its window footprint
