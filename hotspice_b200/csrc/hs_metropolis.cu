@@ -18,9 +18,12 @@
 namespace {
 
 __global__ void __launch_bounds__(MT) metropolis_kernel(HsLattice L, HsCounters *C, HsSwitchList sw, HsGridPlan P,
-                                                        MetroScratch S) {
-    metro_step_cta(L, C, sw, P, S);
+                                                        MetroScratch S, int ws_bytes) {
+    extern __shared__ __align__(16) unsigned char s_ws[];   // the Poisson-disc sampler's arrays, if given
+    metro_step_cta(L, C, sw, P, S, ws_bytes > 0 ? s_ws : nullptr, ws_bytes);
 }
+
+constexpr int64_t METRO_WS_MAX = 200 * 1024;   // dynamic shared memory the Poisson sampler may use
 
 }  // namespace
 
@@ -56,7 +59,17 @@ int hs_launch_metropolis(const HsLattice &L, HsCounters *C, const HsSwitchList &
     S.pty = reinterpret_cast<double *>(p); p += hs_align_up(8LL * gsz, 256);
     S.queue = reinterpret_cast<int32_t *>(p);
     if (P.sample_scheme == HS_SAMPLE_POISSON && gsz < 1) { hs_set_error("Poisson grid empty"); return HS_EINVAL; }
-    metropolis_kernel<<<1, MT, 0, st>>>(L, C, sw, P, S);
+    int ws = 0;
+    if (P.sample_scheme == HS_SAMPLE_POISSON && hs_poisson_mem_bytes(gsz) <= METRO_WS_MAX) {
+        ws = (int)hs_poisson_mem_bytes(gsz);
+        static int granted = 0;
+        if (ws > 48 * 1024 && ws > granted) {
+            cudaError_t e = cudaFuncSetAttribute(metropolis_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)METRO_WS_MAX);
+            if (e != cudaSuccess) { hs_set_error("metropolis_kernel: %s", cudaGetErrorString(e)); return HS_ECUDA; }
+            granted = (int)METRO_WS_MAX;
+        }
+    }
+    metropolis_kernel<<<1, MT, ws, st>>>(L, C, sw, P, S, ws);
     int rc = hs_check_launch("metropolis_kernel");
     if (rc) return rc;
     if (L.has_dipolar) return hs_launch_dipolar_update(L, sw, &C->n_sw, 0, HS_UPDATE_MULTIPLE, C, st);

@@ -112,89 +112,173 @@ HS_DEV int block_compact(int32_t *py, int32_t *px, int n, F keep, int *warp_tot)
 
 HS_DEV int pymod(int a, int n) { int r = a % n; return r < 0 ? r + n : r; }
 
-// Poisson-disc dart throwing in cell units, executed by warp 0. Returns the number of points
-// written to (py, px) as nearest cell indices, and advances `call` by the variates consumed.
-HS_DEV int poisson_warp(const HsLattice &L, const HsGridPlan &P, const MetroScratch &S, uint64_t &call, int *status) {
+// Work arrays of the Poisson-disc sampler: shared memory when they fit, else the step's scratch.
+struct PoissonMem {
+    int32_t *grid;     // background grid: point index per cell, or -1
+    double *ptx, *pty; // points
+    int32_t *queue;    // active list
+};
+
+// Bytes of the work arrays for a grid of gsz cells (one point per cell at most).
+HS_HD inline int64_t hs_poisson_mem_bytes(int64_t gsz) { return 24 * gsz + 64; }
+
+HS_DEV PoissonMem poisson_mem_in(void *base, int gsz) {
+    char *p = reinterpret_cast<char *>(base);
+    PoissonMem M;
+    M.ptx = reinterpret_cast<double *>(p);
+    M.pty = M.ptx + gsz;
+    M.grid = reinterpret_cast<int32_t *>(M.pty + gsz);
+    M.queue = M.grid + gsz;
+    return M;
+}
+
+// Poisson-disc dart throwing in cell units (hotspice/poisson.py:72-128 restated in cells),
+// executed by one warp. Returns the number of points written to (S.py, S.px) as nearest cell
+// indices and advances `call` by the variates consumed.
+// Bridson's loop is sequential over active points, but the k tries of one active point always
+// consume 1 + 2k variates (queue pick, then angle and distance of each try), so the warp
+// evaluates the k candidates at once (lane t: try t) and their 5x5-cell conflict checks against
+// the existing points in parallel, then resolves them in try order: try t is accepted if it is
+// in bounds, conflicts with no existing point, and with no earlier accepted try whose cell is
+// among the 25 it checks. Two points in one cell always conflict (the cell diagonal is r), so an
+// accepted try never hides an existing point from a later try: the accepted set is the one the
+// sequential loop would build, in the same order, with the same variates.
+HS_DEV int poisson_warp(const HsLattice &L, const HsGridPlan &P, const MetroScratch &S, const PoissonMem &M,
+                        uint64_t &call, int *status) {
     const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
     const double width = L.nx, height = L.ny;
     const double r = P.r_cells + 1.0;
     const double cs = r / sqrt(2.0);
     const double rSq = r * r;
     const int gw = (int)ceil(width / cs), gh = (int)ceil(height / cs);
     const int gsz = gw * gh;
-    if (gsz > S.gsz) { if (lane == 0) *status |= HS_ST_POISSON_OVERFLOW; return 0; }
-    for (int g = lane; g < gsz; g += 32) S.grid[g] = -1;
+    const int K = P.poisson_k;
+    if (gsz > S.gsz || K < 1 || 25 * K > 32 * 32) { if (lane == 0) *status |= HS_ST_POISSON_OVERFLOW; return 0; }
+    for (int g = lane; g < gsz; g += 32) M.grid[g] = -1;
     __syncwarp();
-    auto rnd = [&]() { const double u = hs_u53(L.seed, call, 0u); call += 1; return u; };
-    const double p0x = (double)(int)(width * rnd());
-    const double p0y = (double)(int)(height * rnd());
+    auto rnd_at = [&](uint64_t c) { return hs_u53(L.seed, c, 0u); };
+    const double p0x = (double)(int)(width * rnd_at(call));
+    const double p0y = (double)(int)(height * rnd_at(call + 1));
+    call += 2;
     int npts = 1, nq = 1;
-    if (lane == 0) { S.ptx[0] = p0x; S.pty[0] = p0y; S.queue[0] = 0; S.grid[(int)(p0x / cs) + (int)(p0y / cs) * gw] = 0; }
+    if (lane == 0) { M.ptx[0] = p0x; M.pty[0] = p0y; M.queue[0] = 0; M.grid[(int)(p0x / cs) + (int)(p0y / cs) * gw] = 0; }
     __syncwarp();
-    while (nq > 0) {
-        const int qi = (int)(rnd() * nq);
-        const int q = S.queue[qi];
+    auto conflicts = [&](double px, double py, int g) {   // the distance rule of the grid check
+        double dx = fabs(px - M.ptx[g]), dy = fabs(py - M.pty[g]);
+        if (dx > width * 0.5) dx -= width;
+        if (dy > height * 0.5) dy -= height;
+        return (dx * dx + dy * dy) <= rSq;
+    };
+    bool overflow = false;
+    while (nq > 0 && !overflow) {
+        const int qi = (int)(rnd_at(call) * nq);
+        const uint64_t cbase = call + 1;
+        call += 1 + 2 * (uint64_t)K;
+        const int q = M.queue[qi];
         // list.pop(qi): shift the tail left, preserving order
         for (int j = qi + lane; j < nq - 1; j += 32) {
-            const int v = S.queue[j + 1];
+            const int v = M.queue[j + 1];
             __syncwarp(__activemask());
-            S.queue[j] = v;
+            M.queue[j] = v;
         }
         __syncwarp();
         nq -= 1;
-        const double qx = S.ptx[q], qy = S.pty[q];
-        for (int t = 0; t < P.poisson_k; ++t) {
-            const double alpha = 6.283185307179586 * rnd();
-            const double d = r * sqrt(3.0 * rnd() + 1.0);
-            const double px = qx + d * cos(alpha);
-            const double py = qy + d * sin(alpha);
-            if (!(0.0 <= px && px < width && 0.0 <= py && py < height)) continue;
-            const int gx = (int)(px / cs), gy = (int)(py / cs);
-            bool conflict = false;
-            if (lane < 25) {
-                const int xx = gx - 2 + lane / 5, yy = gy - 2 + lane % 5;
-                const int g = S.grid[pymod(xx + yy * gw, gsz)];
-                if (g >= 0) {
-                    double dx = fabs(px - S.ptx[g]), dy = fabs(py - S.pty[g]);
+        const double qx = M.ptx[q], qy = M.pty[q];
+        // candidates of the k tries, one per lane
+        double px = 0.0, py = 0.0;
+        int gx = 0, gy = 0, inb = 0;
+        if (lane < K) {
+            const double alpha = 6.283185307179586 * rnd_at(cbase + 2 * lane);
+            const double d = r * sqrt(3.0 * rnd_at(cbase + 2 * lane + 1) + 1.0);
+            px = qx + d * cos(alpha);
+            py = qy + d * sin(alpha);
+            inb = 0.0 <= px && px < width && 0.0 <= py && py < height;
+            if (inb) { gx = (int)(px / cs); gy = (int)(py / cs); }
+        }
+        // conflicts with existing points: task id = 25 t + c (cell c of try t's 5x5 neighbourhood)
+        unsigned cmask = 0u;
+        for (int base = 0; base < 25 * K; base += 32) {
+            const int id = base + lane;
+            const int t = id < 25 * K ? id / 25 : 0, c = id - 25 * t;
+            const double tx = __shfl_sync(0xffffffffu, px, t), ty = __shfl_sync(0xffffffffu, py, t);
+            const int tgx = __shfl_sync(0xffffffffu, gx, t), tgy = __shfl_sync(0xffffffffu, gy, t);
+            const int tin = __shfl_sync(0xffffffffu, inb, t);
+            if (id < 25 * K && tin) {
+                const int xx = tgx - 2 + c / 5, yy = tgy - 2 + c % 5;
+                const int g = M.grid[pymod(xx + yy * gw, gsz)];
+                if (g >= 0 && conflicts(tx, ty, g)) cmask |= 1u << t;
+            }
+        }
+        cmask = __reduce_or_sync(0xffffffffu, cmask);
+        // resolve in try order (every lane the same decisions)
+        unsigned amask = 0u;
+        int nacc = 0;
+        for (int t = 0; t < K; ++t) {
+            const double tx = __shfl_sync(0xffffffffu, px, t), ty = __shfl_sync(0xffffffffu, py, t);
+            const int tgx = __shfl_sync(0xffffffffu, gx, t), tgy = __shfl_sync(0xffffffffu, gy, t);
+            const int tin = __shfl_sync(0xffffffffu, inb, t);
+            bool ok = tin && !((cmask >> t) & 1u);
+            for (int u = 0; u < t; ++u) {
+                const double ux = __shfl_sync(0xffffffffu, px, u), uy = __shfl_sync(0xffffffffu, py, u);
+                const int ucell = __shfl_sync(0xffffffffu, gx, u) + __shfl_sync(0xffffffffu, gy, u) * gw;
+                if (!ok || !((amask >> u) & 1u)) continue;
+                bool seen = false;   // is u's cell among the 25 that try t checks?
+                for (int c = 0; c < 25 && !seen; ++c) seen = pymod(tgx - 2 + c / 5 + (tgy - 2 + c % 5) * gw, gsz) == ucell;
+                if (seen) {
+                    double dx = fabs(tx - ux), dy = fabs(ty - uy);
                     if (dx > width * 0.5) dx -= width;
                     if (dy > height * 0.5) dy -= height;
-                    conflict = (dx * dx + dy * dy) <= rSq;
+                    if ((dx * dx + dy * dy) <= rSq) ok = false;
                 }
             }
-            if (__any_sync(0xffffffffu, conflict)) continue;
-            if (npts >= S.gsz) { if (lane == 0) *status |= HS_ST_POISSON_OVERFLOW; break; }
-            if (lane == 0) {
-                S.ptx[npts] = px; S.pty[npts] = py;
-                S.queue[nq] = npts;
-                S.grid[gx + gy * gw] = npts;
-            }
-            __syncwarp();
-            npts += 1; nq += 1;
+            if (!ok) continue;
+            if (npts + nacc >= S.gsz) { overflow = true; break; }
+            amask |= 1u << t;
+            ++nacc;
         }
+        if (lane < K && ((amask >> lane) & 1u)) {
+            const int rank = __popc(amask & below);
+            const int id = npts + rank;
+            M.ptx[id] = px; M.pty[id] = py;
+            M.queue[nq + rank] = id;
+            M.grid[gx + gy * gw] = id;
+        }
+        __syncwarp();
+        npts += nacc;
+        nq += nacc;
     }
+    if (overflow && lane == 0) *status |= HS_ST_POISSON_OVERFLOW;
     __syncwarp();
-    // keep points with x < max(r, w - r), y < max(r, h - r) (PBC=True default), then offset
+    // keep points with x < max(r, w - r), y < max(r, h - r) (PBC=True default), then offset;
+    // in grid-cell order, compacted by the warp
     const double lx = fmax(r, width - r), ly = fmax(r, height - r);
-    const double ox = (double)(int)(rnd() * width), oy = (double)(int)(rnd() * height);
-    if (lane == 0) {
-        int k = 0;
-        for (int g = 0; g < gsz; ++g) {
-            const int p = S.grid[g];
-            if (p < 0) continue;
-            const double x = S.ptx[p], y = S.pty[p];
-            if (!(x >= 0.0 && y >= 0.0 && x < lx && y < ly)) continue;
-            const double fx = fmod(x + ox, width), fy = fmod(y + oy, height);
-            // nearest cell index, ties to the lower index
-            int ix = (int)floor(fx); if (fx - ix > 0.5) ix += 1; ix = min(max(ix, 0), L.nx - 1);
-            int iy = (int)floor(fy); if (fy - iy > 0.5) iy += 1; iy = min(max(iy, 0), L.ny - 1);
-            if (k < S.cap) { S.py[k] = iy; S.px[k] = ix; }
-            ++k;
+    const double ox = (double)(int)(rnd_at(call) * width), oy = (double)(int)(rnd_at(call + 1) * height);
+    call += 2;
+    int k = 0;
+    for (int g0 = 0; g0 < gsz; g0 += 32) {
+        const int g = g0 + lane;
+        const int p = g < gsz ? M.grid[g] : -1;
+        bool keep = false;
+        int ix = 0, iy = 0;
+        if (p >= 0) {
+            const double x = M.ptx[p], y = M.pty[p];
+            keep = x >= 0.0 && y >= 0.0 && x < lx && y < ly;
+            if (keep) {
+                const double fx = fmod(x + ox, width), fy = fmod(y + oy, height);
+                // nearest cell index, ties to the lower index
+                ix = (int)floor(fx); if (fx - ix > 0.5) ix += 1; ix = min(max(ix, 0), L.nx - 1);
+                iy = (int)floor(fy); if (fy - iy > 0.5) iy += 1; iy = min(max(iy, 0), L.ny - 1);
+            }
         }
-        if (k > S.cap) { *status |= HS_ST_POISSON_OVERFLOW; k = S.cap; }
-        S.grid[0] = k;  // hand the count back through memory
+        const unsigned b = __ballot_sync(0xffffffffu, keep);
+        const int pos = k + __popc(b & below);
+        if (keep && pos < S.cap) { S.py[pos] = iy; S.px[pos] = ix; }
+        k += __popc(b);
     }
+    if (k > S.cap) { if (lane == 0) *status |= HS_ST_POISSON_OVERFLOW; k = S.cap; }
     __syncwarp();
-    return S.grid[0];
+    return k;
 }
 
 // Block-wide exclusive scans of two flags at once (3 barriers in total).
@@ -426,7 +510,7 @@ HS_DEV bool metro_grid_warp(const HsLattice &L, HsCounters *C, const HsSwitchLis
 
 // One Metropolis step executed by one CTA (selection, acceptance, flips, switch list).
 HS_DEV void metro_step_cta(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, const HsGridPlan &P,
-                           const MetroScratch &S) {
+                           const MetroScratch &S, void *ws = nullptr, int ws_bytes = 0) {
     __shared__ int warp_tot[33];
     __shared__ int s_k;
     __shared__ uint64_t s_call;
@@ -513,7 +597,12 @@ HS_DEV void metro_step_cta(const HsLattice &L, HsCounters *C, const HsSwitchList
             if (threadIdx.x < 32) {
                 uint64_t c = call;
                 int st = 0;
-                const int n = poisson_warp(L, P, S, c, &st);
+                // the sampler's arrays in the shared workspace when they fit, else in the scratch
+                const int64_t g = (int64_t)hs_poisson_grid_cells(L, P);
+                PoissonMem M;
+                if (ws && hs_poisson_mem_bytes(g) <= ws_bytes) M = poisson_mem_in(ws, (int)g);
+                else { M.grid = S.grid; M.ptx = S.ptx; M.pty = S.pty; M.queue = S.queue; }
+                const int n = poisson_warp(L, P, S, M, c, &st);
                 if (threadIdx.x == 0) { s_k = n; s_call = c; s_status |= st; }
             }
             __syncthreads();

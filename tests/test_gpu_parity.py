@@ -171,6 +171,28 @@ def test_update_single_and_multiple_match_oracle():
         assert rel_err(_np(mp.E), mo.E) < E_TOL, k
 
 
+def test_metropolis_poisson_lockstep_large():
+    """Poisson-disc selection on a 192 x 192 periodic lattice at r = 5a (hundreds of points a
+    step): the warp's parallel evaluation of each active point's tries, resolved in try order,
+    gives the oracle's sequential Bridson candidates, and the same acceptances, step by step."""
+    a, n = 200e-9, 192
+    g = np.random.Generator(np.random.PCG64(78))
+    spec = {'lattice': 'OOP_Square', 'a': a, 'moment': 1e-15, 'nx': n, 'ny': n, 'seed': 78, 'kw': {'PBC': True},
+            'energies': [{'type': 'dipolar', 'cutoff': 6 * a}, {'type': 'zeeman', 'B': 1e-3, 'angle': 0.0}],
+            'params': {'UPDATE_SCHEME': 'Metropolis', 'MULTISAMPLING_SCHEME': 'Poisson'}}
+    fx = {'T': 300.0, 'E_B': 5e-20 * np.ones((n, n)), 'm0': g.integers(0, 2, size=(n, n)) * 2 - 1}
+    mo = build_oracle('poisson_large', spec=spec, fx=fx)
+    mp = build_product('poisson_large', spec=spec, fx=fx)
+    near, decisions, _ = run_metropolis(mp, mo, 8, {'r': 5 * a})
+    assert decisions > 8 * 300
+    assert mp.attempted_switches == mo.attempted_switches
+    assert mp.switches == mo.switches
+    assert np.array_equal(_np(mp.m), mo.m)
+    assert rel_err(_np(mp.E), mo.E) < 2 * E_TOL
+    assert near <= near_bound(decisions)
+    print(f'poisson 192^2: 8 steps, {decisions} candidates, {near} near-threshold')
+
+
 def test_metropolis_poisson_lockstep():
     """Poisson-disc multisampling in cell units: the device's dart throwing (one warp)
     consumes the oracle's variates in the same order, so candidates, acceptances, switch
