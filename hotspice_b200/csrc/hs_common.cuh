@@ -31,6 +31,29 @@ HS_DEV HsU4 hs_philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32
     return HsU4{c0, c1, c2, c3};
 }
 
+// Philox round keys of a seed: (k0 + r 0x9E3779B9, k1 + r 0xBB67AE85), r = 0..9. A loop over
+// many elements with one seed computes them once (they are warp-uniform).
+struct HsRoundKeys { uint32_t k0[10], k1[10]; };
+HS_DEV HsRoundKeys hs_round_keys(uint64_t seed) {
+    HsRoundKeys R;
+    uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+#pragma unroll
+    for (int r = 0; r < 10; ++r) { R.k0[r] = k0; R.k1[r] = k1; k0 += 0x9E3779B9u; k1 += 0xBB67AE85u; }
+    return R;
+}
+// hs_philox with precomputed round keys (the same rounds, bit for bit).
+HS_DEV HsU4 hs_philox_rk(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, const HsRoundKeys &R) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        const uint32_t lo0 = (uint32_t)p0, hi0 = (uint32_t)(p0 >> 32);
+        const uint32_t lo1 = (uint32_t)p1, hi1 = (uint32_t)(p1 >> 32);
+        const uint32_t n0 = hi1 ^ c1 ^ R.k0[r], n2 = hi0 ^ c3 ^ R.k1[r];
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+    }
+    return HsU4{c0, c1, c2, c3};
+}
+
 HS_DEV double hs_u53_of(HsU4 w) {
     const double hi = (double)(w.x >> 5), lo = (double)(w.y >> 6);
     return (hi * 67108864.0 + lo) * (1.0 / 9007199254740992.0);

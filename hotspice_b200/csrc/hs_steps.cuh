@@ -1007,6 +1007,8 @@ HS_DEV HsKeyIdx neel_scan_cached(const HsLattice &L, const float *cache, int64_t
     const int start = (int)start64, stride = (int)stride64;
     const double slack = (two ? 0.6931471805599453 : 0.0) + 1e-4;
     const double beta = L.beta_uniform;
+    const HsRoundKeys RK = hs_round_keys(L.seed);
+    const uint32_t call_lo = (uint32_t)call, call_hi = (uint32_t)(call >> 32);
     for (int base = start; base < M; base += stride * NEEL_UNR) {
         int ci[NEEL_UNR];
         float sc[NEEL_UNR];
@@ -1019,7 +1021,7 @@ HS_DEV HsKeyIdx neel_scan_cached(const HsLattice &L, const float *cache, int64_t
 #pragma unroll
         for (int k = 0; k < NEEL_UNR; ++k) sc[k] = base + k * stride < M ? __ldcg(cache + ci[k]) : INFINITY;
 #pragma unroll
-        for (int k = 0; k < NEEL_UNR; ++k) wv[k] = hs_philox_at(L.seed, call, (uint32_t)ci[k]);
+        for (int k = 0; k < NEEL_UNR; ++k) wv[k] = hs_philox_rk((uint32_t)ci[k], call_lo, call_hi, 0u, RK);
 #pragma unroll
         for (int k = 0; k < NEEL_UNR; ++k) {
             if (sc[k] == INFINITY) continue;
