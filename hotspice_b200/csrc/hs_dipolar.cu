@@ -472,228 +472,6 @@ dip_update_persist_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev,
     }
 }
 
-// Streaming form of the persistent update for 4-cell vectors (nx a multiple of 4): the rows of
-// E, E_perp and m*moment of every touched tile go from HBM into a shared-memory buffer with
-// cp.async 16-byte copies, double-buffered across the CTA's tiles, so tile t+1 is on its way
-// while tile t is computed from shared memory. Hit lists, arithmetic and summation order are
-// those of dip_update_persist_kernel (every cell of a touched tile is written, E + 0 where no
-// window reaches it), so the results are the same bits.
-constexpr int STR_CELLS = UPD_TY * 128;   // cells of one tile
-
-struct StreamSmem {
-    HS_HD static int64_t list_bytes(int cap) { return hs_align_up_d((int64_t)cap * sizeof(SwInfo) + 4LL * hs_align_up_d(cap, 8), 16); }
-    HS_HD static int64_t bytes(int cap) { return list_bytes(cap) + 2LL * STR_CELLS * (8 + 8 + 4); }
-};
-
-HS_DEV void cp_async16(void *dst, const void *src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
-                 : "memory");
-}
-
-__global__ void __launch_bounds__(32 * UPD_WARPS, 2)
-dip_update_stream_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev, int n_host, int semantics,
-                         const HsCounters *C, int tiles, int cap) {
-    if (C && C->done) return;
-    const int nsw = n_sw_dev ? *n_sw_dev : n_host;
-    if (nsw <= 0 || nsw > cap) return;
-    constexpr int VEC = 4, TX = 128;
-    extern __shared__ __align__(16) unsigned char s_dyn[];
-    SwInfo *s_sw = reinterpret_cast<SwInfo *>(s_dyn);
-    int16_t *s_hit[2];
-    s_hit[0] = reinterpret_cast<int16_t *>(s_dyn + (int64_t)cap * sizeof(SwInfo));
-    s_hit[1] = s_hit[0] + hs_align_up_d(cap, 8);
-    double *bufE = reinterpret_cast<double *>(s_dyn + StreamSmem::list_bytes(cap));   // [2][STR_CELLS]
-    double *bufP = bufE + 2 * STR_CELLS;                                                // [2][STR_CELLS]
-    float *bufM = reinterpret_cast<float *>(bufP + 2 * STR_CELLS);                      // [2][STR_CELLS]
-    __shared__ int s_tot[UPD_WARPS + 1];
-    __shared__ int s_nhit[2];
-    {   // stage the list; the loads of 8 entries per thread are issued before any is used
-        constexpr int SU = 8;
-        for (int k0 = threadIdx.x; k0 < nsw; k0 += SU * blockDim.x) {
-            int yy[SU], xx[SU], md[SU], sb[SU];
-            float mv[SU];
-#pragma unroll
-            for (int j = 0; j < SU; ++j) {
-                const int k = k0 + j * blockDim.x;
-                const bool v = k < nsw;
-                yy[j] = v ? sw.y[k] : 0;
-                xx[j] = v ? sw.x[k] : 0;
-                md[j] = (v && sw.mode) ? sw.mode[k] : 0;
-            }
-#pragma unroll
-            for (int j = 0; j < SU; ++j) {
-                sb[j] = k0 + j * blockDim.x < nsw ? hs_sub(L, yy[j], xx[j]) : -1;
-                mv[j] = sb[j] >= 0 ? L.mm[(int64_t)yy[j] * L.nx + xx[j]] : 0.f;
-            }
-#pragma unroll
-            for (int j = 0; j < SU; ++j)
-                if (k0 + j * blockDim.x < nsw) s_sw[k0 + j * blockDim.x] = SwInfo{yy[j], xx[j], md[j], sb[j], mv[j]};
-        }
-    }
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int tiles_x = (L.nx + TX - 1) / TX;
-    const float pref2 = (float)(2.0 * L.dip_pref);
-    const bool flip_perp = !(L.dip_keep_perp_sign && nsw > 1);
-    const bool perp = L.use_perp != 0;
-    const int KW = 2 * L.dip_wx + 1, KH = 2 * L.dip_wy + 1;
-    const int chunk = (nsw + blockDim.x - 1) / blockDim.x;
-
-    auto hits_tile = [&](const SwInfo &w, int ty0, int tx0) {
-        if (w.sub < 0)
-            return semantics == HS_UPDATE_MULTIPLE && w.y >= ty0 && w.y < ty0 + UPD_TY && w.x >= tx0 && w.x < tx0 + TX;
-        int hy, wy_, hx, wx_;
-        hs_window(L, w.mode, true, hy, wy_);
-        hs_window(L, w.mode, false, hx, wx_);
-        return hs_axis_overlap(w.y, hy, wy_, L.ny, ty0, UPD_TY) && hs_axis_overlap(w.x, hx, wx_, L.nx, tx0, TX);
-    };
-    // hit list of `tile` (list order) into s_hit[b], count into s_nhit[b]; then, if the tile is
-    // touched, its rows go into buffer b by cp.async (block-wide: every thread calls it)
-    auto prepare = [&](int tile, int b) {
-        const int ty0 = (tile / tiles_x) * UPD_TY, tx0 = (tile % tiles_x) * TX;
-        const int k0 = min(nsw, (int)threadIdx.x * chunk), k1 = min(nsw, k0 + chunk);
-        unsigned mask = 0u;
-        int cnt = 0;
-        for (int k = k0; k < k1; ++k)
-            if (hits_tile(s_sw[k], ty0, tx0)) { mask |= 1u << (k - k0); ++cnt; }
-        int incl = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) { const int t = __shfl_up_sync(0xffffffffu, incl, o); if (lane >= o) incl += t; }
-        if (lane == 31) s_tot[warp] = incl;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int acc = 0;
-            for (int q = 0; q < UPD_WARPS; ++q) { const int v = s_tot[q]; s_tot[q] = acc; acc += v; }
-            s_nhit[b] = acc;
-        }
-        __syncthreads();
-        int pos = s_tot[warp] + incl - cnt;
-        for (int k = k0; mask; ++k, mask >>= 1)
-            if (mask & 1u) s_hit[b][pos++] = (int16_t)k;
-        if (s_nhit[b] > 0) {
-            const int cols = min(TX, L.nx - tx0);            // a multiple of 4
-            double *dE = bufE + b * STR_CELLS, *dP = bufP + b * STR_CELLS;
-            float *dM = bufM + b * STR_CELLS;
-            for (int c = threadIdx.x; c < UPD_TY * 64; c += blockDim.x) {   // 2 doubles per copy
-                const int r = c >> 6, q = 2 * (c & 63), y = ty0 + r;
-                if (y < L.ny && q < cols) {
-                    const int64_t i = (int64_t)y * L.nx + tx0 + q;
-                    cp_async16(dE + r * TX + q, L.E_dip + i);
-                    if (perp) cp_async16(dP + r * TX + q, L.E_dip_perp + i);
-                }
-            }
-            for (int c = threadIdx.x; c < UPD_TY * 32; c += blockDim.x) {   // 4 floats per copy
-                const int r = c >> 5, q = 4 * (c & 31), y = ty0 + r;
-                if (y < L.ny && q < cols) cp_async16(dM + r * TX + q, L.mm + (int64_t)y * L.nx + tx0 + q);
-            }
-        }
-        asm volatile("cp.async.commit_group;" ::: "memory");
-    };
-
-    int tile = blockIdx.x, cur = 0;
-    if (tile < tiles) prepare(tile, cur);
-    for (; tile < tiles; tile += gridDim.x, cur ^= 1) {
-        const int next = tile + gridDim.x;
-        if (next < tiles) prepare(next, cur ^ 1);
-        else asm volatile("cp.async.commit_group;" ::: "memory");
-        asm volatile("cp.async.wait_group 1;" ::: "memory");   // this tile's copies (not the next one's) have landed
-        __syncthreads();
-        const int nhit = s_nhit[cur];
-        const int16_t *hl = s_hit[cur];
-        const int y0 = (tile / tiles_x) * UPD_TY + warp * UPD_RPW;
-        const int tx0 = (tile % tiles_x) * TX;
-        const int x0 = tx0 + lane * VEC;
-        if (nhit > 0 && y0 < L.ny && x0 < L.nx) {
-            const int nrows = min(UPD_RPW, L.ny - y0);
-            float acc[UPD_RPW][VEC], accp[UPD_RPW][VEC];
-#pragma unroll
-            for (int r = 0; r < UPD_RPW; ++r)
-#pragma unroll
-                for (int v = 0; v < VEC; ++v) { acc[r][v] = 0.f; accp[r][v] = 0.f; }
-            unsigned negate = 0u;   // bit r * VEC + v
-            for (int h = 0; h < nhit; ++h) {
-                const SwInfo w = s_sw[hl[h]];
-                if (w.sub >= 0 && !w.mode && !L.dip_wrap) {
-                    const int64_t kb = (int64_t)w.sub * KH * KW + (L.dip_wx - w.x);
-#pragma unroll
-                    for (int r = 0; r < UPD_RPW; ++r) {
-                        if (r >= nrows) continue;
-                        const int dy = y0 + r - w.y;
-                        if (dy < -L.dip_wy || dy > L.dip_wy) continue;
-                        const float *Kr = L.K + kb + (int64_t)(dy + L.dip_wy) * KW;
-                        const float *Kpr = perp ? L.Kpo + kb + (int64_t)(dy + L.dip_wy) * KW : nullptr;
-#pragma unroll
-                        for (int v = 0; v < VEC; ++v) {
-                            const int x = x0 + v, dx = x - w.x;
-                            if (dx >= -L.dip_wx && dx <= L.dip_wx) {
-                                acc[r][v] += w.mm * __ldg(Kr + x);
-                                if (perp) accp[r][v] += w.mm * __ldg(Kpr + x);
-                                if (dy == 0 && dx == 0) negate |= 1u << (r * VEC + v);
-                            }
-                        }
-                    }
-                    continue;
-                }
-#pragma unroll
-                for (int r = 0; r < UPD_RPW; ++r) {
-                    if (r >= nrows) continue;
-                    const int y = y0 + r;
-#pragma unroll
-                    for (int v = 0; v < VEC; ++v) {
-                        const int x = x0 + v;
-                        if (w.sub >= 0) {
-                            float a = acc[r][v], ap = accp[r][v];
-                            hs_contrib(L, w, y, x, a, ap);
-                            acc[r][v] = a; accp[r][v] = ap;
-                        }
-                        if (w.y == y && w.x == x) negate |= 1u << (r * VEC + v);
-                    }
-                }
-            }
-            const double *sE = bufE + cur * STR_CELLS, *sP = bufP + cur * STR_CELLS;
-            const float *sM = bufM + cur * STR_CELLS;
-#pragma unroll
-            for (int r = 0; r < UPD_RPW; ++r) {
-                if (r >= nrows) continue;
-                const int lr = warp * UPD_RPW + r, lc = lane * VEC;
-                const float4 mm4 = *reinterpret_cast<const float4 *>(sM + lr * TX + lc);
-                const float mmv[4] = {mm4.x, mm4.y, mm4.z, mm4.w};
-                const double2 e01 = *reinterpret_cast<const double2 *>(sE + lr * TX + lc);
-                const double2 e23 = *reinterpret_cast<const double2 *>(sE + lr * TX + lc + 2);
-                double ev[4] = {e01.x, e01.y, e23.x, e23.y};
-                double pv[4] = {0.0, 0.0, 0.0, 0.0};
-                if (perp) {
-                    const double2 p01 = *reinterpret_cast<const double2 *>(sP + lr * TX + lc);
-                    const double2 p23 = *reinterpret_cast<const double2 *>(sP + lr * TX + lc + 2);
-                    pv[0] = p01.x; pv[1] = p01.y; pv[2] = p23.x; pv[3] = p23.y;
-                }
-#pragma unroll
-                for (int v = 0; v < 4; ++v) {
-                    const bool ng = (negate >> (r * VEC + v)) & 1u;
-                    if (semantics == HS_UPDATE_MULTIPLE) {
-                        if (ng) { ev[v] = -ev[v]; if (flip_perp) pv[v] = -pv[v]; }
-                        ev[v] += (double)(pref2 * (mmv[v] * acc[r][v]));
-                        pv[v] += (double)(pref2 * (mmv[v] * accp[r][v]));
-                    } else {
-                        ev[v] += (double)(pref2 * (mmv[v] * acc[r][v]));
-                        pv[v] += (double)(pref2 * (mmv[v] * accp[r][v]));
-                        if (ng) { ev[v] = -ev[v]; pv[v] = -pv[v]; }
-                    }
-                }
-                const int64_t row = (int64_t)(y0 + r) * L.nx;
-                *reinterpret_cast<double2 *>(L.E_dip + row + x0) = make_double2(ev[0], ev[1]);
-                *reinterpret_cast<double2 *>(L.E_dip + row + x0 + 2) = make_double2(ev[2], ev[3]);
-                if (perp) {
-                    *reinterpret_cast<double2 *>(L.E_dip_perp + row + x0) = make_double2(pv[0], pv[1]);
-                    *reinterpret_cast<double2 *>(L.E_dip_perp + row + x0 + 2) = make_double2(pv[2], pv[3]);
-                }
-            }
-        }
-        __syncthreads();   // buffer cur and s_hit[cur] are refilled by the next iteration's prepare
-    }
-    asm volatile("cp.async.wait_group 0;" ::: "memory");   // nothing left in flight at exit
-}
-
 // Direct-sum full recompute, one thread per target cell (hotspice/energies.py:290-308):
 //   E_i = pref * mu_i * m_i * sum_j K_{s(i)}(j - i) * mm_j,  E_perp with the perp-self kernel.
 template <typename Acc, bool FULLWIN>
@@ -781,25 +559,6 @@ int hs_launch_dipolar_update(const HsLattice &L, const HsSwitchList &sw, const i
     // a list that fits the shared-memory staging goes to the persistent kernel (a device-side
     // count is bounded by the list's capacity)
     const int most = n_sw_dev ? sw.cap : n_host;
-    const bool aligned = ((reinterpret_cast<uintptr_t>(L.E_dip) | reinterpret_cast<uintptr_t>(L.mm) |
-                           (L.use_perp ? reinterpret_cast<uintptr_t>(L.E_dip_perp) : 0)) & 15u) == 0;
-    if (vec && aligned && most <= UPD_PLOC && tiles <= 1 << 20) {
-        const int cap = std::max(most, 1);
-        const int64_t smem = StreamSmem::bytes(cap);
-        static int64_t granted = 0;
-        if (smem > 48 * 1024 && smem > granted) {
-            cudaError_t e = cudaFuncSetAttribute(dip_update_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) { hs_set_error("dip_update_stream_kernel: %s", cudaGetErrorString(e)); return HS_ECUDA; }
-            granted = smem;
-        }
-        int dev = 0, sms = 148, per = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dip_update_stream_kernel, 32 * UPD_WARPS, (size_t)smem);
-        const int grid = std::max(1, std::min(tiles, sms * std::max(per, 1)));
-        dip_update_stream_kernel<<<grid, 32 * UPD_WARPS, (size_t)smem, st>>>(L, sw, n_sw_dev, n_host, semantics, C, tiles, cap);
-        return hs_check_launch("dip_update_stream_kernel");
-    }
     if (most <= UPD_PLOC && tiles <= 1 << 20) {
         const int cap = std::max(most, 1);
         return vec ? launch_persist<4>(L, sw, n_sw_dev, n_host, semantics, C, tiles, cap, st)

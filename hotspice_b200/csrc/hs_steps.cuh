@@ -223,8 +223,10 @@ HS_DEV int poisson_warp(const HsLattice &L, const HsGridPlan &P, const MetroScra
                 const double ux = __shfl_sync(0xffffffffu, px, u), uy = __shfl_sync(0xffffffffu, py, u);
                 const int ucell = __shfl_sync(0xffffffffu, gx, u) + __shfl_sync(0xffffffffu, gy, u) * gw;
                 if (!ok || !((amask >> u) & 1u)) continue;
-                bool seen = false;   // is u's cell among the 25 that try t checks?
-                for (int c = 0; c < 25 && !seen; ++c) seen = pymod(tgx - 2 + c / 5 + (tgy - 2 + c % 5) * gw, gsz) == ucell;
+                // is u's cell among the 25 that try t checks (flat indices (xx + yy gw) mod gsz,
+                // xx in [tgx-2, tgx+2])? per row yy: (ucell - yy gw - (tgx-2)) mod gsz <= 4
+                bool seen = false;
+                for (int b = 0; b < 5 && !seen; ++b) seen = pymod(ucell - (tgy - 2 + b) * gw - (tgx - 2), gsz) <= 4;
                 if (seen) {
                     double dx = fabs(tx - ux), dy = fabs(ty - uy);
                     if (dx > width * 0.5) dx -= width;
