@@ -1010,7 +1010,9 @@ def run_served(dev, args, dist, rank, ws, sample=32):
     mine_stats = dict(lat=[x.latency for x in res], att=sum(x.attempts for x in res), makespan=srv.stats.makespan,
                       seq_lat=list(seq_lat), seq_end=seq_end, rounds=srv.stats.rounds, max_active=srv.stats.max_active,
                       peak=srv.stats.admitted_bytes_peak, budget=srv.hbm_budget, steady=steady, calib=calib,
-                      sample_s=sum(meas.values()), peak_alloc=peak_alloc)
+                      sample_s=sum(meas.values()), peak_alloc=peak_alloc, build_s=srv.stats.build_s,
+                      last_active=srv.stats.last_active_s, round_ms=srv.stats.round_ms_sum,
+                      finish_p90=float(np.percentile([x.finished for x in res], 90)))
     allst = [mine_stats]
     if dist:
         allst = [None] * ws
@@ -1031,6 +1033,10 @@ def run_served(dev, args, dist, rank, ws, sample=32):
             "steady_resident_mean": allst[0]['steady'],
             "hbm_budget_bytes": allst[0]['budget'], "peak_admitted_bytes": max(a['peak'] for a in allst),
             "peak_allocated_bytes": max(a['peak_alloc'] for a in allst),
+            "host_build_s": sum(a['build_s'] for a in allst),
+            "last_request_resident_s": max(a['last_active'] for a in allst),
+            "round_device_s": sum(a['round_ms'] for a in allst) * 1e-3,
+            "finish_p90_s": max(a['finish_p90'] for a in allst),
             "sequential": {"p50_s": float(np.percentile(seq, 50)), "p99_s": float(np.percentile(seq, 99)),
                            "makespan_s": seq_end, "value": att / seq_end,
                            "sample": f"{len(pick)} requests run alone to completion ({allst[0]['sample_s']:.1f} s of "

@@ -232,6 +232,9 @@ class ServeStats:
     attempts: int = 0
     admitted_bytes_peak: int = 0
     history: list = field(default_factory=list)
+    build_s: float = 0.0          # host time spent building admitted requests (summed over builders)
+    last_active_s: float = 0.0    # when the last request became resident (s after the start)
+    round_ms_sum: float = 0.0     # device time of the rounds (two may overlap)
 
 
 class Server:
@@ -344,11 +347,13 @@ class Server:
 
         def build(r):
             # runs on the builder thread: its own stream, an event the rounds wait on
+            tb = time.perf_counter()
             torch.cuda.set_device(self.device)
             with torch.cuda.stream(self.build_stream):
                 mm = build_magnets(r.spec, device=self.device)
                 ev = torch.cuda.Event()
                 ev.record(self.build_stream)
+            st.build_s += time.perf_counter() - tb
             return mm, ev
 
         def admit():
@@ -369,6 +374,7 @@ class Server:
                 if fut.done():
                     mm, ev = fut.result()
                     active.append(_Active(r, mm, int(r.steps), step_model(mm), time.perf_counter(), b, ev))
+                    st.last_active_s = clock()
                     changed = True
                 else:
                     still.append((r, b, fut))
@@ -402,6 +408,7 @@ class Server:
                     speed = rd['sm_us'] / (ms * 1e3) / busy
                     self.speed = min(4.0, max(0.25, 0.5 * self.speed + 0.5 * speed))
                 st.history.append((clock(), len(rd['members']), ms))
+                st.round_ms_sum += ms
                 now = time.perf_counter()
                 done_ids = set()
                 for a in rd['members']:
