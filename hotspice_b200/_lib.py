@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(HERE, 'libhotspice_sm100.so')
 HS_OK, HS_EINVAL, HS_ENOMEM, HS_ETIMEDOUT, HS_ECUDA, HS_ERANGE = 0, -1, -2, -3, -4, -5
 HS_ST_SELECT_RETRY, HS_ST_SWITCH_OVERFLOW, HS_ST_POISSON_OVERFLOW, HS_ST_WOLFF_OVERFLOW, HS_ST_STEP_CAP = 1, 2, 4, 8, 16
 HS_PROGRESS_STEPS_MAX = 1 << 22
+HS_ENGINE_WS_DEFAULT, HS_ENGINE_WS_MAX = 64 * 1024, 160 * 1024
 HS_SAMPLE_SINGLE, HS_SAMPLE_GRID, HS_SAMPLE_POISSON = 0, 1, 2
 HS_BARRIER_SIMPLE, HS_BARRIER_PARABOLIC = 0, 1
 HS_UPDATE_SINGLE, HS_UPDATE_MULTIPLE = 0, 1
@@ -108,6 +109,7 @@ SIGNATURES = {
     'hs_square_vertex_counts': (C.c_int, [P, C.c_int32, C.c_int32, P, P]),
     'hs_segments_copy': (C.c_int, [P, P, C.c_int32, C.c_int32, P]),
     'hs_engine_run': (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, P, P]),
+    'hs_engine_run_ws': (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, P, C.c_int32, P]),
     'hs_engine_max_clusters': (C.c_int, [C.c_int32]),
     'hs_exchange_energy': (C.c_int, [C.POINTER(HsLattice), P, P, P]),
     'hs_switch_energy': (C.c_int, [C.POINTER(HsLattice), P, P]),

@@ -330,7 +330,21 @@ int hs_engine_run(const HsInstance *insts, int32_t n_inst, int32_t cluster_size,
                   void *stream) {
     if (!insts || !work || n_inst < 0 || n_clusters <= 0) { hs_set_error("hs_engine_run: bad arguments"); return HS_EINVAL; }
     if (n_inst == 0) return HS_OK;
-    return hs_launch_engine(insts, n_inst, cluster_size, n_clusters, work, (cudaStream_t)stream);
+    return hs_launch_engine(insts, n_inst, cluster_size, n_clusters, work, HS_ENGINE_WS_DEFAULT, (cudaStream_t)stream);
+}
+
+int hs_engine_run_ws(const HsInstance *insts, int32_t n_inst, int32_t cluster_size, int32_t n_clusters, int32_t *work,
+                     int32_t ws_bytes, void *stream) {
+    if (!insts || !work || n_inst < 0 || n_clusters <= 0) {
+        hs_set_error("hs_engine_run_ws: bad arguments");
+        return HS_EINVAL;
+    }
+    if (ws_bytes < 0 || ws_bytes > HS_ENGINE_WS_MAX) {
+        hs_set_error("hs_engine_run_ws: workspace of %d bytes outside [0, %d]", (int)ws_bytes, HS_ENGINE_WS_MAX);
+        return HS_EINVAL;
+    }
+    if (n_inst == 0) return HS_OK;
+    return hs_launch_engine(insts, n_inst, cluster_size, n_clusters, work, ws_bytes, (cudaStream_t)stream);
 }
 
 int hs_engine_max_clusters(int32_t cluster_size) { return hs_engine_max_clusters_impl(cluster_size); }

@@ -37,10 +37,7 @@ namespace {
 constexpr int ENG_NT = HS_ENGINE_THREADS;   // threads per CTA
 constexpr int ENG_MIN_CTAS = 65536 / (ENG_NT * HS_ENGINE_REGS);  // resident CTAs per SM at that register budget
 constexpr int ENG_SWCAP = 512;  // switches staged per CTA in shared memory
-#ifndef HS_ENGINE_WS
-#define HS_ENGINE_WS (64 * 1024)
-#endif
-constexpr int ENG_WS = HS_ENGINE_WS;  // dynamic shared workspace of every CTA (the Poisson-disc sampler's arrays)
+constexpr int ENG_WS_MAX = HS_ENGINE_WS_MAX;  // largest dynamic shared workspace a launch may ask for
 
 struct SwX {                    // staged switch with its window footprint
     int y, x, mode, sub;
@@ -421,7 +418,10 @@ HS_DEV WolffScratch wolff_scratch_of(const HsLattice &L, void *base) {
 }
 
 template <int CS>
-__global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsInstance *insts, int n_inst, int *work) {
+__global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsInstance *insts, int n_inst, int *work,
+                                                                      int ws_bytes) {
+    // dynamic shared workspace (the Poisson-disc sampler's arrays), given only to launches that
+    // hold Poisson-disc instances: it takes L1 capacity from the other phases
     extern __shared__ __align__(16) unsigned char s_ws[];
     __shared__ int s_inst, s_n1, s_y1, s_x1, s_nsw;
     __shared__ int s_go[2];                    // step st runs while s_go[st & 1] (double-buffered)
@@ -491,7 +491,8 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
             if (!s_go[st & 1]) break;
             if (scheme == HS_SCHEME_METROPOLIS) {
                 if (rank == 0) {
-                    metro_step_cta(L, C, sw, P, metro_scratch_of(L, P, I.scratch), s_ws, ENG_WS);
+                    metro_step_cta(L, C, sw, P, metro_scratch_of(L, P, I.scratch), ws_bytes > 0 ? s_ws : nullptr,
+                                   ws_bytes);
                     __syncthreads();
                     if (threadIdx.x == 0) { Sync<CS>::publish(&s_nsw, C->n_sw); decide_next(st + 1); }
                 }
@@ -591,20 +592,20 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
 }
 
 template <int CS>
-cudaError_t engine_allow_ws() {   // opt in to the dynamic workspace beyond 48 KB (once per instantiation)
-    static bool done = false;
-    if (done) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(engine_kernel<CS>, cudaFuncAttributeMaxDynamicSharedMemorySize, ENG_WS);
-    if (e == cudaSuccess) done = true;
+cudaError_t engine_allow_ws(int bytes) {   // opt in to a dynamic workspace beyond 48 KB (once per size)
+    static int granted = 48 * 1024;
+    if (bytes <= granted) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(engine_kernel<CS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) granted = bytes;
     return e;
 }
 
 template <int CS>
-int launch_engine(const HsInstance *insts, int n_inst, int *work, int n_clusters, cudaStream_t st) {
+int launch_engine(const HsInstance *insts, int n_inst, int *work, int n_clusters, int ws_bytes, cudaStream_t st) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(n_clusters * CS, 1, 1);
     cfg.blockDim = dim3(ENG_NT, 1, 1);
-    cfg.dynamicSmemBytes = ENG_WS;
+    cfg.dynamicSmemBytes = (size_t)ws_bytes;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -618,25 +619,30 @@ int launch_engine(const HsInstance *insts, int n_inst, int *work, int n_clusters
         if (e != cudaSuccess) { hs_set_error("engine: cluster size %d not allowed: %s", CS, cudaGetErrorString(e)); return HS_ECUDA; }
     }
     {
-        cudaError_t e = engine_allow_ws<CS>();
+        cudaError_t e = engine_allow_ws<CS>(ws_bytes);
         if (e != cudaSuccess) { hs_set_error("engine: shared workspace: %s", cudaGetErrorString(e)); return HS_ECUDA; }
     }
-    cudaError_t e = cudaLaunchKernelEx(&cfg, engine_kernel<CS>, insts, n_inst, work);
+    cudaError_t e = cudaLaunchKernelEx(&cfg, engine_kernel<CS>, insts, n_inst, work, ws_bytes);
     if (e != cudaSuccess) { hs_set_error("engine launch (cluster %d x %d): %s", CS, n_clusters, cudaGetErrorString(e)); return HS_ECUDA; }
     return hs_check_launch("engine_kernel");
 }
 
 }  // namespace
 
-int hs_launch_engine(const HsInstance *insts, int n_inst, int cluster_size, int n_clusters, int *work, cudaStream_t st) {
+int hs_launch_engine(const HsInstance *insts, int n_inst, int cluster_size, int n_clusters, int *work, int ws_bytes,
+                     cudaStream_t st) {
+    if (ws_bytes < 0 || ws_bytes > ENG_WS_MAX) {
+        hs_set_error("engine: shared workspace of %d bytes outside [0, %d]", ws_bytes, ENG_WS_MAX);
+        return HS_EINVAL;
+    }
     cudaError_t e = cudaMemsetAsync(work, 0, sizeof(int), st);
     if (e != cudaSuccess) { hs_set_error("engine: work counter reset: %s", cudaGetErrorString(e)); return HS_ECUDA; }
     switch (cluster_size) {
-        case 1: return launch_engine<1>(insts, n_inst, work, n_clusters, st);
-        case 2: return launch_engine<2>(insts, n_inst, work, n_clusters, st);
-        case 4: return launch_engine<4>(insts, n_inst, work, n_clusters, st);
-        case 8: return launch_engine<8>(insts, n_inst, work, n_clusters, st);
-        case 16: return launch_engine<16>(insts, n_inst, work, n_clusters, st);
+        case 1: return launch_engine<1>(insts, n_inst, work, n_clusters, ws_bytes, st);
+        case 2: return launch_engine<2>(insts, n_inst, work, n_clusters, ws_bytes, st);
+        case 4: return launch_engine<4>(insts, n_inst, work, n_clusters, ws_bytes, st);
+        case 8: return launch_engine<8>(insts, n_inst, work, n_clusters, ws_bytes, st);
+        case 16: return launch_engine<16>(insts, n_inst, work, n_clusters, ws_bytes, st);
         default: hs_set_error("engine: cluster size must be 1, 2, 4, 8 or 16"); return HS_EINVAL;
     }
 }
@@ -645,15 +651,6 @@ int hs_engine_max_clusters_impl(int cluster_size) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(cluster_size, 1, 1);
     cfg.blockDim = dim3(ENG_NT, 1, 1);
-    cfg.dynamicSmemBytes = ENG_WS;
-    switch (cluster_size) {   // the workspace opt-in must precede the query
-        case 1: engine_allow_ws<1>(); break;
-        case 2: engine_allow_ws<2>(); break;
-        case 4: engine_allow_ws<4>(); break;
-        case 8: engine_allow_ws<8>(); break;
-        case 16: engine_allow_ws<16>(); break;
-        default: break;
-    }
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = cluster_size;

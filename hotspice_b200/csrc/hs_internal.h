@@ -59,7 +59,7 @@ int hs_square_vertex_counts_impl(const int8_t *m, int nx, int ny, int64_t *out, 
 
 int hs_segments_copy_impl(void *staged, const HsSegment *segs, int n, int to_device, cudaStream_t st);
 
-int hs_launch_engine(const HsInstance *insts, int n_inst, int cluster_size, int n_clusters, int *work,
+int hs_launch_engine(const HsInstance *insts, int n_inst, int cluster_size, int n_clusters, int *work, int ws_bytes,
                      cudaStream_t st);
 int hs_engine_max_clusters_impl(int cluster_size);
 

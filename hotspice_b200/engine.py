@@ -35,9 +35,9 @@ class HsInstance(ctypes.Structure):
 
 def _bind():
     lib = _lib.load()
-    lib.hs_engine_run.restype = ctypes.c_int
-    lib.hs_engine_run.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
-                                  ctypes.c_void_p]
+    lib.hs_engine_run_ws.restype = ctypes.c_int
+    lib.hs_engine_run_ws.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+                                     ctypes.c_int32, ctypes.c_void_p]
     lib.hs_engine_max_clusters.restype = ctypes.c_int
     lib.hs_engine_max_clusters.argtypes = [ctypes.c_int32]
     sizes = (ctypes.c_int32 * 6)()
@@ -146,6 +146,19 @@ class _Prepared:
     n: int
     cs: int
     keep: list
+    ws: int = 0         # dynamic shared workspace per CTA (bytes)
+
+
+def poisson_workspace(I: HsInstance) -> int:
+    """Shared workspace bytes that hold a Poisson-disc Metropolis instance's sampler arrays
+    (24 bytes per background-grid cell + 64; the grid has cells of side (r+1)/sqrt(2) over the
+    lattice, hotspice/poisson.py:78-83), 0 for every other instance or when they exceed the
+    largest workspace (the sampler then works in the instance's scratch)."""
+    if I.scheme != SCHEME_ID[Scheme.METROPOLIS] or I.P.sample_scheme != _lib.HS_SAMPLE_POISSON:
+        return 0
+    cs = (I.P.r_cells + 1.0) / math.sqrt(2.0)
+    need = 24 * math.ceil(I.L.nx / cs) * math.ceil(I.L.ny / cs) + 64
+    return need if need <= _lib.HS_ENGINE_WS_MAX else 0
 
 
 class CapturedRun:
@@ -271,6 +284,7 @@ class BatchEngine:
             keep += k
             groups.setdefault(cs, []).append((st * step_time(mm, cs), j, I))
         out = []
+        # the workspace only for groups with Poisson-disc instances: it takes L1 from the rest
         # largest clusters first (launched first, so the longest runs start first), and inside a
         # group the longest runs first on the work counter (longest-processing-time order)
         for cs, lst in sorted(groups.items(), reverse=True):
@@ -279,7 +293,8 @@ class BatchEngine:
             raw = np.frombuffer(bytes(arr), dtype=np.uint8)
             # pinned staging + asynchronous copy on the current stream: no host synchronisation
             t = torch.from_numpy(raw.copy()).pin_memory().to(self.device, non_blocking=True)
-            out.append(_Prepared(t, len(lst), cs, keep))
+            ws = max(poisson_workspace(I) for I in lst)
+            out.append(_Prepared(t, len(lst), cs, keep, (ws + 1023) // 1024 * 1024))
         return out
 
     def launch(self, prepared, stream=None):
@@ -300,8 +315,8 @@ class BatchEngine:
 
     def _launch_one(self, p, g, st):
         n_clusters = min(p.n, self._max(p.cs))
-        _lib.check(self.lib.hs_engine_run(p.inst.data_ptr(), p.n, p.cs, n_clusters, self._work[g:].data_ptr(), st),
-                   'hs_engine_run')
+        _lib.check(self.lib.hs_engine_run_ws(p.inst.data_ptr(), p.n, p.cs, n_clusters, self._work[g:].data_ptr(),
+                                             p.ws, st), 'hs_engine_run_ws')
 
     def resync(self):
         """Recompute every instance's incrementally updated energies from its spins

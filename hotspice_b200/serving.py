@@ -245,13 +245,14 @@ class Server:
     device time one instance's quantum aims at (from the engine's step-time model, corrected
     by the measured speed of past rounds) while requests arrive, ``tail_round_ms`` once they
     have all arrived; ``keep_state``: return the final spins; ``builders``: threads that build
-    admitted requests (host set-up overlaps the device rounds); ``resync_every``: recompute a
-    request's energies from its spins (Magnets.resync_energies) after every that many of its
-    steps (0: never), which bounds the drift of the FP32 increments; quanta are cut at those
-    points, so they fall on the same steps of a request whatever the mix."""
+    admitted requests (host set-up overlaps the device rounds; default half the host cores,
+    2 to 8); ``resync_every``: recompute a request's energies from its spins
+    (Magnets.resync_energies) after every that many of its steps (0: never), which bounds the
+    drift of the FP32 increments; quanta are cut at those points, so they fall on the same
+    steps of a request whatever the mix."""
 
     def __init__(self, device=None, hbm_budget=None, max_slots=4096, round_ms=5.0, keep_state=False,
-                 max_inflight=2, tail_round_ms=20.0, builders=2, resync_every=0):
+                 max_inflight=2, tail_round_ms=20.0, builders=None, resync_every=0):
         import torch
         from .engine import BatchEngine  # noqa: F401  (binds the engine symbols early)
         self.torch = torch
@@ -275,7 +276,11 @@ class Server:
         self.tail_round_ms = float(tail_round_ms)
         self.resync_every = int(resync_every)
         import concurrent.futures
-        self._builder = concurrent.futures.ThreadPoolExecutor(max_workers=max(1, int(builders)))
+        import os
+        if builders is None:   # building is host array work that mostly releases the GIL
+            builders = max(2, min(8, (os.cpu_count() or 4) // 2))
+        self.builders = int(builders)
+        self._builder = concurrent.futures.ThreadPoolExecutor(max_workers=max(1, self.builders))
 
     # -- one round ---------------------------------------------------------------------
     def _launch_round(self, active: list[_Active], round_ms: float):

@@ -54,6 +54,9 @@ extern "C" {
                                     budget before its stop rule held (set by the next
                                     hs_progress_arm / hs_progress_disarm)                     */
 
+/* Dynamic shared workspace of an engine CTA: hs_engine_run's size, and the largest accepted. */
+#define HS_ENGINE_WS_DEFAULT (64 * 1024)
+#define HS_ENGINE_WS_MAX (160 * 1024)
 /* Per-launch step budget of a progress() run in hs_engine_run when HsInstance.steps is 0. */
 #define HS_PROGRESS_STEPS_MAX (1 << 22)
 
@@ -330,6 +333,13 @@ int hs_segments_copy(void *staged, const HsSegment *segs, int32_t n, int32_t to_
  * once. */
 int hs_engine_run(const HsInstance *insts, int32_t n_inst, int32_t cluster_size, int32_t n_clusters,
                   int32_t *work, void *stream);
+/* hs_engine_run with an explicit dynamic shared workspace of ws_bytes per CTA (0 to
+ * HS_ENGINE_WS_MAX; hs_engine_run uses HS_ENGINE_WS_DEFAULT). A Poisson-disc Metropolis
+ * instance keeps its sampler arrays (24 * background-grid cells + 64 bytes) there when they
+ * fit, else in its scratch; the workspace takes L1 capacity from every other phase, so a
+ * launch without Poisson-disc instances passes 0. Results do not depend on ws_bytes. */
+int hs_engine_run_ws(const HsInstance *insts, int32_t n_inst, int32_t cluster_size, int32_t n_clusters,
+                     int32_t *work, int32_t ws_bytes, void *stream);
 /* Number of clusters of `cluster_size` CTAs that can be resident at once (occupancy query). */
 int hs_engine_max_clusters(int32_t cluster_size);
 

@@ -253,3 +253,33 @@ def test_server_resync():
         assert np.array_equal(alone.state, got.state), q.rid
         assert (alone.switches, alone.attempts, alone.t) == (got.switches, got.attempts, got.t)
         assert alone.E_tot == got.E_tot
+
+
+@pytest.mark.parametrize('r_cells', [4, 1])
+def test_poisson_workspace_does_not_change_results(r_cells, monkeypatch):
+    """A Poisson-disc instance gives the same state whether the engine launch keeps its
+    sampler arrays in shared memory (workspace sized by poisson_workspace) or in the
+    instance's scratch (workspace 0), and the same as the per-step kernels. At r = 1a the
+    96 x 96 background grid (68 x 68 cells, 111 KB) still fits; at r = 4a it is 28 x 28."""
+    import hotspice_b200 as hs
+    import hotspice_b200.engine as E
+    a, n = 200e-9, 96
+    g = np.random.Generator(np.random.PCG64(31))
+    spec = {'lattice': 'OOP_Square', 'a': a, 'moment': 1e-15, 'nx': n, 'ny': n, 'seed': 31, 'kw': {'PBC': True},
+            'energies': [{'type': 'dipolar', 'cutoff': 6 * a}, {'type': 'zeeman', 'B': 1e-3, 'angle': 0.0}],
+            'params': {'UPDATE_SCHEME': 'Metropolis', 'MULTISAMPLING_SCHEME': 'Poisson'}}
+    fx = {'T': 300.0, 'E_B': 5e-20 * np.ones((n, n)), 'm0': g.integers(0, 2, size=(n, n)) * 2 - 1}
+    kw = {'r': r_cells * a}
+    steps = 30
+    ref = build_product('ws_ref', spec=spec, fx=fx, engine=hs.EngineConfig(persistent=False, use_graphs=False))
+    ref.run(steps, **kw)
+    shared = build_product('ws_shared', spec=spec, fx=fx, engine=hs.EngineConfig(persistent=True))
+    prep = E.BatchEngine([shared]).run(steps, **kw)
+    assert prep[0].ws > 0, 'the sampler arrays should fit the workspace'
+    monkeypatch.setattr(E, 'poisson_workspace', lambda I: 0)
+    scratch = build_product('ws_scratch', spec=spec, fx=fx, engine=hs.EngineConfig(persistent=True))
+    prep2 = E.BatchEngine([scratch]).run(steps, **kw)
+    assert prep2[0].ws == 0
+    sr = _state(ref)
+    _assert_same(sr, _state(shared), f'r={r_cells}a shared workspace')
+    _assert_same(sr, _state(scratch), f'r={r_cells}a scratch')
