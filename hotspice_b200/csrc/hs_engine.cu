@@ -592,8 +592,10 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
 }
 
 template <int CS>
-cudaError_t engine_allow_ws(int bytes) {   // opt in to a dynamic workspace beyond 48 KB (once per size)
-    static int granted = 48 * 1024;
+cudaError_t engine_allow_ws(int bytes) {
+    // opt in to the dynamic workspace: static (about 30 KB) plus dynamic shared memory above
+    // 48 KB needs it; the largest size granted so far covers every smaller one
+    static int granted = 0;
     if (bytes <= granted) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(engine_kernel<CS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess) granted = bytes;
