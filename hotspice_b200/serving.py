@@ -235,6 +235,8 @@ class ServeStats:
     build_s: float = 0.0          # host time spent building admitted requests (summed over builders)
     last_active_s: float = 0.0    # when the last request became resident (s after the start)
     round_ms_sum: float = 0.0     # device time of the rounds (two may overlap)
+    sm_us_sum: float = 0.0        # modelled SM time of the rounds' quanta at their cluster sizes
+    sm_us_one_cta: float = 0.0    # the same quanta modelled on one CTA each
 
 
 class Server:
@@ -314,6 +316,8 @@ class Server:
         for a, s in zip(active, steps):
             a.remaining -= s
         sm_us = sum(s * t * c for s, t, c in zip(steps, times, sizes))
+        self.stats.sm_us_sum += sm_us
+        self.stats.sm_us_one_cta += sum(s * step_time(a.mm, 1) for s, a in zip(steps, active))
         return dict(prepared=prepared, e0=e0, e1=e1, members=list(active), steps=steps, sm_us=sm_us,
                     ctas=sum(sizes))
 

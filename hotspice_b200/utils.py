@@ -32,13 +32,31 @@ def lower_than(x, y, rtol=1e-10):
 
 
 def check_repetition(arr, nx: int, ny: int) -> bool:
-    """True if ``arr`` is periodic with period nx along axis 1 and ny along axis 0
-    (the property of hotspice/utils.py:42-66)."""
+    """True if ``arr`` is periodic with period nx along axis 1 and ny along axis 0: every
+    element close (numpy.allclose) to the element of the leading ny x nx block at the same
+    phase (hotspice/utils.py:42-66). The block is checked against regions that double in
+    alternating directions, y first, as there, so a wrong period is usually rejected on a
+    small region; each region takes an exact comparison before the tolerance one."""
     arr = np.asarray(arr)
     H, W = arr.shape[:2]
     base = arr[:ny, :nx, ...]
-    reps = (math.ceil(H / ny), math.ceil(W / nx)) + (1,) * (arr.ndim - 2)
-    return bool(np.allclose(np.tile(base, reps)[:H, :W, ...], arr))
+    h, w = base.shape[:2]
+    i = 0
+    while h < H or w < W:
+        if i % 2:   # columns [w, 2w) of rows [0, h)
+            y0, y1, x0, x1 = 0, min(h, H), w, min(2 * w, W)
+            w *= 2
+        else:       # rows [h, 2h) of columns [0, w)
+            y0, y1, x0, x1 = h, min(2 * h, H), 0, min(w, W)
+            h *= 2
+        i += 1
+        if y1 <= y0 or x1 <= x0:
+            continue
+        a = arr[y0:y1, x0:x1, ...]
+        b = base[np.ix_(np.arange(y0, y1) % ny, np.arange(x0, x1) % nx)]
+        if not (np.array_equal(b, a) or np.allclose(b, a)):
+            return False
+    return True
 
 
 def full_obj_name(obj) -> str:
