@@ -1013,6 +1013,7 @@ def run_served(dev, args, dist, rank, ws, sample=32):
                       sample_s=sum(meas.values()), peak_alloc=peak_alloc, build_s=srv.stats.build_s,
                       last_active=srv.stats.last_active_s, round_ms=srv.stats.round_ms_sum,
                       sm_s=srv.stats.sm_us_sum * 1e-6, sm_s_one=srv.stats.sm_us_one_cta * 1e-6,
+                      sm_s_meas=srv.stats.measured_sm_us * 1e-6,
                       n_sm=srv.n_sm,
                       finish_p90=float(np.percentile([x.finished for x in res], 90)))
     allst = [mine_stats]
@@ -1040,8 +1041,10 @@ def run_served(dev, args, dist, rank, ws, sample=32):
             "round_device_s": sum(a['round_ms'] for a in allst) * 1e-3,
             "modelled_sm_s": sum(a['sm_s'] for a in allst),
             "modelled_sm_s_one_cta": sum(a['sm_s_one'] for a in allst),
-            "sm_time_note": "modelled SM time of all quanta at the planned cluster sizes, and on one CTA each; "
-                            "/ (round_device_s x SMs) is the modelled SM use of the rounds",
+            "measured_sm_s": sum(a['sm_s_meas'] for a in allst),
+            "sm_time_note": "SM time of all quanta: planned (the step-time model scaled per request by its measured "
+                            "quanta) at the planned cluster sizes, the same on one CTA each, and measured by the engine "
+                            "(device time per quantum x CTAs); / (round_device_s x SMs) is the SM use of the rounds",
             "n_sm": allst[0]['n_sm'],
             "finish_p90_s": max(a['finish_p90'] for a in allst),
             "sequential": {"p50_s": float(np.percentile(seq, 50)), "p99_s": float(np.percentile(seq, 99)),

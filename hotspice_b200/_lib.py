@@ -109,7 +109,7 @@ SIGNATURES = {
     'hs_square_vertex_counts': (C.c_int, [P, C.c_int32, C.c_int32, P, P]),
     'hs_segments_copy': (C.c_int, [P, P, C.c_int32, C.c_int32, P]),
     'hs_engine_run': (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, P, P]),
-    'hs_engine_run_ws': (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, P, C.c_int32, P]),
+    'hs_engine_run_ws': (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, P, C.c_int32, P, P]),
     'hs_engine_max_clusters': (C.c_int, [C.c_int32]),
     'hs_exchange_energy': (C.c_int, [C.POINTER(HsLattice), P, P, P]),
     'hs_switch_energy': (C.c_int, [C.POINTER(HsLattice), P, P]),

@@ -330,11 +330,12 @@ int hs_engine_run(const HsInstance *insts, int32_t n_inst, int32_t cluster_size,
                   void *stream) {
     if (!insts || !work || n_inst < 0 || n_clusters <= 0) { hs_set_error("hs_engine_run: bad arguments"); return HS_EINVAL; }
     if (n_inst == 0) return HS_OK;
-    return hs_launch_engine(insts, n_inst, cluster_size, n_clusters, work, HS_ENGINE_WS_DEFAULT, (cudaStream_t)stream);
+    return hs_launch_engine(insts, n_inst, cluster_size, n_clusters, work, HS_ENGINE_WS_DEFAULT, nullptr,
+                            (cudaStream_t)stream);
 }
 
 int hs_engine_run_ws(const HsInstance *insts, int32_t n_inst, int32_t cluster_size, int32_t n_clusters, int32_t *work,
-                     int32_t ws_bytes, void *stream) {
+                     int32_t ws_bytes, int64_t *elapsed_ns, void *stream) {
     if (!insts || !work || n_inst < 0 || n_clusters <= 0) {
         hs_set_error("hs_engine_run_ws: bad arguments");
         return HS_EINVAL;
@@ -344,7 +345,8 @@ int hs_engine_run_ws(const HsInstance *insts, int32_t n_inst, int32_t cluster_si
         return HS_EINVAL;
     }
     if (n_inst == 0) return HS_OK;
-    return hs_launch_engine(insts, n_inst, cluster_size, n_clusters, work, ws_bytes, (cudaStream_t)stream);
+    return hs_launch_engine(insts, n_inst, cluster_size, n_clusters, work, ws_bytes,
+                            reinterpret_cast<long long *>(elapsed_ns), (cudaStream_t)stream);
 }
 
 int hs_engine_max_clusters(int32_t cluster_size) { return hs_engine_max_clusters_impl(cluster_size); }

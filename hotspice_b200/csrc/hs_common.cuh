@@ -98,6 +98,13 @@ HS_DEV int hs_sub(const HsLattice &L, int y, int x) {
 
 HS_DEV int hs_wrap(int v, int n) { v %= n; return v < 0 ? v + n : v; }
 
+// Device wall clock (PTX %globaltimer), nanoseconds.
+HS_DEV unsigned long long hs_globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // Minimum-image offset of d for period n, in [-(n/2), n - n/2 - 1].
 HS_DEV int hs_minimage(int d, int n) {
     int r = hs_wrap(d, n);

@@ -419,7 +419,7 @@ HS_DEV WolffScratch wolff_scratch_of(const HsLattice &L, void *base) {
 
 template <int CS>
 __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsInstance *insts, int n_inst, int *work,
-                                                                      int ws_bytes) {
+                                                                      int ws_bytes, long long *elapsed_ns) {
     // dynamic shared workspace (the Poisson-disc sampler's arrays), given only to launches that
     // hold Poisson-disc instances: it takes L1 capacity from the other phases
     extern __shared__ __align__(16) unsigned char s_ws[];
@@ -444,6 +444,7 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
         Sync<CS>::all();
         const int ii = s_inst;
         if (ii >= n_inst) break;
+        const unsigned long long t_claim = hs_globaltimer_ns();   // used by rank 0, thread 0
         {   // stage the instance descriptor in shared memory (read through references below)
             const unsigned long long *src = reinterpret_cast<const unsigned long long *>(insts + ii);
             unsigned long long *dst = reinterpret_cast<unsigned long long *>(&s_I);
@@ -586,6 +587,8 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
             const unsigned long long *src = reinterpret_cast<const unsigned long long *>(&s_C);
             unsigned long long *dst = reinterpret_cast<unsigned long long *>(Cg);
             for (int k = threadIdx.x; k < (int)(sizeof(HsCounters) / 8); k += blockDim.x) dst[k] = src[k];
+            // the cluster's device time on this instance in this launch
+            if (elapsed_ns && threadIdx.x == 0) elapsed_ns[ii] = (long long)(hs_globaltimer_ns() - t_claim);
         }
         __syncthreads();
     }
@@ -603,7 +606,8 @@ cudaError_t engine_allow_ws(int bytes) {
 }
 
 template <int CS>
-int launch_engine(const HsInstance *insts, int n_inst, int *work, int n_clusters, int ws_bytes, cudaStream_t st) {
+int launch_engine(const HsInstance *insts, int n_inst, int *work, int n_clusters, int ws_bytes, long long *elapsed_ns,
+                  cudaStream_t st) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(n_clusters * CS, 1, 1);
     cfg.blockDim = dim3(ENG_NT, 1, 1);
@@ -624,7 +628,7 @@ int launch_engine(const HsInstance *insts, int n_inst, int *work, int n_clusters
         cudaError_t e = engine_allow_ws<CS>(ws_bytes);
         if (e != cudaSuccess) { hs_set_error("engine: shared workspace: %s", cudaGetErrorString(e)); return HS_ECUDA; }
     }
-    cudaError_t e = cudaLaunchKernelEx(&cfg, engine_kernel<CS>, insts, n_inst, work, ws_bytes);
+    cudaError_t e = cudaLaunchKernelEx(&cfg, engine_kernel<CS>, insts, n_inst, work, ws_bytes, elapsed_ns);
     if (e != cudaSuccess) { hs_set_error("engine launch (cluster %d x %d): %s", CS, n_clusters, cudaGetErrorString(e)); return HS_ECUDA; }
     return hs_check_launch("engine_kernel");
 }
@@ -632,7 +636,7 @@ int launch_engine(const HsInstance *insts, int n_inst, int *work, int n_clusters
 }  // namespace
 
 int hs_launch_engine(const HsInstance *insts, int n_inst, int cluster_size, int n_clusters, int *work, int ws_bytes,
-                     cudaStream_t st) {
+                     long long *elapsed_ns, cudaStream_t st) {
     if (ws_bytes < 0 || ws_bytes > ENG_WS_MAX) {
         hs_set_error("engine: shared workspace of %d bytes outside [0, %d]", ws_bytes, ENG_WS_MAX);
         return HS_EINVAL;
@@ -640,11 +644,11 @@ int hs_launch_engine(const HsInstance *insts, int n_inst, int cluster_size, int 
     cudaError_t e = cudaMemsetAsync(work, 0, sizeof(int), st);
     if (e != cudaSuccess) { hs_set_error("engine: work counter reset: %s", cudaGetErrorString(e)); return HS_ECUDA; }
     switch (cluster_size) {
-        case 1: return launch_engine<1>(insts, n_inst, work, n_clusters, ws_bytes, st);
-        case 2: return launch_engine<2>(insts, n_inst, work, n_clusters, ws_bytes, st);
-        case 4: return launch_engine<4>(insts, n_inst, work, n_clusters, ws_bytes, st);
-        case 8: return launch_engine<8>(insts, n_inst, work, n_clusters, ws_bytes, st);
-        case 16: return launch_engine<16>(insts, n_inst, work, n_clusters, ws_bytes, st);
+        case 1: return launch_engine<1>(insts, n_inst, work, n_clusters, ws_bytes, elapsed_ns, st);
+        case 2: return launch_engine<2>(insts, n_inst, work, n_clusters, ws_bytes, elapsed_ns, st);
+        case 4: return launch_engine<4>(insts, n_inst, work, n_clusters, ws_bytes, elapsed_ns, st);
+        case 8: return launch_engine<8>(insts, n_inst, work, n_clusters, ws_bytes, elapsed_ns, st);
+        case 16: return launch_engine<16>(insts, n_inst, work, n_clusters, ws_bytes, elapsed_ns, st);
         default: hs_set_error("engine: cluster size must be 1, 2, 4, 8 or 16"); return HS_EINVAL;
     }
 }

@@ -81,11 +81,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
-__device__ __forceinline__ unsigned long long globaltimer_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-    return t;
-}
+__device__ __forceinline__ unsigned long long globaltimer_ns() { return hs_globaltimer_ns(); }
 
 // Parity wait bounded in wall time; returns false when it gave up or another thread aborted.
 // `backoff` makes an idle waiter sleep between polls so that it does not steal issue slots.

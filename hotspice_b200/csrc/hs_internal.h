@@ -60,7 +60,7 @@ int hs_square_vertex_counts_impl(const int8_t *m, int nx, int ny, int64_t *out, 
 int hs_segments_copy_impl(void *staged, const HsSegment *segs, int n, int to_device, cudaStream_t st);
 
 int hs_launch_engine(const HsInstance *insts, int n_inst, int cluster_size, int n_clusters, int *work, int ws_bytes,
-                     cudaStream_t st);
+                     long long *elapsed_ns, cudaStream_t st);
 int hs_engine_max_clusters_impl(int cluster_size);
 
 inline int64_t hs_align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }

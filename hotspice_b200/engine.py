@@ -37,7 +37,7 @@ def _bind():
     lib = _lib.load()
     lib.hs_engine_run_ws.restype = ctypes.c_int
     lib.hs_engine_run_ws.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
-                                     ctypes.c_int32, ctypes.c_void_p]
+                                     ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p]
     lib.hs_engine_max_clusters.restype = ctypes.c_int
     lib.hs_engine_max_clusters.argtypes = [ctypes.c_int32]
     sizes = (ctypes.c_int32 * 6)()
@@ -68,14 +68,15 @@ def step_model(mm: Magnets) -> tuple[float, float, float]:
     return 5.0, c * n ** beta, 0.5
 
 
-def _t(m, cs):
+def model_time(m, cs):
+    """Step time (us) of a step model (fixed us, cell-dependent us, alpha) on ``cs`` CTAs."""
     s0, p, alpha = m
     return s0 + (p / cs ** alpha if alpha > 0 else p) + 0.1 * (cs - 1)
 
 
 def step_time(mm: Magnets, cs: int = 1) -> float:
     """Modelled device time (us) of one step of ``mm`` on a cluster of ``cs`` CTAs."""
-    return _t(step_model(mm), cs)
+    return model_time(step_model(mm), cs)
 
 
 def step_cost(mm: Magnets) -> float:
@@ -111,7 +112,7 @@ def plan_uniform_size(models, steps, n_sm, sizes=CLUSTER_SIZES, workers=None):
     modelled run times over the clusters that fit (``workers[cs]``, the resident clusters of
     that size, else SM count / size) finishes first. One size per launch keeps clusters of
     different shapes from fragmenting the GPCs."""
-    t = _t
+    t = model_time
     best, best_t = 1, math.inf
     for cs in sizes:
         nw = workers[cs] if workers else n_sm // cs
@@ -126,7 +127,7 @@ def plan_sizes(models, steps, n_sm, max_cs=16):
     longer than the even share of the GPU (total SM time / SM count) gets twice the CTAs
     while that shortens it by at least 20%, until no run exceeds the share (or max_cs).
     ``models``: (fixed us, cell-dependent us, alpha) per instance, as step_model gives."""
-    t = _t
+    t = model_time
     cs = [1] * len(models)
     for _ in range(5):
         share = sum(st * t(m, c) * c for m, st, c in zip(models, steps, cs)) / n_sm
@@ -147,6 +148,8 @@ class _Prepared:
     cs: int
     keep: list
     ws: int = 0         # dynamic shared workspace per CTA (bytes)
+    order: list = None  # index into the engine's instance list of each launch slot
+    ns: torch.Tensor = None   # device time (ns) of each launch slot, written by the launch
 
 
 def poisson_workspace(I: HsInstance) -> int:
@@ -269,7 +272,7 @@ class BatchEngine:
                                workers={c: self._max(c) for c in CLUSTER_SIZES})
         return [cs] * len(self.magnets)
 
-    def _prepare(self, steps, kws, sizes=None):
+    def _prepare(self, steps, kws, sizes=None, costs=None):
         groups = {}
         keep = []
         tsizes = self._throughput_sizes(steps) if (self.throughput and not self.cluster_size and not sizes) else None
@@ -282,19 +285,23 @@ class BatchEngine:
                 raise ValueError(f'cluster size {cs} not in {CLUSTER_SIZES}')
             I, k = self._describe_cached(mm, st, kw)
             keep += k
-            groups.setdefault(cs, []).append((st * step_time(mm, cs), j, I))
+            cost = costs[j] if costs is not None else st * step_time(mm, cs)
+            groups.setdefault(cs, []).append((cost, j, I))
         out = []
         # the workspace only for groups with Poisson-disc instances: it takes L1 from the rest
         # largest clusters first (launched first, so the longest runs start first), and inside a
         # group the longest runs first on the work counter (longest-processing-time order)
         for cs, lst in sorted(groups.items(), reverse=True):
-            lst = [I for _, _, I in sorted(lst, key=lambda e: (-e[0], e[1]))]
+            lst = sorted(lst, key=lambda e: (-e[0], e[1]))
+            order = [j for _, j, _ in lst]
+            lst = [I for _, _, I in lst]
             arr = (HsInstance * len(lst))(*lst)
             raw = np.frombuffer(bytes(arr), dtype=np.uint8)
             # pinned staging + asynchronous copy on the current stream: no host synchronisation
             t = torch.from_numpy(raw.copy()).pin_memory().to(self.device, non_blocking=True)
             ws = max(poisson_workspace(I) for I in lst)
-            out.append(_Prepared(t, len(lst), cs, keep, (ws + 1023) // 1024 * 1024))
+            out.append(_Prepared(t, len(lst), cs, keep, (ws + 1023) // 1024 * 1024, order,
+                                 torch.zeros(len(lst), dtype=torch.int64, device=self.device)))
         return out
 
     def launch(self, prepared, stream=None):
@@ -316,7 +323,7 @@ class BatchEngine:
     def _launch_one(self, p, g, st):
         n_clusters = min(p.n, self._max(p.cs))
         _lib.check(self.lib.hs_engine_run_ws(p.inst.data_ptr(), p.n, p.cs, n_clusters, self._work[g:].data_ptr(),
-                                             p.ws, st), 'hs_engine_run_ws')
+                                             p.ws, p.ns.data_ptr(), st), 'hs_engine_run_ws')
 
     def resync(self):
         """Recompute every instance's incrementally updated energies from its spins
@@ -334,9 +341,12 @@ class BatchEngine:
             left = [r - k for r, k in zip(left, c)]
         return out
 
-    def run(self, steps, sizes=None, resync_every: int = 0, **kwargs):
+    def run(self, steps, sizes=None, resync_every: int = 0, costs=None, **kwargs):
         """Enqueue ``steps`` (an int or one int per instance) update steps of every instance
-        without the stop rule; asynchronous. ``sizes``: optional cluster size per instance.
+        without the stop rule; asynchronous. ``sizes``: optional cluster size per instance;
+        ``costs``: optional expected device time per instance, which orders the work counter
+        (longest first; default: the step-time model). Each returned group's ``ns`` holds the
+        device time of each of its instances (launch slot ``order[i]``) once the launch ends.
         ``resync_every``: recompute the energies from the spins after every that many steps
         (one engine launch per stretch; the FP64 resync that bounds the drift of the FP32
         increments)."""
@@ -344,7 +354,7 @@ class BatchEngine:
         if resync_every and resync_every > 0:
             prepared = None
             for c in self._chunks(steps, int(resync_every)):
-                prepared = self.run(c, sizes=sizes, **kwargs)
+                prepared = self.run(c, sizes=sizes, costs=costs, **kwargs)
                 for mm, k, total in zip(self.magnets, c, steps):
                     if k == int(resync_every):
                         mm.resync_energies()
@@ -356,7 +366,7 @@ class BatchEngine:
                tuple(mm._version for mm in self.magnets), tuple(id(mm) for mm in self.magnets),
                tuple(sizes) if sizes else None, self.cluster_size, self.throughput)
         if self._cache is None or self._cache[0] != key:
-            self._cache = (key, self._prepare(steps, kws, sizes))
+            self._cache = (key, self._prepare(steps, kws, sizes, costs))
         prepared = self._cache[1]
         self.launch(prepared)
         return prepared

@@ -31,7 +31,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .engine import plan_sizes, step_model, step_time
+from .engine import model_time, plan_sizes, step_model, step_time
 
 LATTICE_GEOMETRY = {
     # lattice: (a, moment) of the sweep's instances
@@ -222,6 +222,13 @@ class _Active:
     bytes: int
     event: object = None         # build finished (stream event)
     since_resync: int = 0        # steps run since the energies were last recomputed
+    ratio: float = 1.0           # measured / modelled device time of its quanta (running average)
+    measured: bool = False
+
+    def calibrated(self):
+        """The step-time model scaled by what the request's quanta measured."""
+        s0, p, alpha = self.model
+        return (s0 * self.ratio, p * self.ratio, alpha)
 
 
 @dataclass
@@ -237,6 +244,7 @@ class ServeStats:
     round_ms_sum: float = 0.0     # device time of the rounds (two may overlap)
     sm_us_sum: float = 0.0        # modelled SM time of the rounds' quanta at their cluster sizes
     sm_us_one_cta: float = 0.0    # the same quanta modelled on one CTA each
+    measured_sm_us: float = 0.0   # device time the engine measured per quantum x its CTAs
 
 
 class Server:
@@ -287,8 +295,10 @@ class Server:
     # -- one round ---------------------------------------------------------------------
     def _launch_round(self, active: list[_Active], round_ms: float):
         torch = self.torch
-        sizes = plan_sizes([a.model for a in active], [a.remaining for a in active], self.n_sm)
-        times = [step_time(a.mm, c) for a, c in zip(active, sizes)]
+        # per-request step times: the engine's model, scaled by the request's measured quanta
+        models = [a.calibrated() for a in active]
+        sizes = plan_sizes(models, [a.remaining for a in active], self.n_sm)
+        times = [model_time(m, c) for m, c in zip(models, sizes)]
         steps = plan_quanta(times, [a.remaining for a in active], self.speed * round_ms * 1e3)
         if self.resync_every > 0:   # a quantum ends at the request's next resync point
             steps = [min(s, self.resync_every - a.since_resync) for s, a in zip(steps, active)]
@@ -306,7 +316,13 @@ class Server:
                     self.stream.wait_event(a.event)
                     a.event = None
             e0.record(self.stream)
-            prepared = eng.run(steps, sizes=sizes)
+            prepared = eng.run(steps, sizes=sizes, costs=[s * t for s, t in zip(steps, times)])
+            # each quantum's device time, copied out behind the launch (read when the round ends)
+            elapsed = []
+            for p in prepared:
+                h = torch.empty(p.n, dtype=torch.int64, pin_memory=True)
+                h.copy_(p.ns, non_blocking=True)
+                elapsed.append((p.order, p.cs, h))
             for a, s in zip(active, steps):
                 a.since_resync += s
                 if self.resync_every > 0 and a.since_resync == self.resync_every:
@@ -319,7 +335,22 @@ class Server:
         self.stats.sm_us_sum += sm_us
         self.stats.sm_us_one_cta += sum(s * step_time(a.mm, 1) for s, a in zip(steps, active))
         return dict(prepared=prepared, e0=e0, e1=e1, members=list(active), steps=steps, sm_us=sm_us,
-                    ctas=sum(sizes))
+                    ctas=sum(sizes), sizes=sizes, elapsed=elapsed)
+
+    def _calibrate(self, rd):
+        """Update each member's measured/modelled ratio from the finished round's quantum
+        times (running average; the first measurement replaces the prior)."""
+        for order, cs, h in rd['elapsed']:
+            ns = h.numpy()
+            for slot, j in enumerate(order):
+                a, q = rd['members'][j], rd['steps'][j]
+                if q <= 0 or ns[slot] <= 0:
+                    continue
+                us = float(ns[slot]) * 1e-3
+                self.stats.measured_sm_us += us * cs
+                r = min(10.0, max(0.1, us / (q * model_time(a.model, cs))))
+                a.ratio = r if not a.measured else 0.5 * a.ratio + 0.5 * r
+                a.measured = True
 
     def _retire(self, a: _Active, now: float, t0: float) -> SimResult:
         mm = a.mm
@@ -416,6 +447,7 @@ class Server:
                     busy = max(1, min(self.n_sm, rd['ctas']))
                     speed = rd['sm_us'] / (ms * 1e3) / busy
                     self.speed = min(4.0, max(0.25, 0.5 * self.speed + 0.5 * speed))
+                self._calibrate(rd)
                 st.history.append((clock(), len(rd['members']), ms))
                 st.round_ms_sum += ms
                 now = time.perf_counter()

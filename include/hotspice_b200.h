@@ -337,9 +337,11 @@ int hs_engine_run(const HsInstance *insts, int32_t n_inst, int32_t cluster_size,
  * HS_ENGINE_WS_MAX; hs_engine_run uses HS_ENGINE_WS_DEFAULT). A Poisson-disc Metropolis
  * instance keeps its sampler arrays (24 * background-grid cells + 64 bytes) there when they
  * fit, else in its scratch; the workspace takes L1 capacity from every other phase, so a
- * launch without Poisson-disc instances passes 0. Results do not depend on ws_bytes. */
+ * launch without Poisson-disc instances passes 0. Results do not depend on ws_bytes.
+ * elapsed_ns (device memory, n_inst entries, or NULL): per instance of `insts`, the device
+ * wall time (ns) its cluster spent on it in this launch, from claim to counter write-back. */
 int hs_engine_run_ws(const HsInstance *insts, int32_t n_inst, int32_t cluster_size, int32_t n_clusters,
-                     int32_t *work, int32_t ws_bytes, void *stream);
+                     int32_t *work, int32_t ws_bytes, int64_t *elapsed_ns, void *stream);
 /* Number of clusters of `cluster_size` CTAs that can be resident at once (occupancy query). */
 int hs_engine_max_clusters(int32_t cluster_size);
 

@@ -283,3 +283,23 @@ def test_poisson_workspace_does_not_change_results(r_cells, monkeypatch):
     sr = _state(ref)
     _assert_same(sr, _state(shared), f'r={r_cells}a shared workspace')
     _assert_same(sr, _state(scratch), f'r={r_cells}a scratch')
+
+
+def test_engine_reports_device_time_per_instance():
+    """hs_engine_run_ws writes each instance's device time: a permutation of the instances
+    over the launch slots, every time positive, and longer runs take longer."""
+    from hotspice_b200.engine import BatchEngine
+    names = ['neel_oop16', 'metro_pin32_grid', 'neel_pin16_perp', 'metro_oop30_trunc']
+    mms = [build_product(n) for n in names]
+    eng = BatchEngine(mms, cluster_size=1)
+    prep = eng.run([40, 40, 40, 400])
+    ns = {}
+    for p in prep:
+        assert sorted(p.order) == list(range(p.n)) or len(prep) > 1
+        for slot, j in enumerate(p.order):
+            ns[j] = int(p.ns[slot].item())
+    assert sorted(ns) == list(range(len(names)))
+    assert all(v > 0 for v in ns.values()), ns
+    prep = eng.run([40, 40, 40, 4000])
+    long = {j: int(p.ns[s].item()) for p in prep for s, j in enumerate(p.order)}
+    assert long[3] > ns[3], (long[3], ns[3])
