@@ -983,7 +983,17 @@ def run_served(dev, args, dist, rank, ws, sample=32):
     res = srv.serve(mine, realtime=True)
     torch.cuda.synchronize(dev)
     peak_alloc = torch.cuda.max_memory_allocated(dev)
-    hist = np.asarray(srv.stats.history, dtype=float).reshape(-1, 3)   # (clock s, resident, round ms)
+    hist = np.asarray(srv.stats.history, dtype=float).reshape(-1, 7)
+    # (clock s, resident, round ms, measured SM-us, longest quantum us, idle ms before, host ms)
+    rounds_diag = None
+    if len(hist):
+        busy = hist[:, 2] > 0
+        rounds_diag = {
+            "sm_use_median": float(np.median(hist[busy, 3] / (hist[busy, 2] * 1e3 * srv.n_sm))),
+            "longest_quantum_over_round_median": float(np.median(hist[busy, 4] / (hist[busy, 2] * 1e3))),
+            "device_idle_between_rounds_s": float(hist[:, 5].sum() * 1e-3),
+            "host_ms_per_round_median": float(np.median(hist[:, 6])),
+            "round_ms_median": float(np.median(hist[:, 2]))}
     mid = hist[(hist[:, 0] > 0.25 * srv.stats.makespan) & (hist[:, 0] < 0.75 * srv.stats.makespan)]
     steady = float(mid[:, 1].mean()) if len(mid) else None
     # one at a time: a measured sample, the rest modelled and calibrated on it
@@ -1013,7 +1023,7 @@ def run_served(dev, args, dist, rank, ws, sample=32):
                       sample_s=sum(meas.values()), peak_alloc=peak_alloc, build_s=srv.stats.build_s,
                       last_active=srv.stats.last_active_s, round_ms=srv.stats.round_ms_sum,
                       sm_s=srv.stats.sm_us_sum * 1e-6, sm_s_one=srv.stats.sm_us_one_cta * 1e-6,
-                      sm_s_meas=srv.stats.measured_sm_us * 1e-6,
+                      sm_s_meas=srv.stats.measured_sm_us * 1e-6, rounds_diag=rounds_diag,
                       n_sm=srv.n_sm,
                       finish_p90=float(np.percentile([x.finished for x in res], 90)))
     allst = [mine_stats]
@@ -1042,6 +1052,7 @@ def run_served(dev, args, dist, rank, ws, sample=32):
             "modelled_sm_s": sum(a['sm_s'] for a in allst),
             "modelled_sm_s_one_cta": sum(a['sm_s_one'] for a in allst),
             "measured_sm_s": sum(a['sm_s_meas'] for a in allst),
+            "rounds_diag": allst[0]['rounds_diag'],
             "sm_time_note": "SM time of all quanta: planned (the step-time model scaled per request by its measured "
                             "quanta) at the planned cluster sizes, the same on one CTA each, and measured by the engine "
                             "(device time per quantum x CTAs); / (round_device_s x SMs) is the SM use of the rounds",

@@ -238,6 +238,8 @@ class ServeStats:
     max_active: int = 0
     attempts: int = 0
     admitted_bytes_peak: int = 0
+    # per round: (host clock s, resident, round device ms, measured SM-us of its quanta,
+    # longest quantum us, device idle ms before it, host ms to plan and launch it)
     history: list = field(default_factory=list)
     build_s: float = 0.0          # host time spent building admitted requests (summed over builders)
     last_active_s: float = 0.0    # when the last request became resident (s after the start)
@@ -295,6 +297,7 @@ class Server:
     # -- one round ---------------------------------------------------------------------
     def _launch_round(self, active: list[_Active], round_ms: float):
         torch = self.torch
+        th = time.perf_counter()
         # per-request step times: the engine's model, scaled by the request's measured quanta
         models = [a.calibrated() for a in active]
         sizes = plan_sizes(models, [a.remaining for a in active], self.n_sm)
@@ -335,11 +338,13 @@ class Server:
         self.stats.sm_us_sum += sm_us
         self.stats.sm_us_one_cta += sum(s * step_time(a.mm, 1) for s, a in zip(steps, active))
         return dict(prepared=prepared, e0=e0, e1=e1, members=list(active), steps=steps, sm_us=sm_us,
-                    ctas=sum(sizes), sizes=sizes, elapsed=elapsed)
+                    ctas=sum(sizes), sizes=sizes, elapsed=elapsed, host_ms=(time.perf_counter() - th) * 1e3)
 
     def _calibrate(self, rd):
         """Update each member's measured/modelled ratio from the finished round's quantum
-        times (running average; the first measurement replaces the prior)."""
+        times (running average; the first measurement replaces the prior); returns the round's
+        measured SM-us and its longest quantum (us)."""
+        sm, longest = 0.0, 0.0
         for order, cs, h in rd['elapsed']:
             ns = h.numpy()
             for slot, j in enumerate(order):
@@ -347,10 +352,13 @@ class Server:
                 if q <= 0 or ns[slot] <= 0:
                     continue
                 us = float(ns[slot]) * 1e-3
-                self.stats.measured_sm_us += us * cs
+                sm += us * cs
+                longest = max(longest, us)
                 r = min(10.0, max(0.1, us / (q * model_time(a.model, cs))))
                 a.ratio = r if not a.measured else 0.5 * a.ratio + 0.5 * r
                 a.measured = True
+        self.stats.measured_sm_us += sm
+        return sm, longest
 
     def _retire(self, a: _Active, now: float, t0: float) -> SimResult:
         mm = a.mm
@@ -384,6 +392,7 @@ class Server:
             return time.perf_counter() - t0
 
         building: list = []      # (request, footprint, future) of admitted requests being built
+        prev_end = None          # end event of the last finished round
 
         def build(r):
             # runs on the builder thread: its own stream, an event the rounds wait on
@@ -447,8 +456,10 @@ class Server:
                     busy = max(1, min(self.n_sm, rd['ctas']))
                     speed = rd['sm_us'] / (ms * 1e3) / busy
                     self.speed = min(4.0, max(0.25, 0.5 * self.speed + 0.5 * speed))
-                self._calibrate(rd)
-                st.history.append((clock(), len(rd['members']), ms))
+                sm, longest = self._calibrate(rd)
+                idle = prev_end.elapsed_time(rd['e0']) if prev_end is not None else 0.0
+                prev_end = rd['e1']
+                st.history.append((clock(), len(rd['members']), ms, sm, longest, idle, rd['host_ms']))
                 st.round_ms_sum += ms
                 now = time.perf_counter()
                 done_ids = set()
