@@ -113,6 +113,34 @@ def _ptr(t):
     return None if t is None else t.data_ptr()
 
 
+class RunSummary:
+    """What Magnets.summary_async copied out: pinned host buffers filled by the stream,
+    readable once the event has completed."""
+
+    def __init__(self, mm, host, divs, event):
+        self._mm, self._host, self._divs, self.event = mm, host, divs, event
+
+    def ready(self) -> bool:
+        return self.event.query()
+
+    def result(self) -> dict:
+        """counters (record), E_tot, m_avg and state (int8 spins or None); raises when an
+        enqueued recompute reported a status, like Magnets.check_resync."""
+        self.event.synchronize()
+        h = self._host
+        if 'status' in h:
+            for st in h['status'].tolist():
+                if st:
+                    raise RuntimeError(f'hs_dipolar_full_igemm reported status {st} '
+                                       f'(1: wait timed out, 2: moment not uniform)')
+        vals = h['scal'].tolist()
+        ne = len(self._divs)
+        rec = np.frombuffer(h['counters'].numpy().tobytes(), dtype=_lib.COUNTERS_DTYPE)[0]
+        return dict(counters=rec, E_tot=float(sum(v / d for v, d in zip(vals[:ne], self._divs))),
+                    m_avg=self._mm._m_avg_from(vals[ne:]),
+                    state=h['state'].numpy().copy() if 'state' in h else None)
+
+
 class Magnets(ABC):
     """hotspice/core.py:56-980. See the module docstring for what runs where."""
 
@@ -596,21 +624,61 @@ class Magnets(ABC):
         return torch.minimum(b1, b2) if min_only else (b1, b2)
 
     # observables ----------------------------------------------------------------------
+    def _m_means(self) -> list:
+        """Device scalars behind the magnetisation averages: the means of m ox and m oy for
+        in-plane lattices, of m otherwise."""
+        if self.in_plane:
+            o = self._orient64()
+            return [torch.mean(self.m * o[:, :, 0]), torch.mean(self.m * o[:, :, 1])]
+        return [torch.mean(self.m)]
+
+    def _m_avg_from(self, means) -> float:
+        if not self.in_plane:
+            return float(means[0])
+        mx = float(means[0]) * self.nx * self.ny / self.n
+        my = float(means[1]) * self.nx * self.ny / self.n
+        return (mx ** 2 + my ** 2) ** 0.5
+
     @property
     def m_avg_x(self) -> float:
         if not self.in_plane:
             return 0
-        return float(torch.mean(self.m * torch.as_tensor(self.orientation[:, :, 0], device=self.device))) * self.nx * self.ny / self.n
+        return float(self._m_means()[0]) * self.nx * self.ny / self.n
 
     @property
     def m_avg_y(self) -> float:
         if not self.in_plane:
             return 0
-        return float(torch.mean(self.m * torch.as_tensor(self.orientation[:, :, 1], device=self.device))) * self.nx * self.ny / self.n
+        return float(self._m_means()[1]) * self.nx * self.ny / self.n
 
     @property
     def m_avg(self) -> float:
-        return (self.m_avg_x ** 2 + self.m_avg_y ** 2) ** 0.5 if self.in_plane else float(torch.mean(self.m))
+        return self._m_avg_from(self._m_means())
+
+    def summary_async(self, keep_state: bool = False) -> 'RunSummary':
+        """Enqueue on the current stream what a finished run's summary reads: the counters,
+        the energy sums behind E_tot, the magnetisation means behind m_avg, the status words of
+        enqueued recomputes, and the spins when ``keep_state``; all copied into pinned host
+        memory. The host does not wait: RunSummary.ready() polls, result() gives the values
+        (equal to the synchronous properties')."""
+        torch_ = torch
+        parts = [e.E_sum() for e in self._energies] + self._m_means()
+        scal = torch_.stack([p.to(torch_.float64) for p in parts])
+        pend, self._pending_status = getattr(self, '_pending_status', []), []
+        host = {'scal': torch_.empty(scal.shape, dtype=torch_.float64, pin_memory=True),
+                'counters': torch_.empty(self._counters.shape, dtype=self._counters.dtype, pin_memory=True)}
+        host['scal'].copy_(scal, non_blocking=True)
+        host['counters'].copy_(self._counters, non_blocking=True)
+        if pend:
+            st = torch_.stack([buf[n - 256:n - 252].view(torch_.int32)[0] for buf, n in pend])
+            host['status'] = torch_.empty(st.shape, dtype=torch_.int32, pin_memory=True)
+            host['status'].copy_(st, non_blocking=True)
+        if keep_state:
+            host['state'] = torch_.empty(self._m_dev.shape, dtype=self._m_dev.dtype, pin_memory=True)
+            host['state'].copy_(self._m_dev, non_blocking=True)
+        ev = torch_.cuda.Event()
+        ev.record(torch_.cuda.current_stream(self.device))
+        return RunSummary(self, host, [e.E_div for e in self._energies], ev)
 
     @property
     def m_avg_angle(self) -> float:

@@ -55,9 +55,15 @@ class Energy:
     def update_multiple(self, indices2D):
         raise NotImplementedError
 
+    E_div = 1   # E_tot = E_sum() / E_div (2 for pair energies, counted once per pair)
+
+    def E_sum(self) -> torch.Tensor:
+        """The sum behind E_tot as a 0-d device tensor (read later without a host sync)."""
+        raise NotImplementedError
+
     @property
     def E_tot(self):
-        raise NotImplementedError
+        return float(self.E_sum()) / self.E_div
 
     @cached_property
     def shortname(self):
@@ -121,9 +127,8 @@ class ZeemanEnergy(Energy):
             return torch.zeros_like(self.E_factor)
         return self.mm._m_dev.double() * self.E_factor_perp
 
-    @property
-    def E_tot(self):
-        return float(torch.sum(self.E))
+    def E_sum(self):
+        return torch.sum(self.E)
 
     def set_field_device(self, magnitude: float, pattern: torch.Tensor | None = None, angle: float | None = None):
         """set_field(magnitude * pattern, angle) computed on the device into the existing
@@ -262,9 +267,10 @@ class DipolarEnergy(Energy):
             return torch.zeros_like(self._E, dtype=torch.float64)
         return self._Ep.clone()
 
-    @property
-    def E_tot(self):
-        return float(torch.sum(self._E)) / 2
+    E_div = 2
+
+    def E_sum(self):
+        return torch.sum(self._E)
 
     def get_NN_interaction(self):
         """Largest nearest-neighbour kernel magnitude times prefactor * <moment>^2
@@ -434,6 +440,7 @@ class ExchangeEnergy(Energy):
             return torch.zeros_like(E, dtype=torch.float64)
         return Ep.double()
 
-    @property
-    def E_tot(self):
-        return float(torch.sum(self.E)) / 2
+    E_div = 2
+
+    def E_sum(self):
+        return torch.sum(self.E)

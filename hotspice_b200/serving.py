@@ -254,9 +254,10 @@ class Server:
 
     ``hbm_budget``: device bytes the resident instances may hold (default: half of the free
     memory when the server starts); ``max_slots``: resident instances at most; ``round_ms``:
-    device time one instance's quantum aims at (from the engine's step-time model, corrected
-    by the measured speed of past rounds) while requests arrive, ``tail_round_ms`` once they
-    have all arrived; ``keep_state``: return the final spins; ``builders``: threads that build
+    device time one instance's quantum aims at (the engine's step-time model, scaled per request
+    by the device time its past quanta measured; longer when the host's planning of a round
+    would outlast the round) while requests arrive, ``tail_round_ms`` once they have all
+    arrived; ``keep_state``: return the final spins; ``builders``: threads that build
     admitted requests (host set-up overlaps the device rounds; default half the host cores,
     2 to 8); ``resync_every``: recompute a request's energies from its spins
     (Magnets.resync_energies) after every that many of its steps (0: never), which bounds the
@@ -280,8 +281,9 @@ class Server:
         self.keep_state = keep_state
         self.max_inflight = max(1, int(max_inflight))
         self.n_sm = torch.cuda.get_device_properties(self.device).multi_processor_count
-        self.speed = 1.0              # modelled device-us per measured us; refined from measured rounds
+        self.host_us = 0.0            # host time to plan and launch a round (running average)
         self.stream = torch.cuda.Stream(self.device)
+        self.retire_stream = torch.cuda.Stream(self.device)
         self.build_stream = torch.cuda.Stream(self.device)
         self.stats = ServeStats()
         self._engine = None
@@ -302,7 +304,13 @@ class Server:
         models = [a.calibrated() for a in active]
         sizes = plan_sizes(models, [a.remaining for a in active], self.n_sm)
         times = [model_time(m, c) for m, c in zip(models, sizes)]
-        steps = plan_quanta(times, [a.remaining for a in active], self.speed * round_ms * 1e3)
+        rem = [a.remaining for a in active]
+        steps = plan_quanta(times, rem, round_ms * 1e3)
+        # two rounds stay in flight, so a round's device time should cover the host's planning
+        # of the next one: lengthen the quanta (up to 8x) when the resident set is too small
+        dev_us = sum(s * t * c for s, t, c in zip(steps, times, sizes)) / self.n_sm
+        if dev_us < 2.0 * self.host_us:
+            steps = plan_quanta(times, rem, round_ms * 1e3 * min(8.0, 2.0 * self.host_us / max(dev_us, 1.0)))
         if self.resync_every > 0:   # a quantum ends at the request's next resync point
             steps = [min(s, self.resync_every - a.since_resync) for s, a in zip(steps, active)]
         if self._engine is None:
@@ -338,7 +346,12 @@ class Server:
         self.stats.sm_us_sum += sm_us
         self.stats.sm_us_one_cta += sum(s * step_time(a.mm, 1) for s, a in zip(steps, active))
         return dict(prepared=prepared, e0=e0, e1=e1, members=list(active), steps=steps, sm_us=sm_us,
-                    ctas=sum(sizes), sizes=sizes, elapsed=elapsed, host_ms=(time.perf_counter() - th) * 1e3)
+                    ctas=sum(sizes), sizes=sizes, elapsed=elapsed, host_ms=self._host_time(th))
+
+    def _host_time(self, th):
+        ms = (time.perf_counter() - th) * 1e3
+        self.host_us = ms * 1e3 if self.host_us == 0.0 else 0.7 * self.host_us + 0.3 * ms * 1e3
+        return ms
 
     def _calibrate(self, rd):
         """Update each member's measured/modelled ratio from the finished round's quantum
@@ -360,19 +373,23 @@ class Server:
         self.stats.measured_sm_us += sm
         return sm, longest
 
-    def _retire(self, a: _Active, now: float, t0: float) -> SimResult:
-        mm = a.mm
-        with self.torch.cuda.stream(self.stream):
-            mm.check_resync()
-            c = mm._read_counters()
-            res = SimResult(rid=a.req.rid, steps=a.req.steps, arrival=a.req.arrival, admitted=a.admitted - t0,
-                            finished=now - t0, switches=int(c['switches']), attempts=int(c['attempted']),
-                            t=float(c['t']), E_tot=float(mm.E_tot), m_avg=float(mm.m_avg),
-                            state=mm._m_dev.cpu().numpy().copy() if self.keep_state else None)
-            st = int(c['status'])
+    def _retire_begin(self, a: _Active, end_event):
+        """Enqueue the summary of a finished request on the retire stream, behind the round
+        that finished it: its copies and small reductions run while the next round does (the
+        host does not wait on the round stream, which already holds the next round)."""
+        self.retire_stream.wait_event(end_event)
+        with self.torch.cuda.stream(self.retire_stream):
+            return a, a.mm.summary_async(keep_state=self.keep_state)
+
+    def _retire_end(self, a: _Active, summary, now: float, t0: float) -> SimResult:
+        r = summary.result()
+        c = r['counters']
+        st = int(c['status'])
         if st:
             raise RuntimeError(f'request {a.req.rid}: device step reported status {st} (HS_ST_* bits)')
-        return res
+        return SimResult(rid=a.req.rid, steps=a.req.steps, arrival=a.req.arrival, admitted=a.admitted - t0,
+                         finished=now - t0, switches=int(c['switches']), attempts=int(c['attempted']),
+                         t=float(c['t']), E_tot=r['E_tot'], m_avg=r['m_avg'], state=r['state'])
 
     # -- the loop ----------------------------------------------------------------------
     def serve(self, requests, realtime=True) -> list[SimResult]:
@@ -392,7 +409,22 @@ class Server:
             return time.perf_counter() - t0
 
         building: list = []      # (request, footprint, future) of admitted requests being built
+        retiring: list = []      # (active record, RunSummary) of finished requests being read out
         prev_end = None          # end event of the last finished round
+
+        def collect():
+            """Turn the read-outs that have landed into results."""
+            if not retiring:
+                return
+            now = time.perf_counter()
+            still = []
+            for a, sm in retiring:
+                if sm.ready():
+                    results.append(self._retire_end(a, sm, now, t0))
+                    st.attempts += results[-1].attempts
+                else:
+                    still.append((a, sm))
+            retiring[:] = still
 
         def build(r):
             # runs on the builder thread: its own stream, an event the rounds wait on
@@ -400,6 +432,8 @@ class Server:
             torch.cuda.set_device(self.device)
             with torch.cuda.stream(self.build_stream):
                 mm = build_magnets(r.spec, device=self.device)
+                if mm.in_plane:
+                    mm._orient64()   # device orientation for the read-out of m_avg
                 ev = torch.cuda.Event()
                 ev.record(self.build_stream)
             st.build_s += time.perf_counter() - tb
@@ -414,7 +448,8 @@ class Server:
                 queue.push(pending.popleft())
             changed = False
             if queue:
-                reserved = sum(a.bytes for a in active) + sum(b for _, b, _ in building)
+                reserved = sum(a.bytes for a in active) + sum(b for _, b, _ in building) + \
+                    sum(a.bytes for a, _ in retiring)
                 new = queue.admit(self.hbm_budget - reserved, self.max_slots - len(active) - len(building))
                 for r in new:
                     building.append((r, footprint_bytes(r.spec), self._builder.submit(build, r)))
@@ -432,8 +467,9 @@ class Server:
             st.admitted_bytes_peak = max(st.admitted_bytes_peak, used_bytes)
             return changed
 
-        while pending or queue or active or inflight or building:
+        while pending or queue or active or inflight or building or retiring:
             admit()
+            collect()
             runnable = [a for a in active if a.remaining > 0]
             if runnable and len(inflight) < self.max_inflight:
                 # short rounds while requests still arrive (they join at round boundaries),
@@ -447,29 +483,27 @@ class Server:
                 rd = inflight[0]
                 # overlap: activate newly built requests while the oldest round runs
                 while not rd['e1'].query():
+                    collect()
                     if not admit():
                         time.sleep(50e-6)
                 rd['e1'].synchronize()
                 inflight.popleft()
                 ms = rd['e0'].elapsed_time(rd['e1'])
-                if ms > 0.05:
-                    busy = max(1, min(self.n_sm, rd['ctas']))
-                    speed = rd['sm_us'] / (ms * 1e3) / busy
-                    self.speed = min(4.0, max(0.25, 0.5 * self.speed + 0.5 * speed))
                 sm, longest = self._calibrate(rd)
                 idle = prev_end.elapsed_time(rd['e0']) if prev_end is not None else 0.0
                 prev_end = rd['e1']
                 st.history.append((clock(), len(rd['members']), ms, sm, longest, idle, rd['host_ms']))
                 st.round_ms_sum += ms
-                now = time.perf_counter()
                 done_ids = set()
                 for a in rd['members']:
                     if a.remaining <= 0 and not any(a is m for r2 in inflight for m in r2['members']):
-                        results.append(self._retire(a, now, t0))
-                        st.attempts += results[-1].attempts
+                        retiring.append(self._retire_begin(a, rd['e1']))
                         done_ids.add(id(a))
                 if done_ids:
                     active[:] = [a for a in active if id(a) not in done_ids]
+                continue
+            if retiring and not building:
+                retiring[0][1].event.synchronize()
                 continue
             if building:
                 for _, _, fut in building:
