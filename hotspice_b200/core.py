@@ -30,7 +30,7 @@ import torch
 
 from . import _lib, config
 from .energies import DiMonopolarEnergy, DipolarEnergy, Energy, ExchangeEnergy, ZeemanEnergy
-from .utils import as_2D_array, check_repetition, full_obj_name, lower_than
+from .utils import as_2D_array, check_repetition, copy_to_device, full_obj_name, lower_than, to_device
 
 __all__ = ['kB', 'SimParams', 'Magnets', 'Scheme', 'EngineConfig', 'Unitcell']
 
@@ -184,12 +184,12 @@ class Magnets(ABC):
         self.PBC = PBC
         # device state
         dev = self.device
-        self._occ_dev = torch.as_tensor(self.occupation, device=dev, dtype=torch.int8).contiguous()
-        self._nonzero_dev = torch.as_tensor(np.flatnonzero(self.occupation), device=dev, dtype=torch.int32)
+        self._occ_dev = to_device(self.occupation, dev, torch.int8)
+        self._nonzero_dev = to_device(np.flatnonzero(self.occupation), dev, torch.int32)
         self._m_dev = torch.zeros((self.ny, self.nx), device=dev, dtype=torch.int8)
         self._mm_dev = torch.zeros((self.ny, self.nx), device=dev, dtype=torch.float32)
         self._counters = torch.zeros(ctypes.sizeof(_lib.HsCounters), device=dev, dtype=torch.uint8)
-        self._orient_dev = torch.as_tensor(self.orientation, device=dev, dtype=torch.float32).contiguous() if self.in_plane else None
+        self._orient_dev = to_device(self.orientation, dev, torch.float32) if self.in_plane else None
         self._moment_np = np.ones((self.ny, self.nx))
         self._mom_dev = torch.ones((self.ny, self.nx), device=dev, dtype=torch.float32)
         self.initialize_m(self._get_groundstate() if pattern is None else pattern, update_energy=False)
@@ -324,7 +324,7 @@ class Magnets(ABC):
 
     def _set_m_array(self, arr):
         arr = np.sign(np.asarray(arr, dtype=float))
-        self._m_dev.copy_(torch.as_tensor(arr, dtype=torch.int8))
+        copy_to_device(self._m_dev, arr)
         self._mm_dev.copy_(self._m_dev.float() * self._mom_dev)
 
     def initialize_m(self, pattern='random', *, angle: float = 0, update_energy: bool = True):
@@ -397,7 +397,7 @@ class Magnets(ABC):
         bu = self.beta[occ] if occ.any() else self.beta.reshape(-1)
         self._beta_uniform = float(bu[0]) if (np.all(bu == bu[0]) and np.isfinite(bu[0])) else 0.0
         b = np.where(np.isfinite(self.beta), self.beta, 0.0)
-        self._beta_dev = torch.as_tensor(b, device=self.device, dtype=torch.float32).contiguous()
+        self._beta_dev = to_device(b, self.device, torch.float32)
         if hasattr(self, '_version'):
             self._state_changed()
 
@@ -415,7 +415,7 @@ class Magnets(ABC):
     @E_B.setter
     def E_B(self, value):
         self._EB_np = as_2D_array(value, self.shape)
-        self._EB_dev = torch.as_tensor(self._EB_np, device=self.device, dtype=torch.float32).contiguous()
+        self._EB_dev = to_device(self._EB_np, self.device, torch.float32)
         self._state_changed()
 
     @property
@@ -426,7 +426,7 @@ class Magnets(ABC):
     def moment(self, value):
         self._moment_np = as_2D_array(value, self.shape)
         self._momentSq = self._moment_np * self._moment_np
-        self._mom_dev = torch.as_tensor(self._moment_np, device=self.device, dtype=torch.float32).contiguous()
+        self._mom_dev = to_device(self._moment_np, self.device, torch.float32)
         self._mm_dev.copy_(self._m_dev.float() * self._mom_dev)
         for e in self._energies:
             if isinstance(e, ZeemanEnergy):
@@ -767,7 +767,7 @@ class Magnets(ABC):
                     counts = np.arange(25, dtype=float)
                     kbt = np.full(25, kB * float(self._T_np[self.occupation.astype(bool)][0]))
                     bond = 1 - np.exp(-2 * e.J / kbt * counts)
-                    self._bond_dev = torch.as_tensor(bond, device=self.device, dtype=torch.float64)
+                    self._bond_dev = to_device(bond, self.device, torch.float64)
                     L.wolff_bond = self._bond_dev.data_ptr()
         if not override:
             self._L = L
@@ -1101,14 +1101,14 @@ class Magnets(ABC):
         """FP64 device copy of the moment (the Zeeman factors are formed from it on the device)."""
         c = getattr(self, '_mom64_cache', None)
         if c is None or c[0] is not self._moment_np:
-            c = (self._moment_np, torch.as_tensor(self._moment_np, device=self.device, dtype=torch.float64).contiguous())
+            c = (self._moment_np, to_device(self._moment_np, self.device, torch.float64))
             self._mom64_cache = c
         return c[1]
 
     def _orient64(self):
         c = getattr(self, '_ori64_cache', None)
         if c is None or c[0] is not self.orientation:
-            c = (self.orientation, torch.as_tensor(self.orientation, device=self.device, dtype=torch.float64).contiguous())
+            c = (self.orientation, to_device(self.orientation, self.device, torch.float64))
             self._ori64_cache = c
         return c[1]
 

@@ -22,6 +22,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from .utils import copy_to_device, to_device
 from .kernels import build_dimonopolar_kernels, build_kernels
 
 
@@ -102,8 +103,8 @@ class ZeemanEnergy(Energy):
         else:
             ef = -mom * mag
             efp = np.zeros_like(ef)
-        self.E_factor = torch.as_tensor(ef, device=mm.device, dtype=torch.float64)
-        self.E_factor_perp = torch.as_tensor(efp, device=mm.device, dtype=torch.float64)
+        self.E_factor = to_device(ef, mm.device, torch.float64)
+        self.E_factor_perp = to_device(efp, mm.device, torch.float64)
         self._ef32 = self.E_factor.float().contiguous()
         self._efp32 = self.E_factor_perp.float().contiguous()
         mm._state_changed()
@@ -227,10 +228,10 @@ class DipolarEnergy(Energy):
         mm = self.mm
         self.kernel_set = ks
         dev = mm.device
-        self._K = torch.as_tensor(ks.K, device=dev, dtype=torch.float32).contiguous()
-        self._Kpo = torch.as_tensor(ks.Kpo, device=dev, dtype=torch.float32).contiguous() if mm.in_plane else None
-        self._Kps = torch.as_tensor(ks.Kps, device=dev, dtype=torch.float32).contiguous() if mm.in_plane else None
-        self._sub_of = torch.as_tensor(ks.sub_of.reshape(-1), device=dev, dtype=torch.int32)
+        self._K = to_device(ks.K, dev, torch.float32)
+        self._Kpo = to_device(ks.Kpo, dev, torch.float32) if mm.in_plane else None
+        self._Kps = to_device(ks.Kps, dev, torch.float32) if mm.in_plane else None
+        self._sub_of = to_device(ks.sub_of.reshape(-1), dev, torch.int32)
         self.kernel_unitcell_indices = ks.sub_of
         # FP64 accumulators of the FP32 per-switch increments (see hs_dipolar.cu)
         self._E = torch.zeros((mm.ny, mm.nx), device=dev, dtype=torch.float64)
@@ -349,10 +350,10 @@ class DiMonopolarEnergy(DipolarEnergy):
         ks = self._scaled(self._K_phys, self._charge_sq / mu ** 2)
         self.kernel_set = ks
         dev = self.mm.device
-        self._K.copy_(torch.as_tensor(ks.K, device=dev, dtype=torch.float32))
+        copy_to_device(self._K, ks.K)
         if self._Kpo is not None:
-            self._Kpo.copy_(torch.as_tensor(ks.Kpo, device=dev, dtype=torch.float32))
-            self._Kps.copy_(torch.as_tensor(ks.Kps, device=dev, dtype=torch.float32))
+            copy_to_device(self._Kpo, ks.Kpo)
+            copy_to_device(self._Kps, ks.Kps)
         self._mu_kernels = mu
         self.mm._state_changed()
 

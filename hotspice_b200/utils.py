@@ -59,6 +59,29 @@ def check_repetition(arr, nx: int, ny: int) -> bool:
     return True
 
 
+_NP_OF = {torch.int8: np.int8, torch.int32: np.int32, torch.int64: np.int64, torch.float32: np.float32,
+          torch.float64: np.float64, torch.uint8: np.uint8}
+
+
+def to_device(arr, device, dtype: torch.dtype | None = None) -> torch.Tensor:
+    """A new contiguous device tensor holding ``arr`` (cast to ``dtype`` on the host), copied
+    from a pinned staging buffer asynchronously on the current stream: the host does not wait
+    for the stream, as it does for a copy from pageable memory. Same values as
+    torch.as_tensor(arr, device=device, dtype=dtype)."""
+    a = np.asarray(arr)
+    if dtype is not None:
+        a = a.astype(_NP_OF[dtype], copy=False)
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    return t.pin_memory().to(device, non_blocking=True)
+
+
+def copy_to_device(dst: torch.Tensor, arr) -> torch.Tensor:
+    """dst.copy_(arr) from a pinned staging buffer, asynchronously on the current stream."""
+    a = np.ascontiguousarray(np.asarray(arr).astype(_NP_OF[dst.dtype], copy=False))
+    dst.copy_(torch.from_numpy(a).pin_memory().reshape(dst.shape), non_blocking=True)
+    return dst
+
+
 def full_obj_name(obj) -> str:
     cls = type(obj)
     return f'{cls.__module__}.{cls.__qualname__}'

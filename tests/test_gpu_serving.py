@@ -73,3 +73,25 @@ def test_request_too_large_for_budget_raises():
     r = _requests()[0]
     with pytest.raises(RuntimeError, match='HBM budget'):
         S.Server(hbm_budget=1024).serve([r], realtime=False)
+
+
+def test_building_a_request_does_not_synchronise():
+    """A request's Magnets is built without the host waiting on the device (pinned
+    asynchronous uploads, no read-backs), so the server's builder threads never stall behind
+    the engine rounds that hold the SMs."""
+    import torch
+    specs = [dict(lattice='OOP_Square', n=70, T=300.0, B=1e-3, angle=0.3, scheme='Neel', seed=201),
+             dict(lattice='IP_Pinwheel', n=64, T=250.0, B=2e-3, angle=1.1, scheme='Metropolis', seed=202),
+             dict(lattice='IP_Kagome', n=66, T=350.0, B=0.0, angle=0.0, scheme='Neel', seed=203),
+             dict(lattice='Ising_Square', n=48, T=180.0, seed=204, J=1e-21)]
+    for s in specs:
+        S.build_magnets(s)          # first build of each kind: library load, lazy set-up
+    torch.cuda.synchronize()
+    torch.cuda.set_sync_debug_mode('error')
+    try:
+        built = [S.build_magnets(dict(s, seed=s['seed'] + 10)) for s in specs]
+    finally:
+        torch.cuda.set_sync_debug_mode('default')
+    torch.cuda.synchronize()
+    for mm in built:   # and the instances are complete: a summary reads back normally
+        assert np.isfinite(mm.E_tot)
