@@ -185,13 +185,23 @@ class AdmissionQueue:
         return out
 
 
-def plan_quanta(times, remaining, round_us):
-    """Steps each active instance runs in the next round: about ``round_us`` of modelled
-    device time (``times``: modelled time of one step of each instance on its cluster), at
-    least one step, at most what remains of its budget."""
+def plan_quanta(times, remaining, round_us, sizes=None, n_sm=None):
+    """Steps each active instance runs in the next round: about ``round_us`` of device time
+    (``times``: time of one step of each instance on its cluster), at least one step, at most
+    what remains of its budget. With the cluster ``sizes`` and the SM count, an instance whose
+    remaining run is longer than the time the resident work needs to drain (its total
+    remaining SM time / SMs) gets a quantum longer in proportion, up to the length of the
+    round, so that the longest requests do not end alone on an otherwise idle GPU."""
+    targets = [round_us] * len(times)
+    if sizes is not None and n_sm:
+        rem_us = [r * t for r, t in zip(remaining, times)]
+        drain = sum(x * c for x, c in zip(rem_us, sizes)) / n_sm
+        W = max(round_us, sum(min(round_us, x) * c for x, c in zip(rem_us, sizes)) / n_sm)
+        if drain > 0:
+            targets = [min(W, max(round_us, W * x / drain)) for x in rem_us]
     out = []
-    for t, r in zip(times, remaining):
-        q = max(1, int(round_us // max(t, 1e-9)))
+    for t, r, u in zip(times, remaining, targets):
+        q = max(1, int(u // max(t, 1e-9)))
         out.append(int(min(q, r)))
     return out
 
@@ -305,12 +315,13 @@ class Server:
         sizes = plan_sizes(models, [a.remaining for a in active], self.n_sm)
         times = [model_time(m, c) for m, c in zip(models, sizes)]
         rem = [a.remaining for a in active]
-        steps = plan_quanta(times, rem, round_ms * 1e3)
+        steps = plan_quanta(times, rem, round_ms * 1e3, sizes, self.n_sm)
         # two rounds stay in flight, so a round's device time should cover the host's planning
         # of the next one: lengthen the quanta (up to 8x) when the resident set is too small
         dev_us = sum(s * t * c for s, t, c in zip(steps, times, sizes)) / self.n_sm
         if dev_us < 2.0 * self.host_us:
-            steps = plan_quanta(times, rem, round_ms * 1e3 * min(8.0, 2.0 * self.host_us / max(dev_us, 1.0)))
+            steps = plan_quanta(times, rem, round_ms * 1e3 * min(8.0, 2.0 * self.host_us / max(dev_us, 1.0)),
+                                sizes, self.n_sm)
         if self.resync_every > 0:   # a quantum ends at the request's next resync point
             steps = [min(s, self.resync_every - a.since_resync) for s, a in zip(steps, active)]
         if self._engine is None:

@@ -69,6 +69,23 @@ def test_plan_quanta():
     assert steps == [50, 10, 1]                    # capped by what remains; at least one step
 
 
+def test_plan_quanta_lengthens_the_critical_runs():
+    # 300 short runs and one long one on 148 SMs: the long run's remaining 2 s exceed the drain
+    # time of the resident work, so its quantum grows in proportion, up to the round's length
+    times = [10.0] * 300 + [100.0]
+    remaining = [400] * 300 + [20000]
+    sizes = [1] * 300 + [16]
+    steps = S.plan_quanta(times, remaining, 1000.0, sizes, 148)
+    assert steps[:300] == [100] * 300              # round_us / 10 us
+    rem_us = [r * t for r, t in zip(remaining, times)]
+    drain = sum(x * c for x, c in zip(rem_us, sizes)) / 148
+    W = max(1000.0, sum(min(1000.0, x) * c for x, c in zip(rem_us, sizes)) / 148)
+    assert steps[300] == int(min(W, W * rem_us[300] / drain) // 100.0)
+    assert 10 < steps[300] <= W / 100.0 + 1
+    # without the sizes, every run gets the plain quantum
+    assert S.plan_quanta(times, remaining, 1000.0)[300] == 10
+
+
 def test_plan_sizes():
     from hotspice_b200.engine import plan_sizes, plan_uniform_size, lpt_makespan
     neel_big = (9.0, 600.0, 0.62)                   # ~500^2-cell Néel lattice
