@@ -92,8 +92,13 @@ HS_HD inline double hs_poisson_grid_cells(const HsLattice &L, const HsGridPlan &
 // ---------------------------------------------------------------------------------------
 // Lattice helpers
 // ---------------------------------------------------------------------------------------
+// Sublattice of cell (y, x), both >= 0; -1 for a unit-cell site without a magnet. Unit cells
+// whose sides are powers of two (1, 2 and 4 cells for every lattice here) take masks instead of
+// integer divisions (the same remainders for non-negative coordinates).
 HS_DEV int hs_sub(const HsLattice &L, int y, int x) {
-    return L.sub_of[(y % L.uy) * L.ux + (x % L.ux)];
+    const int ry = (L.uy & (L.uy - 1)) == 0 ? (y & (L.uy - 1)) : y % L.uy;
+    const int rx = (L.ux & (L.ux - 1)) == 0 ? (x & (L.ux - 1)) : x % L.ux;
+    return L.sub_of[ry * L.ux + rx];
 }
 
 HS_DEV int hs_wrap(int v, int n) { v %= n; return v < 0 ? v + n : v; }

@@ -113,8 +113,10 @@ HS_DEV int stage_switches(const HsLattice &L, const HsSwitchList &sw, int nsw, S
     return n;
 }
 
-// Contributions of staged switch w to the 4 cells x0..x0+3 of `row`.
-HS_DEV void contrib4(const HsLattice &L, const SwX &w, int row, int x0, float acc[4], float accp[4], bool neg[4]) {
+// Contributions of staged switch w to the 4 cells x0..x0+3 of `row`; tch[v] is set for every
+// cell inside the switch's window.
+HS_DEV void contrib4(const HsLattice &L, const SwX &w, int row, int x0, float acc[4], float accp[4], bool neg[4],
+                     bool tch[4]) {
     if (!w.mode && !L.dip_wrap) {
         // exact window without wrapping: one kernel row, consecutive columns
         const int dy = row - w.y;
@@ -125,6 +127,7 @@ HS_DEV void contrib4(const HsLattice &L, const SwX &w, int row, int x0, float ac
         for (int v = 0; v < 4; ++v) {
             const int x = x0 + v, dx = x - w.x;
             if (x < L.nx && dx >= -L.dip_wx && dx <= L.dip_wx) {
+                tch[v] = true;
                 acc[v] += w.mm * __ldg(L.K + base + x);
                 if (L.use_perp) accp[v] += w.mm * __ldg(L.Kpo + base + x);
             }
@@ -137,6 +140,7 @@ HS_DEV void contrib4(const HsLattice &L, const SwX &w, int row, int x0, float ac
     for (int v = 0; v < 4; ++v) {
         const int x = x0 + v;
         if (x >= L.nx) continue;
+        tch[v] = true;
         hs_contrib(L, wi, row, x, acc[v], accp[v]);
         if (w.y == row && w.x == x) neg[v] = true;
     }
@@ -185,11 +189,11 @@ HS_DEV void update_items(const HsLattice &L, const SwX *s_sw, const int *s_pre, 
                     if (!owned) continue;  // warp-uniform
                     const int x0 = seg * 128 + lane * 4;
                     float acc[4] = {0.f, 0.f, 0.f, 0.f}, accp[4] = {0.f, 0.f, 0.f, 0.f};
-                    bool neg[4] = {false, false, false, false};
+                    bool neg[4] = {false, false, false, false}, tch[4] = {false, false, false, false};
                     for (int q = k; q < n; ++q) {
                         const SwX &w = s_sw[q];
                         if (w.sub < 0 || !covers_seg(L, w, row, seg)) continue;
-                        contrib4(L, w, row, x0, acc, accp, neg);
+                        contrib4(L, w, row, x0, acc, accp, neg, tch);
                     }
                     for (int q = n; q < nsw_total; ++q) {  // beyond the staged ones: from global memory
                         SwX w;
@@ -199,9 +203,11 @@ HS_DEV void update_items(const HsLattice &L, const SwX *s_sw, const int *s_pre, 
                         w.mm = __ldcg(L.mm + (int64_t)w.y * L.nx + w.x);
                         footprint(L, w);
                         if (!covers_seg(L, w, row, seg)) continue;
-                        contrib4(L, w, row, x0, acc, accp, neg);
+                        contrib4(L, w, row, x0, acc, accp, neg, tch);
                     }
-                    if (x0 >= L.nx) continue;
+                    // cells that no window reaches keep their energies (E + 0 = E): skip the
+                    // read-modify-write of lanes whose 4 cells are all outside the windows
+                    if (x0 >= L.nx || !(tch[0] || tch[1] || tch[2] || tch[3])) continue;
                     const int64_t i = (int64_t)row * L.nx + x0;
                     float mv[4];
                     double ev[4], pv[4];
@@ -280,6 +286,9 @@ HS_DEV void update_one(const HsLattice &L, int sy, int sx, float smm, int t0, in
     const float pref2 = (float)(2.0 * L.dip_pref);
     const bool two = L.use_perp != 0;
     constexpr int U = 4;
+    // window cell c = r ncols + q of this thread, advanced by nt cells per slot without divisions
+    const int dr = nt / ncols, dq = nt - dr * ncols;
+    int r0 = t0 / ncols, q0 = t0 - r0 * ncols;
     for (int base = t0; base < total; base += nt * U) {
         int idx[U], rw[U], cl[U];
         float kv[U], kp[U], mv[U], zf[U], zp[U], eb[U];
@@ -289,7 +298,9 @@ HS_DEV void update_one(const HsLattice &L, int sy, int sx, float smm, int t0, in
 #pragma unroll
         for (int k = 0; k < U; ++k) {
             const int c = base + k * nt;
-            const int r = c < total ? c / ncols : 0, q = c < total ? c - r * ncols : 0;
+            const int r = r0, q = q0;
+            r0 += dr; q0 += dq;
+            if (q0 >= ncols) { q0 -= ncols; ++r0; }
             int row = ylo + r, col = xlo + q;
             if (row >= L.ny) row -= L.ny;
             if (col >= L.nx) col -= L.nx;
@@ -362,8 +373,9 @@ struct Sync {
     }
 };
 
-HS_DEV HsKeyIdx eng_block_kmin(HsKeyIdx v, HsKeyIdx *sm) {
-    v = hs_warp_kmin(v);
+// Block minimum of (key, index); `warp_uniform`: v is already the warp's minimum on every lane.
+HS_DEV HsKeyIdx eng_block_kmin(HsKeyIdx v, HsKeyIdx *sm, bool warp_uniform = false) {
+    if (!warp_uniform) v = hs_warp_kmin(v);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) sm[warp] = v;
     __syncthreads();
@@ -432,6 +444,7 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
     __shared__ HsKeyIdx s_part[16];
     __shared__ HsKeyIdx s_red[32];
     __shared__ double s_dred[32];
+    __shared__ int s_nq[ENG_NT / 32][NEEL_QCAP];   // per-warp candidate queues of the cached Néel scan
     __shared__ SwX s_sw[ENG_SWCAP];
     __shared__ int s_pre[ENG_SWCAP];
     __shared__ __align__(16) HsInstance s_I;
@@ -540,9 +553,9 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
                 float *cache = (unif && !L.has_exchange && I.scratch_bytes >= HS_NEEL_CACHE_OFFSET + 4 * N)
                                    ? reinterpret_cast<float *>(reinterpret_cast<char *>(I.scratch) + HS_NEEL_CACHE_OFFSET)
                                    : nullptr;
-                HsKeyIdx best = (cache && st > 0) ? neel_scan_cached(L, cache, gt, gs, N, call, HsKeyIdx{0.0, -1})
+                HsKeyIdx best = (cache && st > 0) ? neel_scan_cached(L, cache, gt, gs, N, call, HsKeyIdx{0.0, -1}, s_nq[warp])
                                                   : neel_scan_range(L, gt, gs, N, call, bmin, HsKeyIdx{0.0, -1}, cache);
-                best = eng_block_kmin(best, s_red);
+                best = eng_block_kmin(best, s_red, cache && st > 0);
                 if (threadIdx.x == 0) {
                     if constexpr (CS == 1) s_part[0] = best;
                     else *cg::this_cluster().map_shared_rank(&s_part[rank], 0) = best;
@@ -551,7 +564,8 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
                 if (rank == 0 && threadIdx.x == 0) {
                     HsKeyIdx w{0.0, -1};
                     for (int r = 0; r < CS; ++r) w = hs_kmin(w, s_part[r]);
-                    neel_finalize(L, C, sw, w, call, bmin, unif, two, I.attempt_freq);
+                    float mm1 = 0.f;
+                    neel_finalize(L, C, sw, w, call, bmin, unif, two, I.attempt_freq, &mm1);
                     const int n1 = C->n_sw;
                     if (cache && !L.has_dipolar && n1 > 0) {  // no window update: refresh the flipped cell
                         const int64_t i = w.idx;
@@ -565,7 +579,7 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
                     if (n1 > 0) {
                         Sync<CS>::publish(&s_y1, (int)(w.idx / L.nx));
                         Sync<CS>::publish(&s_x1, (int)(w.idx % L.nx));
-                        Sync<CS>::publish(&s_mm1, L.mm[w.idx]);
+                        Sync<CS>::publish(&s_mm1, mm1);
                     }
                     decide_next(st + 1);
                 }

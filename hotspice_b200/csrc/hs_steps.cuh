@@ -827,7 +827,7 @@ HS_DEV void wolff_step_cta(const HsLattice &L, HsCounters *C, const HsSwitchList
 // switching time in FP64, flip, counters and the one-entry switch list
 // (hotspice/core.py:699-709). Executed by a single thread.
 HS_DEV void neel_finalize(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, HsKeyIdx w, uint64_t call,
-                          double bmin, bool unif, bool two, double attempt_freq) {
+                          double bmin, bool unif, bool two, double attempt_freq, float *mm_new = nullptr) {
     C->rng_call = call + 1;
     C->attempted += 1;
     C->steps += 1;
@@ -839,6 +839,10 @@ HS_DEV void neel_finalize(const HsLattice &L, HsCounters *C, const HsSwitchList 
         return;
     }
     const int64_t i = w.idx;
+    // the cell's spin and moment are loaded first, so that their round trips overlap the
+    // switching-time arithmetic below
+    const int8_t m_old = L.m[i];
+    const float mm_old = L.mm[i];
     const int y = (int)(i / L.nx), x = (int)(i % L.nx);
     // the barriers the scan computed for this cell (the same operations as hs_barriers)
     const double b1 = w.b1, b2 = w.b2;
@@ -861,8 +865,9 @@ HS_DEV void neel_finalize(const HsLattice &L, HsCounters *C, const HsSwitchList 
         C->n_sw = 0;
         return;
     }
-    L.m[i] = (int8_t)(-L.m[i]);
-    L.mm[i] = -L.mm[i];
+    L.m[i] = (int8_t)(-m_old);
+    L.mm[i] = -mm_old;
+    if (mm_new) *mm_new = -mm_old;
     C->switches += 1;
     C->t += time;
     sw.y[0] = y;
@@ -998,55 +1003,111 @@ HS_DEV HsKeyIdx neel_scan_range(const HsLattice &L, int64_t start64, int64_t str
     return best;
 }
 
+// Exact log-domain key of occupied cell i from its energies (uniform beta, b_min = 0): the
+// operations of neel_scan_range, so both give the same key bit for bit.
+HS_DEV HsKeyIdx neel_key_exact(const HsLattice &L, int i, uint32_t call_lo, uint32_t call_hi, const HsRoundKeys &RK) {
+    const bool two = L.use_perp != 0;
+    const double beta = L.beta_uniform;
+    const double uk = hs_u53_of(hs_philox_rk((uint32_t)i, call_lo, call_hi, 0u, RK));
+    double E = L.has_dipolar ? __ldcg(L.E_dip + i) : 0.0;
+    double Ep = (L.has_dipolar && two) ? __ldcg(L.E_dip_perp + i) : 0.0;
+    const int mv = __ldcg(L.m + i);
+    if (L.zee) { E += (double)mv * (double)__ldg(L.zee + i); if (two) Ep += (double)mv * (double)__ldg(L.zee_perp + i); }
+    double b1, b2;
+    hs_barriers_from(L, E, Ep, (double)__ldg(L.E_B + i), b1, b2);
+    const double le1 = (double)hs_log_exp1_f32(uk);
+    double key;
+    if (!two) key = le1 + b1 * beta;
+    else {
+        const double bm = fmin(b1, b2), dd = fabs(b1 - b2);
+        key = le1 + bm * beta - (double)log1pf(expf((float)(-dd * beta)));
+    }
+    return HsKeyIdx{key, i, b1, b2};
+}
+
+// Per-warp queue of the cached scan (shared memory, ints): cells whose lower bound does not rule
+// them out wait there and are evaluated 32 at a time, one per lane.
+constexpr int NEEL_QCAP = 64;
+
 // The same scan from the barrier cache (uniform beta, b_min = 0): per cell the cached
 // s = b_low beta, the Philox variate and the lower bound log u + s; the exact key (computed as
 // in neel_scan_range, from the energies) only for the cells the bound does not rule out.
+// Warp-collective: the 32 lanes of a warp call it together with consecutive `start`s
+// (start = warp base + lane) and share one running best (the warp's minimum so far), so a
+// cell is tested against the best of every cell the warp has evaluated. Cells the bound admits
+// go to the warp's queue `q` (NEEL_QCAP ints) in ballot order and are evaluated when 32 or more
+// wait, with every lane busy: a per-lane branch to the exact evaluation would cost the warp that
+// evaluation on almost every cell, since some lane of 32 usually admits one. Only cells whose
+// bound is strictly above a key already found are skipped, so the (key, index) minimum is that
+// of the exhaustive scan. Returns the warp's minimum on every lane.
 HS_DEV HsKeyIdx neel_scan_cached(const HsLattice &L, const float *cache, int64_t start64, int64_t stride64, int64_t N64,
-                                 uint64_t call, HsKeyIdx best) {
+                                 uint64_t call, HsKeyIdx best, int *q) {
     const bool two = L.use_perp != 0;
     const bool sparse = 4 * (int64_t)L.n_occ < 3 * N64;
     const int M = sparse ? L.n_occ : (int)N64;
-    const int start = (int)start64, stride = (int)stride64;
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    const int start0 = (int)start64 - lane, stride = (int)stride64;
     const double slack = (two ? 0.6931471805599453 : 0.0) + 1e-4;
-    const double beta = L.beta_uniform;
     const HsRoundKeys RK = hs_round_keys(L.seed);
     const uint32_t call_lo = (uint32_t)call, call_hi = (uint32_t)(call >> 32);
-    for (int base = start; base < M; base += stride * NEEL_UNR) {
+    best = hs_warp_kmin(best);
+    int qn = 0;   // warp-uniform
+    auto flush = [&]() {
+        __syncwarp();
+        for (int b = 0; b < qn; b += 32) {
+            HsKeyIdx c{0.0, -1};
+            if (b + lane < qn) c = neel_key_exact(L, q[b + lane], call_lo, call_hi, RK);
+            best = hs_kmin(best, hs_warp_kmin(c));
+        }
+        qn = 0;
+        __syncwarp();
+    };
+    for (int base = start0; base < M; base += stride * NEEL_UNR) {   // warp-uniform trip count
         int ci[NEEL_UNR];
         float sc[NEEL_UNR];
         HsU4 wv[NEEL_UNR];
 #pragma unroll
         for (int k = 0; k < NEEL_UNR; ++k) {
-            const int j = base + k * stride;
+            const int j = base + lane + k * stride;
             ci[k] = j < M ? (sparse ? __ldg(L.nonzero + j) : j) : 0;
         }
 #pragma unroll
-        for (int k = 0; k < NEEL_UNR; ++k) sc[k] = base + k * stride < M ? __ldcg(cache + ci[k]) : INFINITY;
+        for (int k = 0; k < NEEL_UNR; ++k) sc[k] = base + lane + k * stride < M ? __ldcg(cache + ci[k]) : INFINITY;
 #pragma unroll
         for (int k = 0; k < NEEL_UNR; ++k) wv[k] = hs_philox_rk((uint32_t)ci[k], call_lo, call_hi, 0u, RK);
+        // bounds from the first Philox word (below u53): the FP64 variate only for admitted cells
+        double lbk[NEEL_UNR];
+#pragma unroll
+        for (int k = 0; k < NEEL_UNR; ++k)
+            lbk[k] = sc[k] != INFINITY ? (double)__logf(hs_u24_low(wv[k])) + (double)sc[k] - slack : INFINITY;
+        if (best.idx < 0) {
+            // no key yet (warp-uniform): seed the best with the exact key of the cell with the
+            // warp's smallest bound, so that the first cells are not all admitted
+            double v = INFINITY;
+            int c = -1;
+#pragma unroll
+            for (int k = 0; k < NEEL_UNR; ++k)
+                if (lbk[k] < v) { v = lbk[k]; c = ci[k]; }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+                const int c2 = __shfl_xor_sync(0xffffffffu, c, o);
+                if (v2 < v || (v2 == v && c2 < c)) { v = v2; c = c2; }
+            }
+            if (c >= 0) best = neel_key_exact(L, c, call_lo, call_hi, RK);
+        }
 #pragma unroll
         for (int k = 0; k < NEEL_UNR; ++k) {
-            if (sc[k] == INFINITY) continue;
-            // bound from the first Philox word (below u53): the FP64 variate only for admitted cells
-            const double lbk = (double)__logf(hs_u24_low(wv[k])) + (double)sc[k] - slack;
-            if (best.idx >= 0 && lbk > best.key) continue;
-            const double uk = hs_u53_of(wv[k]);
-            const int i = ci[k];
-            double E = L.has_dipolar ? __ldcg(L.E_dip + i) : 0.0;
-            double Ep = (L.has_dipolar && two) ? __ldcg(L.E_dip_perp + i) : 0.0;
-            const int mv = __ldcg(L.m + i);
-            if (L.zee) { E += (double)mv * (double)__ldg(L.zee + i); if (two) Ep += (double)mv * (double)__ldg(L.zee_perp + i); }
-            double b1, b2;
-            hs_barriers_from(L, E, Ep, (double)__ldg(L.E_B + i), b1, b2);
-            const double le1 = (double)hs_log_exp1_f32(uk);
-            double key;
-            if (!two) key = le1 + b1 * beta;
-            else {
-                const double bm = fmin(b1, b2), dd = fabs(b1 - b2);
-                key = le1 + bm * beta - (double)log1pf(expf((float)(-dd * beta)));
+            const bool adm = lbk[k] != INFINITY && !(best.idx >= 0 && lbk[k] > best.key);
+            const unsigned m = __ballot_sync(0xffffffffu, adm);
+            if (m) {
+                if (adm) q[qn + __popc(m & below)] = ci[k];
+                qn += __popc(m);
+                if (qn >= 32) flush();
             }
-            best = hs_kmin(best, HsKeyIdx{key, i, b1, b2});
         }
     }
+    if (qn) flush();
     return best;
 }
