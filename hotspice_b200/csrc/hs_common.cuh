@@ -173,10 +173,10 @@ HS_DEV void hs_energy_at(const HsLattice &L, int y, int x, double &E, double &Ep
         E += (double)__ldcg(L.E_dip + i);
         if (L.use_perp) Ep += (double)__ldcg(L.E_dip_perp + i);
     }
-    if (L.zee) {
+    if (L.zee) {   // the Zeeman factors are read-only during a launch
         const double mi = (double)__ldcg(L.m + i);
-        E += mi * (double)L.zee[i];
-        if (L.use_perp) Ep += mi * (double)L.zee_perp[i];
+        E += mi * (double)__ldg(L.zee + i);
+        if (L.use_perp) Ep += mi * (double)__ldg(L.zee_perp + i);
     }
     if (L.has_exchange) {
         double e, ep;
@@ -230,8 +230,9 @@ HS_DEV bool hs_progress_continue(const HsCounters *C, int n_occ) {
 }
 
 // Arg-min helpers: smaller key wins, ties go to the smaller index (numpy nanargmin). A Néel
-// candidate also carries its two barriers, so the step's decision needs no reload of them.
-struct HsKeyIdx { double key; int idx; double b1, b2; };
+// candidate also carries its two barriers and, when the scan loaded them, its moment mm and
+// spin m (m = 0: not carried), so the step's decision needs no reload of them.
+struct HsKeyIdx { double key; int idx; double b1, b2; float mm; int m; };
 HS_DEV HsKeyIdx hs_kmin(HsKeyIdx a, HsKeyIdx b) {
     if (b.idx < 0) return a;
     if (a.idx < 0) return b;
@@ -246,6 +247,8 @@ HS_DEV HsKeyIdx hs_warp_kmin(HsKeyIdx v) {
         w.idx = __shfl_xor_sync(0xffffffffu, v.idx, o);
         w.b1 = __shfl_xor_sync(0xffffffffu, v.b1, o);
         w.b2 = __shfl_xor_sync(0xffffffffu, v.b2, o);
+        w.mm = __shfl_xor_sync(0xffffffffu, v.mm, o);
+        w.m = __shfl_xor_sync(0xffffffffu, v.m, o);
         v = hs_kmin(v, w);
     }
     return v;

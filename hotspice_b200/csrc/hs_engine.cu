@@ -14,7 +14,7 @@
 // Every branch that decides how many barriers are executed is taken on values every CTA of
 // the cluster reads after a barrier, so all CTAs always execute the same barrier sequence.
 //
-// The dipolar update distributes work items (switch k, window row, 32-column segment) over
+// The dipolar update distributes work items (switch k, window row, 128-column segment) over
 // all warps of the cluster. A strip (row, segment) is processed by the item of the first
 // switch whose window covers it, which accumulates the contributions of every covering
 // switch in list order: each strip is written once, deterministically, and the work is
@@ -44,7 +44,6 @@ struct SwX {                    // staged switch with its window footprint
     float mm;
     int ylo, nrows;             // window rows: (ylo + i) mod ny, i < nrows
     int sa0, sa1, sb0, sb1;     // covered 32-column segments: [sa0, sa1) and [sb0, sb1)
-    int items;                  // nrows * (segments)
 };
 
 HS_DEV void footprint(const HsLattice &L, SwX &w) {
@@ -73,27 +72,10 @@ HS_DEV void footprint(const HsLattice &L, SwX &w) {
         const int lo = max(0, w.x - hx), hi = min(L.nx - 1, w.x + hx);
         w.sa0 = lo >> 5; w.sa1 = (hi >> 5) + 1;
     }
-    w.items = w.nrows * ((w.sa1 - w.sa0) + (w.sb1 - w.sb0));
 }
 
-HS_DEV bool covers(const HsLattice &L, const SwX &w, int row, int seg) {
-    int d = row - w.ylo;
-    if (d < 0) d += L.ny;
-    if (d >= w.nrows) return false;
-    return (seg >= w.sa0 && seg < w.sa1) || (seg >= w.sb0 && seg < w.sb1);
-}
-
-// item index -> (row, segment) of switch w
-HS_DEV void item_strip(const HsLattice &L, const SwX &w, int it, int &row, int &seg) {
-    const int na = w.sa1 - w.sa0, nb = w.sb1 - w.sb0, per = na + nb;
-    const int r = it / per, s = it % per;
-    row = w.ylo + r;
-    if (row >= L.ny) row -= L.ny;
-    seg = s < na ? w.sa0 + s : w.sb0 + (s - na);
-}
-
-// Stage the switch list into shared memory with footprints and an inclusive item prefix.
-HS_DEV int stage_switches(const HsLattice &L, const HsSwitchList &sw, int nsw, SwX *s_sw, int *s_pre) {
+// Stage the switch list into shared memory with footprints.
+HS_DEV int stage_switches(const HsLattice &L, const HsSwitchList &sw, int nsw, SwX *s_sw) {
     const int n = min(nsw, ENG_SWCAP);
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
         SwX w;
@@ -101,13 +83,7 @@ HS_DEV int stage_switches(const HsLattice &L, const HsSwitchList &sw, int nsw, S
         w.sub = hs_sub(L, w.y, w.x);
         w.mm = __ldcg(L.mm + (int64_t)w.y * L.nx + w.x);
         footprint(L, w);
-        if (w.sub < 0) w.items = 0;
         s_sw[k] = w;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int acc = 0;
-        for (int k = 0; k < n; ++k) { acc += s_sw[k].items; s_pre[k] = acc; }
     }
     __syncthreads();
     return n;
@@ -160,7 +136,7 @@ HS_DEV bool covers_seg(const HsLattice &L, const SwX &w, int row, int seg128) {
 // Along the row the warp walks 128-column segments (4 cells per lane). A segment is written
 // by the item of the first switch covering it, which accumulates every covering switch in
 // list order.
-HS_DEV void update_items(const HsLattice &L, const SwX *s_sw, const int *s_pre, int n, int semantics, int gw, int nw,
+HS_DEV void update_items(const HsLattice &L, const SwX *s_sw, int n, int semantics, int gw, int nw,
                          const HsSwitchList &sw, int nsw_total) {
     if (n == 0) return;
     const int lane = threadIdx.x & 31;
@@ -269,7 +245,7 @@ HS_DEV void update_items(const HsLattice &L, const SwX *s_sw, const int *s_pre, 
 // cell the arithmetic is that of update_items for one switch (acc = mm_s K, E += 2 pref mm_j acc
 // in the same float order, then E_s negated), so the energies are the same bit for bit; cells
 // outside the window receive nothing there either.
-HS_DEV void update_one(const HsLattice &L, int sy, int sx, float smm, int t0, int nt, float *cache) {
+HS_DEV void update_one(const HsLattice &L, int sy, int sx, float smm, int8_t sm, int t0, int nt, float *cache) {
     const int sub = hs_sub(L, sy, sx);
     if (sub < 0) return;
     int hy, wy, hx, wx;
@@ -316,12 +292,15 @@ HS_DEV void update_one(const HsLattice &L, int sy, int sx, float smm, int t0, in
             const int i = idx[k];
             kv[k] = v ? hs_kval(L, L.K, sub, rw[k] - sy, cl[k] - sx) : 0.f;
             kp[k] = (v && two) ? hs_kval(L, L.Kpo, sub, rw[k] - sy, cl[k] - sx) : 0.f;
-            mv[k] = v ? __ldcg(L.mm + i) : 0.f;
+            // the switched cell's new moment and spin come from the handover (smm, sm): its
+            // global writes may still be in flight
+            const bool src = rw[k] == sy && cl[k] == sx;
+            mv[k] = v ? (src ? smm : __ldcg(L.mm + i)) : 0.f;
             ev[k] = v ? __ldcg(L.E_dip + i) : 0.0;
             pv[k] = (v && two) ? __ldcg(L.E_dip_perp + i) : 0.0;
             if (cache) {
                 oc[k] = v ? L.occ[i] : (int8_t)0;
-                ms[k] = v ? __ldcg(L.m + i) : (int8_t)0;
+                ms[k] = v ? (src ? sm : __ldcg(L.m + i)) : (int8_t)0;
                 zf[k] = (v && L.zee) ? __ldg(L.zee + i) : 0.f;
                 zp[k] = (v && L.zee && two) ? __ldg(L.zee_perp + i) : 0.f;
                 eb[k] = v ? __ldg(L.E_B + i) : 0.f;
@@ -358,6 +337,19 @@ struct Sync {
     HS_DEV static void all() {
         if constexpr (CS == 1) __syncthreads();
         else cg::this_cluster().sync();
+    }
+    // all(), with f() run by the threads for which `run` holds between their arrival and their
+    // wait (cluster barrier: its release covers only what came before the arrival)
+    template <typename F>
+    HS_DEV static void all_then(bool run, F f) {
+        if constexpr (CS == 1) {
+            if (run) f();
+            __syncthreads();
+        } else {
+            asm volatile("barrier.cluster.arrive;" ::: "memory");
+            if (run) f();
+            asm volatile("barrier.cluster.wait;" ::: "memory");
+        }
     }
     HS_DEV static int rank() {
         if constexpr (CS == 1) return 0;
@@ -435,7 +427,7 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
     // dynamic shared workspace (the Poisson-disc sampler's arrays), given only to launches that
     // hold Poisson-disc instances: it takes L1 capacity from the other phases
     extern __shared__ __align__(16) unsigned char s_ws[];
-    __shared__ int s_inst, s_n1, s_y1, s_x1, s_nsw;
+    __shared__ int s_inst, s_n1, s_y1, s_x1, s_m1, s_nsw;
     __shared__ int s_go[2];                    // step st runs while s_go[st & 1] (double-buffered)
     __shared__ float s_mm1;
     __shared__ unsigned long long s_call[2];   // Philox call of step st in s_call[st & 1]
@@ -446,7 +438,6 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
     __shared__ double s_dred[32];
     __shared__ int s_nq[ENG_NT / 32][NEEL_QCAP];   // per-warp candidate queues of the cached Néel scan
     __shared__ SwX s_sw[ENG_SWCAP];
-    __shared__ int s_pre[ENG_SWCAP];
     __shared__ __align__(16) HsInstance s_I;
     static_assert(sizeof(HsInstance) % 8 == 0, "HsInstance is copied in 8-byte words");
     const int rank = Sync<CS>::rank();
@@ -513,8 +504,8 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
                 Sync<CS>::all();
                 if (L.has_dipolar) {
                     const int nsw = s_nsw;
-                    const int n = stage_switches(L, sw, nsw, s_sw, s_pre);
-                    update_items(L, s_sw, s_pre, n, HS_UPDATE_MULTIPLE, rank * nwarps + warp, CS * nwarps, sw, nsw);
+                    const int n = stage_switches(L, sw, nsw, s_sw);
+                    update_items(L, s_sw, n, HS_UPDATE_MULTIPLE, rank * nwarps + warp, CS * nwarps, sw, nsw);
                 }
                 Sync<CS>::all();
             } else if (scheme == HS_SCHEME_NEEL) {
@@ -553,23 +544,32 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
                 float *cache = (unif && !L.has_exchange && I.scratch_bytes >= HS_NEEL_CACHE_OFFSET + 4 * N)
                                    ? reinterpret_cast<float *>(reinterpret_cast<char *>(I.scratch) + HS_NEEL_CACHE_OFFSET)
                                    : nullptr;
-                HsKeyIdx best = (cache && st > 0) ? neel_scan_cached(L, cache, gt, gs, N, call, HsKeyIdx{0.0, -1}, s_nq[warp])
-                                                  : neel_scan_range(L, gt, gs, N, call, bmin, HsKeyIdx{0.0, -1}, cache);
+                HsKeyIdx best{0.0, -1};
+                if (cache && st > 0) {
+                    // as many whole warps as give every thread a full chunk of cells (all threads
+                    // for large lattices): a small lattice is scanned by fewer warps, each with
+                    // the same chain of loads and exact evaluations as a full one
+                    const int64_t M = 4 * (int64_t)L.n_occ < 3 * N ? (int64_t)L.n_occ : N;
+                    const int64_t P = min(gs, (M + NEEL_UNR * 32 - 1) / (NEEL_UNR * 32) * 32);
+                    if (gt - (threadIdx.x & 31) < P) best = neel_scan_cached(L, cache, gt, P, N, call, best, s_nq[warp]);
+                } else {
+                    best = neel_scan_range(L, gt, gs, N, call, bmin, best, cache);
+                }
                 best = eng_block_kmin(best, s_red, cache && st > 0);
                 if (threadIdx.x == 0) {
                     if constexpr (CS == 1) s_part[0] = best;
                     else *cg::this_cluster().map_shared_rank(&s_part[rank], 0) = best;
                 }
                 Sync<CS>::all();
+                NeelFlip flip{};   // thread 0 of rank 0: the step's flip, written after the handover
                 if (rank == 0 && threadIdx.x == 0) {
                     HsKeyIdx w{0.0, -1};
                     for (int r = 0; r < CS; ++r) w = hs_kmin(w, s_part[r]);
-                    float mm1 = 0.f;
-                    neel_finalize(L, C, sw, w, call, bmin, unif, two, I.attempt_freq, &mm1);
+                    neel_finalize(L, C, sw, w, call, bmin, unif, two, I.attempt_freq, &flip);
                     const int n1 = C->n_sw;
                     if (cache && !L.has_dipolar && n1 > 0) {  // no window update: refresh the flipped cell
                         const int64_t i = w.idx;
-                        const double m = (double)L.m[i];
+                        const double m = (double)flip.m_new;
                         double E = 0.0, Ep = 0.0;
                         if (L.zee) { E = m * (double)L.zee[i]; if (two) Ep = m * (double)L.zee_perp[i]; }
                         cache[i] = neel_cache_value(L, E, Ep, (double)L.E_B[i]);
@@ -577,15 +577,20 @@ __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsIn
                     // hand the switch to every CTA through shared memory (no global round trip)
                     Sync<CS>::publish(&s_n1, n1);
                     if (n1 > 0) {
-                        Sync<CS>::publish(&s_y1, (int)(w.idx / L.nx));
-                        Sync<CS>::publish(&s_x1, (int)(w.idx % L.nx));
-                        Sync<CS>::publish(&s_mm1, mm1);
+                        Sync<CS>::publish(&s_y1, flip.y);
+                        Sync<CS>::publish(&s_x1, flip.x);
+                        Sync<CS>::publish(&s_mm1, flip.mm_new);
+                        Sync<CS>::publish(&s_m1, (int)flip.m_new);
                     }
                     decide_next(st + 1);
                 }
-                Sync<CS>::all();
+                // The flip's global writes (spin, moment, switch list) are issued after this
+                // thread's arrival at the barrier, so the barrier does not wait for them: the
+                // window update takes the switched cell's new spin and moment from the handover,
+                // and the writes are ordered before the next step by the barrier that ends this one.
+                Sync<CS>::all_then(rank == 0 && threadIdx.x == 0 && flip.flip, [&] { neel_apply(L, sw, flip); });
                 if (L.has_dipolar && s_n1 > 0)
-                    update_one(L, s_y1, s_x1, s_mm1, rank * blockDim.x + threadIdx.x, CS * blockDim.x, cache);
+                    update_one(L, s_y1, s_x1, s_mm1, (int8_t)s_m1, rank * blockDim.x + threadIdx.x, CS * blockDim.x, cache);
                 Sync<CS>::all();
             } else {  // Wolff
                 if (rank == 0) {

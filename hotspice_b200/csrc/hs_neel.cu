@@ -116,6 +116,8 @@ neel_scan_kernel(HsLattice L, HsCounters *C, HsSwitchList sw, double attempt_fre
         p.idx = __ldcg(&S->part[b].idx);
         p.b1 = __ldcg(&S->part[b].b1);
         p.b2 = __ldcg(&S->part[b].b2);
+        p.mm = __ldcg(&S->part[b].mm);
+        p.m = __ldcg(&S->part[b].m);
         w = hs_kmin(w, p);
     }
     __syncthreads();

@@ -359,8 +359,13 @@ HS_DEV bool metro_grid_fast(const HsLattice &L, HsCounters *C, const HsSwitchLis
     int acc = 0;
     double tpart = 0.0;
     long long near = 0;
+    int8_t m_old = 0;
+    float mm_old = 0.f;
     if (valid) {
         const int64_t i = (int64_t)y * L.nx + x;
+        // the spin and moment for the flip are loaded with the energies (one round trip)
+        m_old = __ldcg(L.m + i);
+        mm_old = __ldcg(L.mm + i);
         double E, Ep;
         hs_energy_at(L, y, x, E, Ep);
         const double beta = hs_beta(L, i);
@@ -380,8 +385,8 @@ HS_DEV bool metro_grid_fast(const HsLattice &L, HsCounters *C, const HsSwitchLis
     const int bin = acc ? (x % L.ux) + (y % L.uy) * L.ux : 0;
     if (acc) {
         const int64_t i = (int64_t)y * L.nx + x;
-        L.m[i] = (int8_t)(-L.m[i]);
-        L.mm[i] = -L.mm[i];
+        L.m[i] = (int8_t)(-m_old);
+        L.mm[i] = -mm_old;
         if (pa < sw.cap) { sw.y[pa] = y; sw.x[pa] = x; }
         atomicAdd(&s_bins[bin], 1);
     }
@@ -422,6 +427,8 @@ HS_DEV bool metro_grid_fast(const HsLattice &L, HsCounters *C, const HsSwitchLis
 HS_DEV bool metro_grid_warp(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, const HsGridPlan &P,
                             uint64_t call) {
     const int lane = threadIdx.x & 31;
+    // the lane's pick variate does not depend on the offsets: drawn alongside them
+    const double upick = lane < P.n_sc ? hs_u53(L.seed, call + 2, (uint32_t)lane) : 0.0;
     int ox, oy;
     if (L.pbc) {
         ox = (int)floor(hs_u53(L.seed, call, 0u) * L.nx);
@@ -438,7 +445,7 @@ HS_DEV bool metro_grid_warp(const HsLattice &L, HsCounters *C, const HsSwitchLis
     const int nscx = (min(P.snx, L.nx) + 1) / 2;
     int ok = 0, valid = 0, x = 0, y = 0;
     if (lane < P.n_sc) {
-        const int pick = (int)floor(hs_u53(L.seed, call + 2, (uint32_t)lane) * len);
+        const int pick = (int)floor(upick * len);
         const int yx = __ldg(P.phase_yx + off + pick);
         x = 2 * (lane % nscx) * P.Rx + (yx & 0xffff);
         y = 2 * (lane / nscx) * P.Ry + (yx >> 16);
@@ -449,7 +456,7 @@ HS_DEV bool metro_grid_warp(const HsLattice &L, HsCounters *C, const HsSwitchLis
             x += ox; y += oy;
             ok = x >= 0 && x < L.nx && y >= 0 && y < L.ny;
         }
-        valid = ok && L.occ[(int64_t)y * L.nx + x] != 0;
+        valid = ok && __ldg(L.occ + (int64_t)y * L.nx + x) != 0;
     }
     const unsigned below = (1u << lane) - 1u;
     const unsigned okb = __ballot_sync(0xffffffffu, ok), vb = __ballot_sync(0xffffffffu, valid);
@@ -462,8 +469,13 @@ HS_DEV bool metro_grid_warp(const HsLattice &L, HsCounters *C, const HsSwitchLis
     int acc = 0;
     double tpart = 0.0;
     int near = 0;
+    int8_t m_old = 0;
+    float mm_old = 0.f;
     if (valid) {
         const int64_t i = (int64_t)y * L.nx + x;
+        // the spin and moment for the flip are loaded with the energies (one round trip)
+        m_old = __ldcg(L.m + i);
+        mm_old = __ldcg(L.mm + i);
         double E, Ep;
         hs_energy_at(L, y, x, E, Ep);
         const double beta = hs_beta(L, i);
@@ -484,8 +496,8 @@ HS_DEV bool metro_grid_warp(const HsLattice &L, HsCounters *C, const HsSwitchLis
     const unsigned same = __match_any_sync(0xffffffffu, acc ? bin : -1);
     if (acc) {
         const int64_t i = (int64_t)y * L.nx + x;
-        L.m[i] = (int8_t)(-L.m[i]);
-        L.mm[i] = -L.mm[i];
+        L.m[i] = (int8_t)(-m_old);
+        L.mm[i] = -mm_old;
         if (pa < sw.cap) {
             sw.y[pa] = y; sw.x[pa] = x;
             if (sw.mode) sw.mode[pa] = __popc(same & accb) > L.trunc_cutoff ? 1 : 0;
@@ -826,8 +838,20 @@ HS_DEV void wolff_step_cta(const HsLattice &L, HsCounters *C, const HsSwitchList
 // Final stage of a Néel step once the global argmin `w` of the log-domain keys is known:
 // switching time in FP64, flip, counters and the one-entry switch list
 // (hotspice/core.py:699-709). Executed by a single thread.
+// The flip a Néel decision made, for a caller that writes it itself (neel_finalize's `defer`).
+struct NeelFlip { int64_t i; int y, x; int8_t m_new; float mm_new; bool flip; };
+HS_DEV void neel_apply(const HsLattice &L, const HsSwitchList &sw, const NeelFlip &f) {
+    L.m[f.i] = f.m_new;
+    L.mm[f.i] = f.mm_new;
+    sw.y[0] = f.y;
+    sw.x[0] = f.x;
+    if (sw.mode) sw.mode[0] = 0;
+}
+
+// `defer`: the flip (spin, moment, switch list) is returned there instead of being written.
 HS_DEV void neel_finalize(const HsLattice &L, HsCounters *C, const HsSwitchList &sw, HsKeyIdx w, uint64_t call,
-                          double bmin, bool unif, bool two, double attempt_freq, float *mm_new = nullptr) {
+                          double bmin, bool unif, bool two, double attempt_freq, NeelFlip *defer = nullptr) {
+    if (defer) defer->flip = false;
     C->rng_call = call + 1;
     C->attempted += 1;
     C->steps += 1;
@@ -839,10 +863,10 @@ HS_DEV void neel_finalize(const HsLattice &L, HsCounters *C, const HsSwitchList 
         return;
     }
     const int64_t i = w.idx;
-    // the cell's spin and moment are loaded first, so that their round trips overlap the
-    // switching-time arithmetic below
-    const int8_t m_old = L.m[i];
-    const float mm_old = L.mm[i];
+    // the cell's spin and moment: carried by the scan's record, else loaded first, so that
+    // their round trips overlap the switching-time arithmetic below
+    const int8_t m_old = w.m ? (int8_t)w.m : L.m[i];
+    const float mm_old = w.m ? w.mm : L.mm[i];
     const int y = (int)(i / L.nx), x = (int)(i % L.nx);
     // the barriers the scan computed for this cell (the same operations as hs_barriers)
     const double b1 = w.b1, b2 = w.b2;
@@ -865,14 +889,11 @@ HS_DEV void neel_finalize(const HsLattice &L, HsCounters *C, const HsSwitchList 
         C->n_sw = 0;
         return;
     }
-    L.m[i] = (int8_t)(-m_old);
-    L.mm[i] = -mm_old;
-    if (mm_new) *mm_new = -mm_old;
+    const NeelFlip f{i, y, x, (int8_t)(-m_old), -mm_old, true};
+    if (defer) *defer = f;
+    else neel_apply(L, sw, f);
     C->switches += 1;
     C->t += time;
-    sw.y[0] = y;
-    sw.x[0] = x;
-    if (sw.mode) sw.mode[0] = 0;
     C->n_sw = 1;
 }
 
@@ -1012,6 +1033,7 @@ HS_DEV HsKeyIdx neel_key_exact(const HsLattice &L, int i, uint32_t call_lo, uint
     double E = L.has_dipolar ? __ldcg(L.E_dip + i) : 0.0;
     double Ep = (L.has_dipolar && two) ? __ldcg(L.E_dip_perp + i) : 0.0;
     const int mv = __ldcg(L.m + i);
+    const float mm = __ldcg(L.mm + i);   // carried to the decision (same round trip)
     if (L.zee) { E += (double)mv * (double)__ldg(L.zee + i); if (two) Ep += (double)mv * (double)__ldg(L.zee_perp + i); }
     double b1, b2;
     hs_barriers_from(L, E, Ep, (double)__ldg(L.E_B + i), b1, b2);
@@ -1022,24 +1044,37 @@ HS_DEV HsKeyIdx neel_key_exact(const HsLattice &L, int i, uint32_t call_lo, uint
         const double bm = fmin(b1, b2), dd = fabs(b1 - b2);
         key = le1 + bm * beta - (double)log1pf(expf((float)(-dd * beta)));
     }
-    return HsKeyIdx{key, i, b1, b2};
+    return HsKeyIdx{key, i, b1, b2, mm, mv};
 }
 
 // Per-warp queue of the cached scan (shared memory, ints): cells whose lower bound does not rule
 // them out wait there and are evaluated 32 at a time, one per lane.
 constexpr int NEEL_QCAP = 64;
 
+// An upper bound of the exact key of a cell (neel_key_exact) from its first Philox word and its
+// cached s = b_low beta rounded down: u53 < u24 + 2^-24 and E1 = -log1p(-u) grows with u, the
+// two-channel term only lowers the key, s is below the next float up; 1e-4 covers the float
+// rounding of the logarithms (their absolute errors here are below 1e-5).
+HS_DEV double neel_key_upper(HsU4 w, float s) {
+    const float uh = hs_u24_low(w) + 5.9604644775390625e-08f;   // exact: a multiple of 2^-24 <= 1
+    const float le = __logf(-log1pf(-uh));
+    const double sh = (double)s + fabs((double)s) * 2.4e-7 + 1e-30;
+    return (double)le + sh + 1e-4;
+}
+
 // The same scan from the barrier cache (uniform beta, b_min = 0): per cell the cached
 // s = b_low beta, the Philox variate and the lower bound log u + s; the exact key (computed as
 // in neel_scan_range, from the energies) only for the cells the bound does not rule out.
 // Warp-collective: the 32 lanes of a warp call it together with consecutive `start`s
-// (start = warp base + lane) and share one running best (the warp's minimum so far), so a
-// cell is tested against the best of every cell the warp has evaluated. Cells the bound admits
-// go to the warp's queue `q` (NEEL_QCAP ints) in ballot order and are evaluated when 32 or more
-// wait, with every lane busy: a per-lane branch to the exact evaluation would cost the warp that
-// evaluation on almost every cell, since some lane of 32 usually admits one. Only cells whose
-// bound is strictly above a key already found are skipped, so the (key, index) minimum is that
-// of the exhaustive scan. Returns the warp's minimum on every lane.
+// (start = warp base + lane). The warp keeps T, an upper bound of the smallest key among the
+// cells it has seen (the minimum of the cells' upper bounds, neel_key_upper, and of the exact
+// keys found), and admits a cell only when its lower bound is not above T. Admitted cells go to
+// the warp's queue `q` (NEEL_QCAP ints) in ballot order and are evaluated exactly when 32 or
+// more wait, with every lane busy: a per-lane branch to the exact evaluation would cost the warp
+// that evaluation on almost every cell, since some lane of 32 usually admits one. The cell of
+// the smallest key always has its lower bound below T (every upper bound is at least that key),
+// so every cell that can win or tie is evaluated, and the (key, index) minimum is that of the
+// exhaustive scan. Returns the warp's minimum on every lane.
 HS_DEV HsKeyIdx neel_scan_cached(const HsLattice &L, const float *cache, int64_t start64, int64_t stride64, int64_t N64,
                                  uint64_t call, HsKeyIdx best, int *q) {
     const bool two = L.use_perp != 0;
@@ -1051,8 +1086,9 @@ HS_DEV HsKeyIdx neel_scan_cached(const HsLattice &L, const float *cache, int64_t
     const double slack = (two ? 0.6931471805599453 : 0.0) + 1e-4;
     const HsRoundKeys RK = hs_round_keys(L.seed);
     const uint32_t call_lo = (uint32_t)call, call_hi = (uint32_t)(call >> 32);
-    best = hs_warp_kmin(best);
-    int qn = 0;   // warp-uniform
+    if (__any_sync(0xffffffffu, best.idx >= 0)) best = hs_warp_kmin(best);
+    double T = best.idx >= 0 ? best.key : INFINITY;   // warp-uniform
+    int qn = 0;                                       // warp-uniform
     auto flush = [&]() {
         __syncwarp();
         for (int b = 0; b < qn; b += 32) {
@@ -1060,46 +1096,51 @@ HS_DEV HsKeyIdx neel_scan_cached(const HsLattice &L, const float *cache, int64_t
             if (b + lane < qn) c = neel_key_exact(L, q[b + lane], call_lo, call_hi, RK);
             best = hs_kmin(best, hs_warp_kmin(c));
         }
+        if (best.idx >= 0) T = fmin(T, best.key);
         qn = 0;
         __syncwarp();
     };
-    for (int base = start0; base < M; base += stride * NEEL_UNR) {   // warp-uniform trip count
-        int ci[NEEL_UNR];
-        float sc[NEEL_UNR];
-        HsU4 wv[NEEL_UNR];
+    // cell indices and cached bounds of the chunk at `base` (cells beyond M: index 0, bound +inf)
+    auto load = [&](int base, int *c, float *b) {
 #pragma unroll
         for (int k = 0; k < NEEL_UNR; ++k) {
             const int j = base + lane + k * stride;
-            ci[k] = j < M ? (sparse ? __ldg(L.nonzero + j) : j) : 0;
+            c[k] = j < M ? (sparse ? __ldg(L.nonzero + j) : j) : 0;
         }
 #pragma unroll
-        for (int k = 0; k < NEEL_UNR; ++k) sc[k] = base + lane + k * stride < M ? __ldcg(cache + ci[k]) : INFINITY;
+        for (int k = 0; k < NEEL_UNR; ++k) b[k] = base + lane + k * stride < M ? __ldcg(cache + c[k]) : INFINITY;
+    };
+    int ci[NEEL_UNR];
+    float sc[NEEL_UNR];
+    load(start0, ci, sc);
+    for (int base = start0; base < M; base += stride * NEEL_UNR) {   // warp-uniform trip count
+        // the next chunk's loads are issued first and complete while this chunk computes
+        int cn[NEEL_UNR];
+        float sn[NEEL_UNR];
+        load(base + stride * NEEL_UNR, cn, sn);
+        HsU4 wv[NEEL_UNR];
 #pragma unroll
         for (int k = 0; k < NEEL_UNR; ++k) wv[k] = hs_philox_rk((uint32_t)ci[k], call_lo, call_hi, 0u, RK);
         // bounds from the first Philox word (below u53): the FP64 variate only for admitted cells
         double lbk[NEEL_UNR];
+        double lmin = INFINITY;   // the lane's smallest bound of the chunk, with its word and s
+        HsU4 wmin = wv[0];
+        float smin = sc[0];
 #pragma unroll
-        for (int k = 0; k < NEEL_UNR; ++k)
+        for (int k = 0; k < NEEL_UNR; ++k) {
             lbk[k] = sc[k] != INFINITY ? (double)__logf(hs_u24_low(wv[k])) + (double)sc[k] - slack : INFINITY;
-        if (best.idx < 0) {
-            // no key yet (warp-uniform): seed the best with the exact key of the cell with the
-            // warp's smallest bound, so that the first cells are not all admitted
-            double v = INFINITY;
-            int c = -1;
+            if (lbk[k] < lmin) { lmin = lbk[k]; wmin = wv[k]; smin = sc[k]; }
+        }
+        if (__any_sync(0xffffffffu, lmin <= T)) {
+            // lower T with the upper bound of each lane's best cell of the chunk (warp-uniform)
+            double t = lmin <= T ? fmin(T, neel_key_upper(wmin, smin)) : T;
 #pragma unroll
-            for (int k = 0; k < NEEL_UNR; ++k)
-                if (lbk[k] < v) { v = lbk[k]; c = ci[k]; }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
-                const int c2 = __shfl_xor_sync(0xffffffffu, c, o);
-                if (v2 < v || (v2 == v && c2 < c)) { v = v2; c = c2; }
-            }
-            if (c >= 0) best = neel_key_exact(L, c, call_lo, call_hi, RK);
+            for (int o = 16; o > 0; o >>= 1) t = fmin(t, __shfl_xor_sync(0xffffffffu, t, o));
+            T = t;
         }
 #pragma unroll
         for (int k = 0; k < NEEL_UNR; ++k) {
-            const bool adm = lbk[k] != INFINITY && !(best.idx >= 0 && lbk[k] > best.key);
+            const bool adm = sc[k] != INFINITY && lbk[k] <= T;
             const unsigned m = __ballot_sync(0xffffffffu, adm);
             if (m) {
                 if (adm) q[qn + __popc(m & below)] = ci[k];
@@ -1107,6 +1148,8 @@ HS_DEV HsKeyIdx neel_scan_cached(const HsLattice &L, const float *cache, int64_t
                 if (qn >= 32) flush();
             }
         }
+#pragma unroll
+        for (int k = 0; k < NEEL_UNR; ++k) { ci[k] = cn[k]; sc[k] = sn[k]; }
     }
     if (qn) flush();
     return best;
