@@ -365,8 +365,7 @@ dip_update_persist_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev,
 #pragma unroll
                 for (int v = 0; v < VEC; ++v) { acc[r][v] = 0.f; accp[r][v] = 0.f; }
             unsigned touched = 0u, negate = 0u;   // bit r * VEC + v
-            for (int h = 0; h < nhit; ++h) {
-                const SwInfo w = s_sw[hl[h]];
+            auto apply = [&](const SwInfo &w) {
                 if (w.sub >= 0 && !w.mode && !L.dip_wrap) {
                     const int64_t kb = (int64_t)w.sub * KH * KW + (L.dip_wx - w.x);
 #pragma unroll
@@ -390,7 +389,7 @@ dip_update_persist_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev,
                             }
                         }
                     }
-                    continue;
+                    return;
                 }
 #pragma unroll
                 for (int r = 0; r < UPD_RPW; ++r) {
@@ -409,6 +408,23 @@ dip_update_persist_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev,
                         if (w.y == y && w.x == x) negate |= 1u << (r * VEC + v);
                     }
                 }
+            };
+            if (nhit <= 64) {
+                // Each lane applies only the hits whose window reaches its own cells (a mask over
+                // the tile's list, visited in list order): with windows narrower than the tile,
+                // most hits of a tile miss most lanes, and skipping them changes no sum.
+                unsigned long long mine = 0ull;
+                const int yhi = y0 + nrows - 1, xhi = x0 + VEC - 1;
+                for (int h = 0; h < nhit; ++h) {
+                    const SwInfo w = s_sw[hl[h]];
+                    const bool exact = w.sub >= 0 && !w.mode && !L.dip_wrap;
+                    const bool reach = !exact || (w.y - L.dip_wy <= yhi && w.y + L.dip_wy >= y0 &&
+                                                  w.x - L.dip_wx <= xhi && w.x + L.dip_wx >= x0);
+                    if (reach) mine |= 1ull << h;
+                }
+                for (; mine; mine &= mine - 1ull) apply(s_sw[hl[__ffsll((long long)mine) - 1]]);
+            } else {
+                for (int h = 0; h < nhit; ++h) apply(s_sw[hl[h]]);
             }
             const bool vec_rows = VEC == 4 && x0 + 3 < L.nx && (L.nx & 3) == 0;
 #pragma unroll
