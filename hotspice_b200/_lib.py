@@ -21,6 +21,7 @@ HS_SAMPLE_SINGLE, HS_SAMPLE_GRID, HS_SAMPLE_POISSON = 0, 1, 2
 HS_BARRIER_SIMPLE, HS_BARRIER_PARABOLIC = 0, 1
 HS_UPDATE_SINGLE, HS_UPDATE_MULTIPLE = 0, 1
 HS_SEGMENT_MAX = 65536
+HS_INST_ONE_CTA = 1   # HsInstance.flags: run on one CTA of its cluster
 
 P = C.c_void_p
 

@@ -421,195 +421,262 @@ HS_DEV WolffScratch wolff_scratch_of(const HsLattice &L, void *base) {
     return S;
 }
 
+// Shared state of one CTA while it runs an instance.
+struct __align__(16) EngShared {
+    HsInstance I;                       // the instance descriptor, staged (read through references)
+    HsCounters C;                       // rank 0: the instance's counters for the whole run
+    unsigned long long call[2];         // Philox call of step st in call[st & 1]
+    HsKeyIdx part[16];
+    HsKeyIdx red[32];
+    double dred[32];
+    int inst, n1, y1, x1, m1, nsw;
+    int go[2];                          // step st runs while go[st & 1] (double-buffered)
+    float mm1;
+    int nq[ENG_NT / 32][NEEL_QCAP];     // per-warp candidate queues of the cached Néel scan
+    SwX sw[ENG_SWCAP];
+};
+static_assert(sizeof(HsInstance) % 8 == 0, "HsInstance is copied in 8-byte words");
+static_assert(sizeof(HsCounters) % 8 == 0, "HsCounters is copied in 8-byte words");
+
+// Barriers and publication over the CTAs that run the current instance: the whole cluster, or
+// this CTA alone (CTA mode). One copy of the step code serves both (a uniform branch per
+// barrier), which keeps the kernel's register allocation that of the cluster path.
+template <int CS>
+struct RunSync {
+    bool alone;
+    HS_DEV void all() const {
+        if (CS == 1 || alone) __syncthreads();
+        else Sync<CS>::all();
+    }
+    template <typename F>
+    HS_DEV void all_then(bool run, F f) const {
+        if (CS == 1 || alone) { if (run) f(); __syncthreads(); }
+        else Sync<CS>::all_then(run, f);
+    }
+    template <typename T>
+    HS_DEV void publish(T *local, T v) const {
+        if (CS == 1 || alone) *local = v;
+        else Sync<CS>::publish(local, v);
+    }
+    // rank 0's slot r of a per-CTA array receives v (r = this CTA's rank)
+    template <typename T>
+    HS_DEV void to_rank0(T *arr, int r, T v) const {
+        if constexpr (CS == 1) arr[0] = v;
+        else if (alone) arr[0] = v;
+        else *cg::this_cluster().map_shared_rank(&arr[r], 0) = v;
+    }
+};
+
+// Run instance ii to the end of its step budget (or its stop rule) on the whole cluster
+// (`rank` = this CTA's rank) or, in CTA mode, on this CTA alone (rank 0).
+template <int CS>
+HS_DEV void run_instance(EngShared &sh, const HsInstance *insts, int ii, int rank, bool alone, unsigned char *s_ws,
+                         int ws_bytes, long long *elapsed_ns) {
+    const RunSync<CS> S{alone};
+    const int SCS = (CS == 1 || alone) ? 1 : CS;   // CTAs running the instance
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    const unsigned long long t_claim = hs_globaltimer_ns();   // used by rank 0, thread 0
+    {   // stage the instance descriptor in shared memory
+        const unsigned long long *src = reinterpret_cast<const unsigned long long *>(insts + ii);
+        unsigned long long *dst = reinterpret_cast<unsigned long long *>(&sh.I);
+        for (int k = threadIdx.x; k < (int)(sizeof(HsInstance) / 8); k += blockDim.x) dst[k] = __ldg(src + k);
+        __syncthreads();
+    }
+    const HsInstance &I = sh.I;
+    const HsLattice &L = sh.I.L;
+    const HsSwitchList &sw = sh.I.sw;
+    const HsGridPlan &P = sh.I.P;
+    // The counters live in rank 0's shared memory while the instance runs (every step reads
+    // and updates them) and go back to global memory when it stops; other CTAs receive the
+    // values they need (Philox call, switch count) through distributed shared memory.
+    HsCounters *const Cg = sh.I.C;
+    HsCounters *const C = &sh.C;
+    if (rank == 0) {
+        const unsigned long long *src = reinterpret_cast<const unsigned long long *>(Cg);
+        unsigned long long *dst = reinterpret_cast<unsigned long long *>(&sh.C);
+        for (int k = threadIdx.x; k < (int)(sizeof(HsCounters) / 8); k += blockDim.x) dst[k] = __ldcg(src + k);
+    }
+    __syncthreads();
+    const int scheme = sh.I.scheme;
+    // progress() runs: at most `budget` steps in this launch; an unfinished run keeps done = 0
+    // and the next launch continues it, so every launch ends
+    const int64_t budget = I.steps > 0 ? I.steps : (int64_t)HS_PROGRESS_STEPS_MAX;
+    // Whether step st runs, and its Philox call, are decided by rank 0's thread 0 as soon as
+    // the counters of step st - 1 are final (right after its decision phase) and published
+    // to every CTA in slot st & 1; the barriers that end step st - 1 make them visible, so a
+    // step needs no barrier of its own for this. Slot st & 1 was last read at the start of
+    // step st - 2, before that step's barriers, so the write cannot overtake a read.
+    auto decide_next = [&](int64_t next) {
+        int go;
+        if (C->done) go = 0;
+        else if (C->progress) {
+            if (C->status || next >= budget) go = 0;   // a failed step, or the budget: not done
+            else { go = hs_progress_continue(C, L.n_occ); if (!go) { C->done = 1; C->n_sw = 0; } }
+        }
+        else go = next < I.steps;
+        S.publish(&sh.go[next & 1], go);
+        S.publish(&sh.call[next & 1], (unsigned long long)C->rng_call);
+    };
+    if (rank == 0 && threadIdx.x == 0) decide_next(0);
+    S.all();
+    for (int64_t st = 0;; ++st) {
+        if (!sh.go[st & 1]) break;
+        if (scheme == HS_SCHEME_METROPOLIS) {
+            if (rank == 0) {
+                metro_step_cta(L, C, sw, P, metro_scratch_of(L, P, I.scratch), ws_bytes > 0 ? s_ws : nullptr,
+                               ws_bytes);
+                __syncthreads();
+                if (threadIdx.x == 0) { S.publish(&sh.nsw, C->n_sw); decide_next(st + 1); }
+            }
+            S.all();
+            if (L.has_dipolar) {
+                const int nsw = sh.nsw;
+                const int n = stage_switches(L, sw, nsw, sh.sw);
+                update_items(L, sh.sw, n, HS_UPDATE_MULTIPLE, rank * nwarps + warp, SCS * nwarps, sw, nsw);
+            }
+            S.all();
+        } else if (scheme == HS_SCHEME_NEEL) {
+            const uint64_t call = sh.call[st & 1];
+            const int64_t N = (int64_t)L.nx * L.ny;
+            const int64_t gt = (int64_t)rank * blockDim.x + threadIdx.x, gs = (int64_t)SCS * blockDim.x;
+            const bool unif = L.beta_uniform > 0.0;
+            double bmin = 0.0;
+            if (!unif) {  // b_min pass (hotspice/core.py:688, 696)
+                double v = INFINITY;
+                for (int64_t i = gt; i < N; i += gs) {
+                    if (!L.occ[i]) continue;
+                    double b1, b2;
+                    hs_barriers(L, (int)(i / L.nx), (int)(i % L.nx), b1, b2);
+                    v = fmin(v, fmin(b1, b2));
+                }
+                v = eng_block_dmin(v, sh.dred);
+                if (threadIdx.x == 0) S.to_rank0(sh.part, rank, HsKeyIdx{v, rank});
+                S.all();
+                if (rank == 0 && threadIdx.x == 0) {
+                    double b = INFINITY;
+                    for (int r = 0; r < SCS; ++r) b = fmin(b, sh.part[r].key);
+                    C->bmin = b;
+                    S.publish(&sh.dred[0], b);
+                }
+                S.all();
+                bmin = sh.dred[0];
+                S.all();
+            }
+            const bool two = L.use_perp != 0;
+            // barrier cache: uniform beta, no exchange (its neighbours change outside the window)
+            float *cache = (unif && !L.has_exchange && I.scratch_bytes >= HS_NEEL_CACHE_OFFSET + 4 * N)
+                               ? reinterpret_cast<float *>(reinterpret_cast<char *>(I.scratch) + HS_NEEL_CACHE_OFFSET)
+                               : nullptr;
+            HsKeyIdx best{0.0, -1};
+            if (cache && st > 0) {
+                // as many whole warps as give every thread a full chunk of cells (all threads
+                // for large lattices): a small lattice is scanned by fewer warps, each with
+                // the same chain of loads and exact evaluations as a full one
+                const int64_t M = 4 * (int64_t)L.n_occ < 3 * N ? (int64_t)L.n_occ : N;
+                const int64_t Pw = min(gs, (M + NEEL_UNR * 32 - 1) / (NEEL_UNR * 32) * 32);
+                if (gt - (threadIdx.x & 31) < Pw) best = neel_scan_cached(L, cache, gt, Pw, N, call, best, sh.nq[warp]);
+            } else {
+                best = neel_scan_range(L, gt, gs, N, call, bmin, best, cache);
+            }
+            best = eng_block_kmin(best, sh.red, cache && st > 0);
+            if (threadIdx.x == 0) S.to_rank0(sh.part, rank, best);
+            S.all();
+            NeelFlip flip{};   // thread 0 of rank 0: the step's flip, written after the handover
+            if (rank == 0 && threadIdx.x == 0) {
+                HsKeyIdx w{0.0, -1};
+                for (int r = 0; r < SCS; ++r) w = hs_kmin(w, sh.part[r]);
+                neel_finalize(L, C, sw, w, call, bmin, unif, two, I.attempt_freq, &flip);
+                const int n1 = C->n_sw;
+                if (cache && !L.has_dipolar && n1 > 0) {  // no window update: refresh the flipped cell
+                    const int64_t i = w.idx;
+                    const double m = (double)flip.m_new;
+                    double E = 0.0, Ep = 0.0;
+                    if (L.zee) { E = m * (double)L.zee[i]; if (two) Ep = m * (double)L.zee_perp[i]; }
+                    cache[i] = neel_cache_value(L, E, Ep, (double)L.E_B[i]);
+                }
+                // hand the switch to every CTA through shared memory (no global round trip)
+                S.publish(&sh.n1, n1);
+                if (n1 > 0) {
+                    S.publish(&sh.y1, flip.y);
+                    S.publish(&sh.x1, flip.x);
+                    S.publish(&sh.mm1, flip.mm_new);
+                    S.publish(&sh.m1, (int)flip.m_new);
+                }
+                decide_next(st + 1);
+            }
+            // The flip's global writes (spin, moment, switch list) are issued after this
+            // thread's arrival at the barrier, so the barrier does not wait for them: the
+            // window update takes the switched cell's new spin and moment from the handover,
+            // and the writes are ordered before the next step by the barrier that ends this one.
+            S.all_then(rank == 0 && threadIdx.x == 0 && flip.flip, [&] { neel_apply(L, sw, flip); });
+            if (L.has_dipolar && sh.n1 > 0)
+                update_one(L, sh.y1, sh.x1, sh.mm1, (int8_t)sh.m1, rank * blockDim.x + threadIdx.x, SCS * blockDim.x, cache);
+            S.all();
+        } else {  // Wolff
+            if (rank == 0) {
+                wolff_step_cta(L, C, sw, wolff_scratch_of(L, I.scratch));
+                __syncthreads();
+                if (threadIdx.x == 0) decide_next(st + 1);
+            }
+            S.all();
+        }
+    }
+    S.all();
+    if (rank == 0) {  // counters back to global memory
+        const unsigned long long *src = reinterpret_cast<const unsigned long long *>(&sh.C);
+        unsigned long long *dst = reinterpret_cast<unsigned long long *>(Cg);
+        for (int k = threadIdx.x; k < (int)(sizeof(HsCounters) / 8); k += blockDim.x) dst[k] = src[k];
+        // the device time spent on this instance in this launch
+        if (elapsed_ns && threadIdx.x == 0) elapsed_ns[ii] = (long long)(hs_globaltimer_ns() - t_claim);
+    }
+    __syncthreads();
+}
+
+// Clusters claim instances from the work counter (rank 0 claims for the cluster). An instance
+// flagged HS_INST_ONE_CTA switches the cluster to CTA mode for the rest of the launch: rank 0
+// runs that instance alone, every other CTA claims one of its own, and from then on each CTA
+// claims and runs instances by itself, with block barriers only. The switch is decided on the
+// same flag by every CTA of the cluster, right after the barrier that follows the claim, and
+// no cluster barrier or distributed shared memory access follows it, so a CTA may leave the
+// launch while the others of its cluster still run. The host lists the flagged instances
+// after all others (a flagged instance is never followed by one that needs the cluster; one
+// that is still runs correctly, on one CTA).
 template <int CS>
 __global__ void __launch_bounds__(ENG_NT, ENG_MIN_CTAS) engine_kernel(const HsInstance *insts, int n_inst, int *work,
                                                                       int ws_bytes, long long *elapsed_ns) {
     // dynamic shared workspace (the Poisson-disc sampler's arrays), given only to launches that
     // hold Poisson-disc instances: it takes L1 capacity from the other phases
     extern __shared__ __align__(16) unsigned char s_ws[];
-    __shared__ int s_inst, s_n1, s_y1, s_x1, s_m1, s_nsw;
-    __shared__ int s_go[2];                    // step st runs while s_go[st & 1] (double-buffered)
-    __shared__ float s_mm1;
-    __shared__ unsigned long long s_call[2];   // Philox call of step st in s_call[st & 1]
-    __shared__ __align__(16) HsCounters s_C;   // rank 0: the instance's counters for the whole run
-    static_assert(sizeof(HsCounters) % 8 == 0, "HsCounters is copied in 8-byte words");
-    __shared__ HsKeyIdx s_part[16];
-    __shared__ HsKeyIdx s_red[32];
-    __shared__ double s_dred[32];
-    __shared__ int s_nq[ENG_NT / 32][NEEL_QCAP];   // per-warp candidate queues of the cached Néel scan
-    __shared__ SwX s_sw[ENG_SWCAP];
-    __shared__ __align__(16) HsInstance s_I;
-    static_assert(sizeof(HsInstance) % 8 == 0, "HsInstance is copied in 8-byte words");
+    __shared__ EngShared sh;
     const int rank = Sync<CS>::rank();
-    const int warp = threadIdx.x >> 5;
-    const int nwarps = blockDim.x >> 5;
+    bool alone = false;
     for (;;) {
-        if (rank == 0 && threadIdx.x == 0) Sync<CS>::publish(&s_inst, atomicAdd(work, 1));
-        Sync<CS>::all();
-        const int ii = s_inst;
-        if (ii >= n_inst) break;
-        const unsigned long long t_claim = hs_globaltimer_ns();   // used by rank 0, thread 0
-        {   // stage the instance descriptor in shared memory (read through references below)
-            const unsigned long long *src = reinterpret_cast<const unsigned long long *>(insts + ii);
-            unsigned long long *dst = reinterpret_cast<unsigned long long *>(&s_I);
-            for (int k = threadIdx.x; k < (int)(sizeof(HsInstance) / 8); k += blockDim.x) dst[k] = __ldg(src + k);
+        int ii;
+        if (!alone) {
+            if (rank == 0 && threadIdx.x == 0) Sync<CS>::publish(&sh.inst, atomicAdd(work, 1));
+            Sync<CS>::all();
+            ii = sh.inst;
+            if (ii >= n_inst) break;
+            if constexpr (CS > 1) {
+                if (__ldg(&insts[ii].flags) & HS_INST_ONE_CTA) {
+                    alone = true;
+                    if (rank != 0) {
+                        __syncthreads();   // every thread has read the cluster's claim
+                        if (threadIdx.x == 0) sh.inst = atomicAdd(work, 1);
+                        __syncthreads();
+                        ii = sh.inst;
+                        if (ii >= n_inst) break;
+                    }
+                }
+            }
+        } else {
+            if (threadIdx.x == 0) sh.inst = atomicAdd(work, 1);
             __syncthreads();
+            ii = sh.inst;
+            if (ii >= n_inst) break;
         }
-        const HsInstance &I = s_I;
-        const HsLattice &L = s_I.L;
-        const HsSwitchList &sw = s_I.sw;
-        const HsGridPlan &P = s_I.P;
-        // The counters live in rank 0's shared memory while the instance runs (every step reads
-        // and updates them) and go back to global memory when it stops; other CTAs receive the
-        // values they need (Philox call, switch count) through distributed shared memory.
-        HsCounters *const Cg = s_I.C;
-        HsCounters *const C = &s_C;
-        if (rank == 0) {
-            const unsigned long long *src = reinterpret_cast<const unsigned long long *>(Cg);
-            unsigned long long *dst = reinterpret_cast<unsigned long long *>(&s_C);
-            for (int k = threadIdx.x; k < (int)(sizeof(HsCounters) / 8); k += blockDim.x) dst[k] = __ldcg(src + k);
-        }
-        __syncthreads();
-        const int scheme = s_I.scheme;
-        // progress() runs: at most `budget` steps in this launch; an unfinished run keeps done = 0
-        // and the next launch continues it, so every launch ends
-        const int64_t budget = I.steps > 0 ? I.steps : (int64_t)HS_PROGRESS_STEPS_MAX;
-        // Whether step st runs, and its Philox call, are decided by rank 0's thread 0 as soon as
-        // the counters of step st - 1 are final (right after its decision phase) and published
-        // to every CTA in slot st & 1; the barriers that end step st - 1 make them visible, so a
-        // step needs no barrier of its own for this. Slot st & 1 was last read at the start of
-        // step st - 2, before that step's barriers, so the write cannot overtake a read.
-        auto decide_next = [&](int64_t next) {
-            int go;
-            if (C->done) go = 0;
-            else if (C->progress) {
-                if (C->status || next >= budget) go = 0;   // a failed step, or the budget: not done
-                else { go = hs_progress_continue(C, L.n_occ); if (!go) { C->done = 1; C->n_sw = 0; } }
-            }
-            else go = next < I.steps;
-            Sync<CS>::publish(&s_go[next & 1], go);
-            Sync<CS>::publish(&s_call[next & 1], (unsigned long long)C->rng_call);
-        };
-        if (rank == 0 && threadIdx.x == 0) decide_next(0);
-        Sync<CS>::all();
-        for (int64_t st = 0;; ++st) {
-            if (!s_go[st & 1]) break;
-            if (scheme == HS_SCHEME_METROPOLIS) {
-                if (rank == 0) {
-                    metro_step_cta(L, C, sw, P, metro_scratch_of(L, P, I.scratch), ws_bytes > 0 ? s_ws : nullptr,
-                                   ws_bytes);
-                    __syncthreads();
-                    if (threadIdx.x == 0) { Sync<CS>::publish(&s_nsw, C->n_sw); decide_next(st + 1); }
-                }
-                Sync<CS>::all();
-                if (L.has_dipolar) {
-                    const int nsw = s_nsw;
-                    const int n = stage_switches(L, sw, nsw, s_sw);
-                    update_items(L, s_sw, n, HS_UPDATE_MULTIPLE, rank * nwarps + warp, CS * nwarps, sw, nsw);
-                }
-                Sync<CS>::all();
-            } else if (scheme == HS_SCHEME_NEEL) {
-                const uint64_t call = s_call[st & 1];
-                const int64_t N = (int64_t)L.nx * L.ny;
-                const int64_t gt = (int64_t)rank * blockDim.x + threadIdx.x, gs = (int64_t)CS * blockDim.x;
-                const bool unif = L.beta_uniform > 0.0;
-                double bmin = 0.0;
-                if (!unif) {  // b_min pass (hotspice/core.py:688, 696)
-                    double v = INFINITY;
-                    for (int64_t i = gt; i < N; i += gs) {
-                        if (!L.occ[i]) continue;
-                        double b1, b2;
-                        hs_barriers(L, (int)(i / L.nx), (int)(i % L.nx), b1, b2);
-                        v = fmin(v, fmin(b1, b2));
-                    }
-                    v = eng_block_dmin(v, s_dred);
-                    if (threadIdx.x == 0) {
-                        HsKeyIdx p{v, rank};
-                        if constexpr (CS == 1) s_part[0] = p;
-                        else *cg::this_cluster().map_shared_rank(&s_part[rank], 0) = p;
-                    }
-                    Sync<CS>::all();
-                    if (rank == 0 && threadIdx.x == 0) {
-                        double b = INFINITY;
-                        for (int r = 0; r < CS; ++r) b = fmin(b, s_part[r].key);
-                        C->bmin = b;
-                        Sync<CS>::publish(&s_dred[0], b);
-                    }
-                    Sync<CS>::all();
-                    bmin = s_dred[0];
-                    Sync<CS>::all();
-                }
-                const bool two = L.use_perp != 0;
-                // barrier cache: uniform beta, no exchange (its neighbours change outside the window)
-                float *cache = (unif && !L.has_exchange && I.scratch_bytes >= HS_NEEL_CACHE_OFFSET + 4 * N)
-                                   ? reinterpret_cast<float *>(reinterpret_cast<char *>(I.scratch) + HS_NEEL_CACHE_OFFSET)
-                                   : nullptr;
-                HsKeyIdx best{0.0, -1};
-                if (cache && st > 0) {
-                    // as many whole warps as give every thread a full chunk of cells (all threads
-                    // for large lattices): a small lattice is scanned by fewer warps, each with
-                    // the same chain of loads and exact evaluations as a full one
-                    const int64_t M = 4 * (int64_t)L.n_occ < 3 * N ? (int64_t)L.n_occ : N;
-                    const int64_t P = min(gs, (M + NEEL_UNR * 32 - 1) / (NEEL_UNR * 32) * 32);
-                    if (gt - (threadIdx.x & 31) < P) best = neel_scan_cached(L, cache, gt, P, N, call, best, s_nq[warp]);
-                } else {
-                    best = neel_scan_range(L, gt, gs, N, call, bmin, best, cache);
-                }
-                best = eng_block_kmin(best, s_red, cache && st > 0);
-                if (threadIdx.x == 0) {
-                    if constexpr (CS == 1) s_part[0] = best;
-                    else *cg::this_cluster().map_shared_rank(&s_part[rank], 0) = best;
-                }
-                Sync<CS>::all();
-                NeelFlip flip{};   // thread 0 of rank 0: the step's flip, written after the handover
-                if (rank == 0 && threadIdx.x == 0) {
-                    HsKeyIdx w{0.0, -1};
-                    for (int r = 0; r < CS; ++r) w = hs_kmin(w, s_part[r]);
-                    neel_finalize(L, C, sw, w, call, bmin, unif, two, I.attempt_freq, &flip);
-                    const int n1 = C->n_sw;
-                    if (cache && !L.has_dipolar && n1 > 0) {  // no window update: refresh the flipped cell
-                        const int64_t i = w.idx;
-                        const double m = (double)flip.m_new;
-                        double E = 0.0, Ep = 0.0;
-                        if (L.zee) { E = m * (double)L.zee[i]; if (two) Ep = m * (double)L.zee_perp[i]; }
-                        cache[i] = neel_cache_value(L, E, Ep, (double)L.E_B[i]);
-                    }
-                    // hand the switch to every CTA through shared memory (no global round trip)
-                    Sync<CS>::publish(&s_n1, n1);
-                    if (n1 > 0) {
-                        Sync<CS>::publish(&s_y1, flip.y);
-                        Sync<CS>::publish(&s_x1, flip.x);
-                        Sync<CS>::publish(&s_mm1, flip.mm_new);
-                        Sync<CS>::publish(&s_m1, (int)flip.m_new);
-                    }
-                    decide_next(st + 1);
-                }
-                // The flip's global writes (spin, moment, switch list) are issued after this
-                // thread's arrival at the barrier, so the barrier does not wait for them: the
-                // window update takes the switched cell's new spin and moment from the handover,
-                // and the writes are ordered before the next step by the barrier that ends this one.
-                Sync<CS>::all_then(rank == 0 && threadIdx.x == 0 && flip.flip, [&] { neel_apply(L, sw, flip); });
-                if (L.has_dipolar && s_n1 > 0)
-                    update_one(L, s_y1, s_x1, s_mm1, (int8_t)s_m1, rank * blockDim.x + threadIdx.x, CS * blockDim.x, cache);
-                Sync<CS>::all();
-            } else {  // Wolff
-                if (rank == 0) {
-                    wolff_step_cta(L, C, sw, wolff_scratch_of(L, I.scratch));
-                    __syncthreads();
-                    if (threadIdx.x == 0) decide_next(st + 1);
-                }
-                Sync<CS>::all();
-            }
-        }
-        Sync<CS>::all();
-        if (rank == 0) {  // counters back to global memory
-            const unsigned long long *src = reinterpret_cast<const unsigned long long *>(&s_C);
-            unsigned long long *dst = reinterpret_cast<unsigned long long *>(Cg);
-            for (int k = threadIdx.x; k < (int)(sizeof(HsCounters) / 8); k += blockDim.x) dst[k] = src[k];
-            // the cluster's device time on this instance in this launch
-            if (elapsed_ns && threadIdx.x == 0) elapsed_ns[ii] = (long long)(hs_globaltimer_ns() - t_claim);
-        }
-        __syncthreads();
+        run_instance<CS>(sh, insts, ii, alone ? 0 : rank, alone, s_ws, ws_bytes, elapsed_ns);
     }
 }
 

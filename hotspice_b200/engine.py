@@ -30,7 +30,7 @@ class HsInstance(ctypes.Structure):
     _fields_ = [('L', _lib.HsLattice), ('P', _lib.HsGridPlan), ('sw', _lib.HsSwitchList),
                 ('C', ctypes.c_void_p), ('scratch', ctypes.c_void_p), ('scratch_bytes', ctypes.c_int64),
                 ('steps', ctypes.c_int64), ('attempt_freq', ctypes.c_double), ('scheme', ctypes.c_int32),
-                ('pad', ctypes.c_int32)]
+                ('flags', ctypes.c_int32)]
 
 
 def _bind():
@@ -122,6 +122,49 @@ def plan_uniform_size(models, steps, n_sm, sizes=CLUSTER_SIZES, workers=None):
     return best
 
 
+def split_makespan(cluster_runs, cta_runs, n_clusters, cs):
+    """Makespan of a split launch (HS_INST_ONE_CTA): ``n_clusters`` clusters of ``cs`` CTAs
+    take the ``cluster_runs`` longest first; each cluster that finds no more of them splits,
+    and its CTAs take the ``cta_runs`` (run times on one CTA) longest first."""
+    import heapq
+    heap = [0.0] * max(1, n_clusters)
+    for d in sorted(cluster_runs, reverse=True):
+        heapq.heappush(heap, heapq.heappop(heap) + d)
+    ctas = [t for t in heap for _ in range(cs)]
+    heapq.heapify(ctas)
+    for d in sorted(cta_runs, reverse=True):
+        heapq.heappush(ctas, heapq.heappop(ctas) + d)
+    return max(ctas)
+
+
+def plan_split(models, steps, workers, sizes=CLUSTER_SIZES):
+    """Cluster size and per-instance mode of one launch: the k longest runs (by their time on
+    one CTA) use whole clusters of ``cs`` CTAs, the others one CTA each (the engine's split
+    mode). Every size and a grid of k (k = n: one size for all) are simulated with
+    :func:`split_makespan` over the modelled run times; ``workers[cs]`` is the number of
+    resident clusters of each size. Returns (cs, one_cta flags, modelled makespan in us)."""
+    t = model_time
+    n = len(models)
+    d1 = [st * t(m, 1) for m, st in zip(models, steps)]
+    order = sorted(range(n), key=lambda i: (-d1[i], i))
+    best = (lpt_makespan(d1, workers[1]), 1, n)
+    ks = sorted(set(range(0, n + 1, max(1, n // 64))) | {n})
+    for cs in sizes:
+        if cs == 1:
+            continue
+        dc = [st * t(m, cs) for m, st in zip(models, steps)]
+        for k in ks:
+            mk = split_makespan([dc[i] for i in order[:k]], [d1[i] for i in order[k:]], workers[cs], cs)
+            if mk < best[0] * 0.99:
+                best = (mk, cs, k)
+    mk, cs, k = best
+    flags = [False] * n
+    if cs > 1:
+        for i in order[k:]:
+            flags[i] = True
+    return cs, flags, mk
+
+
 def plan_sizes(models, steps, n_sm, max_cs=16):
     """Cluster sizes for a batch: start every instance on one CTA; an instance whose run is
     longer than the even share of the GPU (total SM time / SM count) gets twice the CTAs
@@ -150,6 +193,7 @@ class _Prepared:
     ws: int = 0         # dynamic shared workspace per CTA (bytes)
     order: list = None  # index into the engine's instance list of each launch slot
     ns: torch.Tensor = None   # device time (ns) of each launch slot, written by the launch
+    one_cta: int = 0    # instances that run on one CTA of a split cluster (HS_INST_ONE_CTA)
 
 
 def poisson_workspace(I: HsInstance) -> int:
@@ -265,17 +309,19 @@ class BatchEngine:
         return I, [buf, s]
 
     def _throughput_sizes(self, steps):
-        """Cluster sizes for throughput mode: one size for the launch (:func:`plan_uniform_size`
-        over the modelled step times)."""
-        n_sm = torch.cuda.get_device_properties(self.device).multi_processor_count
-        cs = plan_uniform_size([step_model(mm) for mm in self.magnets], [max(1, st) for st in steps], n_sm,
-                               workers={c: self._max(c) for c in CLUSTER_SIZES})
-        return [cs] * len(self.magnets)
+        """Cluster size and per-instance CTA mode for throughput mode: one launch whose longest
+        runs use whole clusters and whose others run on one CTA each (:func:`plan_split` over
+        the modelled step times)."""
+        cs, flags, _ = plan_split([step_model(mm) for mm in self.magnets], [max(1, st) for st in steps],
+                                  {c: self._max(c) for c in CLUSTER_SIZES})
+        return [cs] * len(self.magnets), flags
 
-    def _prepare(self, steps, kws, sizes=None, costs=None):
+    def _prepare(self, steps, kws, sizes=None, costs=None, one_cta=None):
         groups = {}
         keep = []
-        tsizes = self._throughput_sizes(steps) if (self.throughput and not self.cluster_size and not sizes) else None
+        tsizes = None
+        if one_cta is None and self.throughput and not self.cluster_size and not sizes:
+            tsizes, one_cta = self._throughput_sizes(steps)
         for j, (mm, st, kw) in enumerate(zip(self.magnets, steps, kws)):
             if mm._T_zero:
                 raise RuntimeError('an instance has T=0 somewhere in its domain')
@@ -285,23 +331,27 @@ class BatchEngine:
                 raise ValueError(f'cluster size {cs} not in {CLUSTER_SIZES}')
             I, k = self._describe_cached(mm, st, kw)
             keep += k
-            cost = costs[j] if costs is not None else st * step_time(mm, cs)
-            groups.setdefault(cs, []).append((cost, j, I))
+            alone = bool(one_cta and one_cta[j])
+            I.flags = _lib.HS_INST_ONE_CTA if alone else 0
+            cost = costs[j] if costs is not None else st * step_time(mm, 1 if alone else cs)
+            groups.setdefault(cs, []).append((alone, cost, j, I))
         out = []
         # the workspace only for groups with Poisson-disc instances: it takes L1 from the rest
         # largest clusters first (launched first, so the longest runs start first), and inside a
-        # group the longest runs first on the work counter (longest-processing-time order)
+        # group the longest runs first on the work counter (longest-processing-time order),
+        # the instances that run on one CTA after all that use whole clusters
         for cs, lst in sorted(groups.items(), reverse=True):
-            lst = sorted(lst, key=lambda e: (-e[0], e[1]))
-            order = [j for _, j, _ in lst]
-            lst = [I for _, _, I in lst]
+            lst = sorted(lst, key=lambda e: (e[0], -e[1], e[2]))
+            order = [j for _, _, j, _ in lst]
+            n_one = sum(1 for e in lst if e[0])
+            lst = [I for _, _, _, I in lst]
             arr = (HsInstance * len(lst))(*lst)
             raw = np.frombuffer(bytes(arr), dtype=np.uint8)
             # pinned staging + asynchronous copy on the current stream: no host synchronisation
             t = torch.from_numpy(raw.copy()).pin_memory().to(self.device, non_blocking=True)
             ws = max(poisson_workspace(I) for I in lst)
             out.append(_Prepared(t, len(lst), cs, keep, (ws + 1023) // 1024 * 1024, order,
-                                 torch.zeros(len(lst), dtype=torch.int64, device=self.device)))
+                                 torch.zeros(len(lst), dtype=torch.int64, device=self.device), n_one))
         return out
 
     def launch(self, prepared, stream=None):
@@ -341,11 +391,13 @@ class BatchEngine:
             left = [r - k for r, k in zip(left, c)]
         return out
 
-    def run(self, steps, sizes=None, resync_every: int = 0, costs=None, **kwargs):
+    def run(self, steps, sizes=None, resync_every: int = 0, costs=None, one_cta=None, **kwargs):
         """Enqueue ``steps`` (an int or one int per instance) update steps of every instance
         without the stop rule; asynchronous. ``sizes``: optional cluster size per instance;
         ``costs``: optional expected device time per instance, which orders the work counter
-        (longest first; default: the step-time model). Each returned group's ``ns`` holds the
+        (longest first; default: the step-time model); ``one_cta``: optional flag per instance,
+        run on one CTA of its group's clusters (HS_INST_ONE_CTA; the flagged instances of a
+        group are claimed after the others). Each returned group's ``ns`` holds the
         device time of each of its instances (launch slot ``order[i]``) once the launch ends.
         ``resync_every``: recompute the energies from the spins after every that many steps
         (one engine launch per stretch; the FP64 resync that bounds the drift of the FP32
@@ -354,7 +406,7 @@ class BatchEngine:
         if resync_every and resync_every > 0:
             prepared = None
             for c in self._chunks(steps, int(resync_every)):
-                prepared = self.run(c, sizes=sizes, costs=costs, **kwargs)
+                prepared = self.run(c, sizes=sizes, costs=costs, one_cta=one_cta, **kwargs)
                 for mm, k, total in zip(self.magnets, c, steps):
                     if k == int(resync_every):
                         mm.resync_energies()
@@ -364,9 +416,10 @@ class BatchEngine:
             mm._set_control(progress=0, done=0, t_max=float(kw.pop('t_max', math.inf)))
         key = (tuple(steps), tuple(sorted((k, float(v)) for k, v in kwargs.items() if k != 't_max')),
                tuple(mm._version for mm in self.magnets), tuple(id(mm) for mm in self.magnets),
-               tuple(sizes) if sizes else None, self.cluster_size, self.throughput)
+               tuple(sizes) if sizes else None, tuple(one_cta) if one_cta else None, self.cluster_size,
+               self.throughput)
         if self._cache is None or self._cache[0] != key:
-            self._cache = (key, self._prepare(steps, kws, sizes, costs))
+            self._cache = (key, self._prepare(steps, kws, sizes, costs, one_cta))
         prepared = self._cache[1]
         self.launch(prepared)
         return prepared

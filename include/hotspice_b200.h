@@ -179,8 +179,13 @@ typedef struct HsInstance {
                                    the most steps this launch makes (0: HS_PROGRESS_STEPS_MAX) */
     double       attempt_freq;
     int32_t      scheme;        /* HS_SCHEME_*                                                */
-    int32_t      pad;
+    int32_t      flags;         /* HS_INST_* bits                                             */
 } HsInstance;
+
+/* HsInstance.flags: run this instance on one CTA of its cluster. In a launch with clusters of
+ * more than one CTA, the first flagged instance a cluster claims splits it: from then on each
+ * of its CTAs claims and runs instances alone. List flagged instances after all others. */
+#define HS_INST_ONE_CTA 1
 
 /* ---- library ------------------------------------------------------------------------- */
 int hs_version(void);

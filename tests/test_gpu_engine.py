@@ -88,6 +88,31 @@ def test_batch_alone_equals_mixed():
         _assert_same(alone[i], _state(mixed[i]), f'{n} alone vs mixed')
 
 
+@pytest.mark.parametrize('cs', [2, 4])
+def test_split_clusters_equal_alone(cs, monkeypatch):
+    """A launch whose clusters split (HS_INST_ONE_CTA): the unflagged instances run on whole
+    clusters, the flagged ones on single CTAs, and every instance ends as it does alone."""
+    from hotspice_b200.engine import BatchEngine
+    names = ['neel_oop16', 'neel_pin16_perp', 'neel_kagome_perp', 'metro_oop16_single', 'wolff_oop32_pbc',
+             'neel_oop12x9_pbc', 'neel_oop16_exchange', 'neel_pin16_dimono']
+    steps = [90, 70, 60, 50, 20, 80, 40, 60]
+    flags = [False, True, False, True, True, False, True, True]
+    alone = []
+    for n, s in zip(names, steps):
+        mm = build_product(n)
+        BatchEngine([mm]).run(s)
+        alone.append(_state(mm))
+    mixed = [build_product(n) for n in names]
+    eng = BatchEngine(mixed, throughput=True)
+    monkeypatch.setattr(BatchEngine, '_throughput_sizes', lambda self, st: ([cs] * len(names), flags))
+    prepared = eng.run(steps)
+    assert len(prepared) == 1 and prepared[0].cs == cs
+    # flagged instances come last on the work counter
+    assert [flags[j] for j in prepared[0].order] == sorted(flags)
+    for i, n in enumerate(names):
+        _assert_same(alone[i], _state(mixed[i]), f'{n} cs={cs} one_cta={flags[i]}')
+
+
 def test_captured_graph_replays_equal_direct_launches():
     """A CUDA graph holding one engine launch (BatchEngine.capture) advances a mixed batch
     exactly like direct launches of the same steps."""

@@ -105,6 +105,31 @@ def test_plan_sizes():
     assert lpt_makespan([5, 4, 3, 3, 3], 2) == 10
 
 
+def test_plan_split():
+    """One launch whose long runs use whole clusters and whose short runs take one CTA each."""
+    from hotspice_b200.engine import lpt_makespan, model_time, plan_split, split_makespan
+    workers = {1: 148, 2: 74, 4: 37, 8: 18, 16: 9}
+    neel_big = (9.0, 600.0, 0.62)
+    neel_small = (9.0, 2.0, 0.62)
+    # two clusters of 2: cluster runs 10 and 6 on separate clusters, then the CTAs (free at
+    # 6, 6, 10, 10) take 5 and 4 (ending at 11 and 10), and the 3s end at 13
+    assert split_makespan([10, 6], [5, 4, 3, 3], 2, 2) == 13
+    # a few long runs among many short ones: the long ones use clusters, the rest one CTA
+    models = [neel_big] * 6 + [neel_small] * 400
+    steps = [2000] * 6 + [200] * 400
+    cs, flags, mk = plan_split(models, steps, workers)
+    assert cs > 1 and not any(flags[:6]) and all(flags[6:])
+    uniform = min(max(st * model_time(m, c) for m, st in zip(models, steps)) for c in (2, 4, 8, 16))
+    assert mk <= uniform
+    # equal short runs that fill the GPU: no worse than one CTA each
+    cs, flags, mk = plan_split([neel_small] * 600, [100] * 600, workers)
+    assert mk <= lpt_makespan([100 * model_time(neel_small, 1)] * 600, 148)
+    assert cs == 1 or sum(flags) >= 500
+    # a single long run: one wide cluster, nothing on one CTA
+    cs, flags, _ = plan_split([neel_big], [10**4], workers)
+    assert cs >= 8 and flags == [False]
+
+
 def test_fifo_latencies():
     lat = S.fifo_latencies([0.0, 0.1, 0.2], [0.5, 0.1, 0.1])
     assert np.allclose(lat, [0.5, 0.5, 0.5])
