@@ -363,6 +363,9 @@ def run_product(args):
     setup_s = time.perf_counter() - t_setup
     eng = BatchEngine(mms)
     S = args.mc_steps
+    # the launch plan (cluster size, which runs get whole clusters) measured on the device; the
+    # instances' state is restored afterwards
+    tune_cs, tune_k, tune_ms = eng.tune_split(S)
 
     # ---- device-resident throughput: one persistent launch per bench step, replayed from a
     # CUDA graph (BatchEngine.capture) ---------------------------------------------------------
@@ -499,7 +502,9 @@ def run_product(args):
                    "launch": "one persistent engine launch per bench step, replayed from a CUDA graph",
                    "parallelism": f"{ws} independent batches (one per GPU)" if ws > 1 else "one batch, one GPU",
                    "cluster_sizes": cluster_sizes,
-                   "instances_on_one_cta": one_cta, "switches": switches, "attempts": attempts,
+                   "instances_on_one_cta": one_cta,
+                   "launch_plan": f"autotuned (BatchEngine.tune_split): the {tune_k} longest runs on clusters of "
+                                  f"{tune_cs} CTAs, the rest on one CTA each ({tune_ms:.2f} ms per launch while tuning)", "switches": switches, "attempts": attempts,
                    "device_status_nonzero": sum(1 for s in status if s),
                    "near_threshold_decisions": near, "decisions": attempts,
                    "near_threshold_note": "decisions (Neel argmins, Metropolis acceptances) whose FP32 margin was "

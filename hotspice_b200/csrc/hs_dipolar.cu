@@ -368,6 +368,9 @@ dip_update_persist_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev,
             auto apply = [&](const SwInfo &w) {
                 if (w.sub >= 0 && !w.mode && !L.dip_wrap) {
                     const int64_t kb = (int64_t)w.sub * KH * KW + (L.dip_wx - w.x);
+                    // every VEC cells of the lane inside the window's columns (the common case
+                    // for windows wider than a lane): no per-cell column tests
+                    const bool inner = x0 >= w.x - L.dip_wx && x0 + VEC - 1 <= w.x + L.dip_wx && x0 + VEC - 1 < L.nx;
 #pragma unroll
                     for (int r = 0; r < UPD_RPW; ++r) {
                         if (r >= nrows) continue;
@@ -376,6 +379,25 @@ dip_update_persist_kernel(HsLattice L, HsSwitchList sw, const int32_t *n_sw_dev,
                         const bool rowin = dy >= -L.dip_wy && dy <= L.dip_wy;
                         const float *Kr = L.K + kb + (int64_t)(dy + L.dip_wy) * KW;
                         const float *Kpr = L.use_perp ? L.Kpo + kb + (int64_t)(dy + L.dip_wy) * KW : nullptr;
+                        if (inner) {
+                            touched |= ((1u << VEC) - 1u) << (r * VEC);
+                            if (!rowin) continue;
+                            float kv[VEC], kp[VEC];
+#pragma unroll
+                            for (int v = 0; v < VEC; ++v) kv[v] = __ldg(Kr + x0 + v);
+                            if (L.use_perp) {
+#pragma unroll
+                                for (int v = 0; v < VEC; ++v) kp[v] = __ldg(Kpr + x0 + v);
+                            }
+#pragma unroll
+                            for (int v = 0; v < VEC; ++v) {
+                                acc[r][v] += w.mm * kv[v];
+                                if (L.use_perp) accp[r][v] += w.mm * kp[v];
+                            }
+                            const int ds = w.x - x0;
+                            if (dy == 0 && ds >= 0 && ds < VEC) negate |= 1u << (r * VEC + ds);
+                            continue;
+                        }
 #pragma unroll
                         for (int v = 0; v < VEC; ++v) {
                             const int x = x0 + v;

@@ -260,6 +260,7 @@ class BatchEngine:
         self._work = torch.zeros(len(CLUSTER_SIZES), device=self.device, dtype=torch.int32)
         self._max_clusters = {}
         self._desc = {}     # id(mm) -> (version, kw key, HsInstance, buffers it points into)
+        self._tuned = None  # (step budgets, sizes, one-CTA flags) measured best by tune_split
 
     def set_magnets(self, magnets):
         """Replace the instance list (a serving loop changes it between launches); descriptors
@@ -270,6 +271,7 @@ class BatchEngine:
         live = {id(mm) for mm in self.magnets}
         self._desc = {k: v for k, v in self._desc.items() if k in live}
         self._cache = None
+        self._tuned = None
 
     def _max(self, cs):
         if cs not in self._max_clusters:
@@ -311,7 +313,9 @@ class BatchEngine:
     def _throughput_sizes(self, steps):
         """Cluster size and per-instance CTA mode for throughput mode: one launch whose longest
         runs use whole clusters and whose others run on one CTA each (:func:`plan_split` over
-        the modelled step times)."""
+        the modelled step times), or the plan :meth:`tune_split` measured for these budgets."""
+        if self._tuned is not None and self._tuned[0] == tuple(steps):
+            return list(self._tuned[1]), list(self._tuned[2])
         cs, flags, _ = plan_split([step_model(mm) for mm in self.magnets], [max(1, st) for st in steps],
                                   {c: self._max(c) for c in CLUSTER_SIZES})
         return [cs] * len(self.magnets), flags
@@ -374,6 +378,66 @@ class BatchEngine:
         n_clusters = min(p.n, self._max(p.cs))
         _lib.check(self.lib.hs_engine_run_ws(p.inst.data_ptr(), p.n, p.cs, n_clusters, self._work[g:].data_ptr(),
                                              p.ws, p.ns.data_ptr(), st), 'hs_engine_run_ws')
+
+    def tune_split(self, steps, reps: int = 2, sizes=(2, 4), ks=None, **kwargs):
+        """Measure split launches of throughput mode on the device and keep the fastest plan for
+        these step budgets (``run`` and ``capture`` use it until the instance list changes).
+        One launch with every instance on one CTA measures each instance's run time (the
+        engine's per-instance device time); the instances are ranked by it, and for each cluster
+        size in ``sizes`` and each k in ``ks`` the k longest run on whole clusters and the rest
+        on one CTA each, timed over ``reps`` launches after one warm-up launch. The instances'
+        state (spins, moments, energies, counters) is saved on the device first and restored
+        afterwards, so tuning leaves the simulations where they were. Returns (cluster size, k,
+        ms per launch) of the plan kept."""
+        n = len(self.magnets)
+        steps_l = [int(steps)] * n if np.isscalar(steps) else [int(x) for x in steps]
+        if ks is None:
+            ks = [k for k in (4, 8, 12, 16, 24, 32, 40, 48, 64, 96, 128, 192) if k < n] + [n]
+        stream = torch.cuda.current_stream(self.device)
+        stage, total = self._gather(self.STATE_FIELDS, stream.cuda_stream)
+        saved = stage[:total].clone()
+
+        def timed(cs, flags):
+            self._tuned = (tuple(steps_l), [cs] * n, [bool(f) for f in flags])
+            self._cache = None
+            prep = self.run(steps_l, **kwargs)
+            best = math.inf
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                prep = self.run(steps_l, **kwargs)
+                e1.record(stream)
+                e1.synchronize()
+                best = min(best, e0.elapsed_time(e1))
+            return best, prep
+
+        t_one, prep = timed(max(sizes), [True] * n)   # every instance on one CTA
+        d1 = np.zeros(n)
+        for p in prep:
+            ns = p.ns.cpu().numpy()
+            for slot, j in enumerate(p.order):
+                d1[j] = ns[slot]
+        order = np.argsort(-d1, kind='stable')
+        best = (t_one, max(sizes), 0)
+        for cs in sizes:
+            for k in ks:
+                flags = np.ones(n, dtype=bool)
+                flags[order[:k]] = False
+                t, _ = timed(cs, flags)
+                if t < best[0]:
+                    best = (t, cs, k)
+        t, cs, k = best
+        flags = np.ones(n, dtype=bool)
+        flags[order[:k]] = False
+        self._tuned = (tuple(steps_l), [cs] * n, [bool(f) for f in flags])
+        self._cache = None
+        segs, nseg, _, _ = self._segments(self.STATE_FIELDS)
+        _lib.check(self.lib.hs_segments_copy(saved.data_ptr(), segs.data_ptr(), nseg, 1, stream.cuda_stream),
+                   'hs_segments_copy')
+        stream.synchronize()
+        for mm in self.magnets:
+            mm._ctl = None
+        return cs, k, t
 
     def resync(self):
         """Recompute every instance's incrementally updated energies from its spins

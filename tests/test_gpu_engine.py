@@ -113,6 +113,28 @@ def test_split_clusters_equal_alone(cs, monkeypatch):
         _assert_same(alone[i], _state(mixed[i]), f'{n} cs={cs} one_cta={flags[i]}')
 
 
+def test_tune_split_leaves_state_and_results():
+    """tune_split runs timed launches of candidate plans, restores every instance's state, and
+    the tuned plan then gives the same results as an untuned run."""
+    from hotspice_b200.engine import BatchEngine
+    names = ['neel_oop16', 'neel_pin16_perp', 'metro_oop16_single', 'wolff_oop32_pbc', 'neel_oop12x9_pbc',
+             'neel_kagome_perp']
+    a = [build_product(n) for n in names]
+    b = [build_product(n) for n in names]
+    ea, eb = BatchEngine(a, throughput=True), BatchEngine(b, throughput=True)
+    ea.run(20)
+    eb.run(20)
+    before = [_state(x) for x in a]
+    cs, k, ms = ea.tune_split(30, reps=1, ks=[1, 3])
+    assert cs in (2, 4) and k in (0, 1, 3) and ms > 0
+    for n, x, s0 in zip(names, a, before):
+        _assert_same(s0, _state(x), f'{n} restored after tuning')
+    ea.run(30)
+    eb.run(30)
+    for n, x, y in zip(names, a, b):
+        _assert_same(_state(y), _state(x), f'{n} tuned vs untuned')
+
+
 def test_captured_graph_replays_equal_direct_launches():
     """A CUDA graph holding one engine launch (BatchEngine.capture) advances a mixed batch
     exactly like direct launches of the same steps."""
