@@ -952,7 +952,7 @@ HS_DEV float neel_cache_value(const HsLattice &L, double E, double Ep, double EB
 }
 
 #ifndef HS_NEEL_UNROLL
-#define HS_NEEL_UNROLL 4
+#define HS_NEEL_UNROLL 3
 #endif
 constexpr int NEEL_UNR = HS_NEEL_UNROLL;
 HS_DEV HsKeyIdx neel_scan_range(const HsLattice &L, int64_t start64, int64_t stride64, int64_t N64, uint64_t call,
