@@ -34,6 +34,9 @@ namespace {
 #ifndef HS_ENGINE_REGS
 #define HS_ENGINE_REGS 128
 #endif
+#ifndef HS_NEEL_WIN_UNROLL
+#define HS_NEEL_WIN_UNROLL 4
+#endif
 constexpr int ENG_NT = HS_ENGINE_THREADS;   // threads per CTA
 constexpr int ENG_MIN_CTAS = 65536 / (ENG_NT * HS_ENGINE_REGS);  // resident CTAs per SM at that register budget
 constexpr int ENG_SWCAP = 512;  // switches staged per CTA in shared memory
@@ -261,7 +264,7 @@ HS_DEV void update_one(const HsLattice &L, int sy, int sx, float smm, int8_t sm,
     const int total = nrows * ncols;
     const float pref2 = (float)(2.0 * L.dip_pref);
     const bool two = L.use_perp != 0;
-    constexpr int U = 4;
+    constexpr int U = HS_NEEL_WIN_UNROLL;   // window cells per thread per pass
     // window cell c = r ncols + q of this thread, advanced by nt cells per slot without divisions
     const int dr = nt / ncols, dq = nt - dr * ncols;
     int r0 = t0 / ncols, q0 = t0 - r0 * ncols;
