@@ -7,7 +7,9 @@ costs one launch instead of two or three kernel launches per step.
 
 Cluster sizes are chosen per instance by :func:`cluster_size_for` (a cost model on the
 lattice size and the dipolar window), or measured by :class:`Autotuner`, which times each
-candidate on the instance's own shape class and caches the winner.
+candidate on the instance's own shape class and caches the winner. A batch runs as one launch
+whose longest runs take whole clusters and whose others run on single CTAs of the clusters that
+split (:func:`plan_split` on the model, or :meth:`BatchEngine.tune_split` on the device).
 """
 from __future__ import annotations
 
@@ -648,12 +650,13 @@ class BatchEngine:
             ev.record(st)
             self._slot_free[slot] = ev
         if 'C' in in_fields:
-            raw = host_in.numpy()
-            for i, f, off, nb in lay:
-                if f == 'C':
-                    rec = np.frombuffer(raw[off:off + nb].tobytes(), dtype=_lib.COUNTERS_DTYPE)[0]
-                    self.magnets[i]._ctl = {'progress': int(rec['progress']), 'done': int(rec['done']),
-                                            't_max': float(rec['t_max'])}
+            # the loaded counters' run controls, read from the packed buffer in one gather
+            inst = [i for i, f, _, _ in lay if f == 'C']
+            offs = np.array([off for _, f, off, _ in lay if f == 'C'], dtype=np.int64)
+            recs = host_in.numpy()[offs[:, None] + np.arange(_lib.COUNTERS_DTYPE.itemsize)]
+            recs = recs.view(_lib.COUNTERS_DTYPE).ravel()
+            for i, p, d, t in zip(inst, recs['progress'].tolist(), recs['done'].tolist(), recs['t_max'].tolist()):
+                self.magnets[i]._ctl = {'progress': p, 'done': d, 't_max': t}
         prepared = self.run(steps, sizes=sizes, **kwargs)
         if host_out is not None:
             out_stage, out_total = self._gather(out_fields, st.cuda_stream)
