@@ -1026,13 +1026,25 @@ def run_served(dev, args, dist, rank, ws, sample=32):
     import torch
     from hotspice_b200 import serving as SV
     reqs = SV.request_stream(args.served, rate=200.0, seed=SEED)
-    mine = SV.shard_requests(reqs, ws, rank) if ws > 1 else reqs
+    dealer = None
+    if ws > 1 and args.served_placement == 'dynamic':
+        # run-time placement: each rank claims arrived requests while it holds the least work
+        import datetime
+        store = dist.TCPStore(os.environ.get('MASTER_ADDR', '127.0.0.1'), int(os.environ['MASTER_PORT']) + 1, ws,
+                              rank == 0, timeout=datetime.timedelta(seconds=120))
+        dealer = SV.RequestDealer(reqs, store, rank, ws)
+        mine = []
+    else:
+        mine = SV.shard_requests(reqs, ws, rank) if ws > 1 else reqs
     srv = SV.Server(device=dev)
     torch.cuda.synchronize(dev)
     torch.cuda.reset_peak_memory_stats(dev)
     if dist:
         dist.barrier()
-    res = srv.serve(mine, realtime=True)
+    res = srv.serve(mine, realtime=True, dealer=dealer)
+    if dealer is not None:   # the requests this rank served, for its one-at-a-time baseline
+        by_id = {r.rid: r for r in reqs}
+        mine = sorted((by_id[x.rid] for x in res), key=lambda r: r.arrival)
     torch.cuda.synchronize(dev)
     peak_alloc = torch.cuda.max_memory_allocated(dev)
     hist = np.asarray(srv.stats.history, dtype=float).reshape(-1, 7)
@@ -1090,6 +1102,7 @@ def run_served(dev, args, dist, rank, ws, sample=32):
     makespan = max(a['makespan'] for a in allst)
     seq_end = max(a['seq_end'] for a in allst)
     return {"workload": SERVED_WORKLOAD.format(k=args.served), "requests": int(lat.size),
+            "placement": args.served_placement if ws > 1 else "one rank",
             "value": att / makespan, "unit": UNIT, "makespan_s": makespan, "attempts": att,
             "arrivals_span_s": float(max(r.arrival for r in reqs)),
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
@@ -1167,6 +1180,9 @@ def main():
     ap.add_argument('--no-single', action='store_true')
     ap.add_argument('--served', type=int, default=2000, help='requests of the served arrival stream (0: skip)')
     ap.add_argument('--only-served', action='store_true', help='run only the served stream and print it')
+    ap.add_argument('--served-placement', default='static', choices=['static', 'dynamic'],
+                    help='with several ranks: a fixed split of the stream by estimated work (static), or '
+                         'requests claimed at run time by the least-loaded rank (dynamic)')
     ap.add_argument('--recompute-n', type=int, default=2048, help='lattice side of the full-recompute timing (0: skip)')
     ap.add_argument('--only-recompute', action='store_true', help='run only the full-recompute timing and print it')
     ap.add_argument('--incremental-n', type=int, default=2048, help='lattice side of the incremental-update timing (0: skip)')

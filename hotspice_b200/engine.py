@@ -391,6 +391,9 @@ class BatchEngine:
         state (spins, moments, energies, counters) is saved on the device first and restored
         afterwards, so tuning leaves the simulations where they were. Returns (cluster size, k,
         ms per launch) of the plan kept."""
+        if not self.throughput or self.cluster_size:
+            raise ValueError('tune_split plans throughput-mode launches: create the BatchEngine with '
+                             'throughput=True and no fixed cluster_size')
         n = len(self.magnets)
         steps_l = [int(steps)] * n if np.isscalar(steps) else [int(x) for x in steps]
         if ks is None:

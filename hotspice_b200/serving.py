@@ -17,7 +17,8 @@ Results do not depend on the mix: each instance draws its variates from its own 
 per-instance step sequence however the steps are cut into rounds and whichever cluster size
 runs them, so a request gives the same final state alone and in any mix.
 
-The scheduling policy (:class:`AdmissionQueue`, :func:`plan_quanta`, :func:`shard_requests`,
+The scheduling policy (:class:`AdmissionQueue`, :func:`plan_quanta`, :func:`shard_requests` and
+its run-time counterpart :class:`RequestDealer`,
 and the engine's :func:`~hotspice_b200.engine.plan_sizes`)
 is plain host code; the reference has no serving layer (its experiments call
 ``Magnets.progress`` in a loop, hotspice/core.py:736-760, one simulation at a time).
@@ -213,13 +214,80 @@ def shard_requests(requests, world_size, rank):
     load = [0.0] * world_size
     mine = []
     for r in requests:
-        ny, nx = geometry_shape(r.spec)
-        w = r.steps * float(nx * ny + 1089)
+        w = request_work(r)
         k = min(range(world_size), key=lambda j: (load[j], j))
         load[k] += w
         if k == rank:
             mine.append(r)
     return mine
+
+
+def request_work(r) -> float:
+    """Estimated device work of a request (the unit :func:`shard_requests` balances)."""
+    ny, nx = geometry_shape(r.spec)
+    return r.steps * float(nx * ny + 1089)
+
+
+class RequestDealer:
+    """Placement of a shared arrival stream at run time (one dealer per rank, over a
+    ``torch.distributed`` key-value store that all ranks share). Requests are dealt in arrival
+    order: when the next undealt request has arrived, the rank whose published load (the
+    estimated work it still holds, :func:`request_work` units) is the smallest claims it, by a
+    compare-and-set on the shared index; a request that has waited ``grace_s`` is claimed by
+    whichever rank polls first, so a rank busy in a long round delays nobody. A rank that falls
+    behind its estimate (a long request, a slow lattice) keeps a high load and receives nothing
+    until it has worked it off. Store round trips are limited to one poll per ``poll_s``. The
+    shared index is stored as "index:claimer", so a compare-and-set that another rank won can
+    never look like this rank's own. Use a fresh ``prefix`` for every stream on a store."""
+
+    def __init__(self, requests, store, rank, world_size, prefix='hs_dealer', grace_s=0.02, poll_s=1e-3):
+        self.reqs = sorted(requests, key=lambda r: (r.arrival, r.rid))
+        self.store, self.rank, self.world = store, int(rank), int(world_size)
+        self.prefix, self.grace_s, self.poll_s = prefix, float(grace_s), float(poll_s)
+        self.next = 0            # the shared index, as last read
+        self._last_poll = -math.inf
+        if self.rank == 0:
+            store.set(f'{prefix}/next', '0:-1')
+        store.set(f'{prefix}/load{self.rank}', '0')
+        for q in range(self.world):   # every rank's load key exists before anyone reads it
+            store.wait([f'{prefix}/load{q}'])
+        store.wait([f'{prefix}/next'])
+
+    def _get(self, key) -> str:
+        return self.store.get(f'{self.prefix}/{key}').decode()
+
+    def exhausted(self) -> bool:
+        """Every request has been dealt (as last read from the store)."""
+        return self.next >= len(self.reqs)
+
+    def claim(self, now: float, load: float, force: bool = False) -> list:
+        """The requests this rank takes at time ``now`` (s after the start of the stream;
+        ``math.inf`` when every request is present from the start), given its current ``load``;
+        publishes the load. Reads the store at most once per ``poll_s`` unless ``force``."""
+        t = time.perf_counter()
+        if self.exhausted() or (not force and t - self._last_poll < self.poll_s):
+            return []
+        self._last_poll = t
+        self.store.set(f'{self.prefix}/load{self.rank}', repr(float(load)))
+        out = []
+        while True:
+            val = self._get('next')
+            self.next = int(val.split(':')[0])
+            if self.next >= len(self.reqs) or self.reqs[self.next].arrival > now:
+                break
+            r = self.reqs[self.next]
+            # the least-loaded rule (no grace without a clock: all requests present at once)
+            if self.world > 1 and (math.isinf(now) or now - r.arrival < self.grace_s):
+                loads = [float(self._get(f'load{q}')) for q in range(self.world)]
+                if min(range(self.world), key=lambda q: (loads[q], q)) != self.rank:
+                    break
+            mine = f'{self.next + 1}:{self.rank}'
+            if self.store.compare_set(f'{self.prefix}/next', val, mine).decode() == mine:
+                out.append(r)
+                self.next += 1
+                load += request_work(r)
+                self.store.set(f'{self.prefix}/load{self.rank}', repr(float(load)))
+        return out
 
 
 @dataclass(eq=False)
@@ -403,11 +471,14 @@ class Server:
                          t=float(c['t']), E_tot=r['E_tot'], m_avg=r['m_avg'], state=r['state'])
 
     # -- the loop ----------------------------------------------------------------------
-    def serve(self, requests, realtime=True) -> list[SimResult]:
+    def serve(self, requests, realtime=True, dealer: RequestDealer | None = None) -> list[SimResult]:
         """Serve ``requests`` (arrival times relative to now when ``realtime``; otherwise all
-        are present at the start). Returns one SimResult per request, in completion order."""
+        are present at the start). With a ``dealer`` (several ranks serving one stream), the
+        requests come from it instead: this rank claims arrived requests while its held work is
+        the smallest (``requests`` is then ignored). Returns one SimResult per request, in
+        completion order."""
         torch = self.torch
-        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        pending = deque(sorted(requests, key=lambda r: r.arrival)) if dealer is None else deque()
         queue = AdmissionQueue()
         active: list[_Active] = []
         inflight: deque = deque()
@@ -457,6 +528,11 @@ class Server:
             now = clock()
             while pending and (not realtime or pending[0].arrival <= now):
                 queue.push(pending.popleft())
+            if dealer is not None and not dealer.exhausted():
+                held = sum(a.remaining * request_work(a.req) / max(1, a.req.steps) for a in active) + \
+                    sum(request_work(r) for r in queue.waiting) + sum(request_work(r) for r, _, _ in building)
+                for r in dealer.claim(now if realtime else math.inf, held):
+                    queue.push(r)
             changed = False
             if queue:
                 reserved = sum(a.bytes for a in active) + sum(b for _, b, _ in building) + \
@@ -478,14 +554,18 @@ class Server:
             st.admitted_bytes_peak = max(st.admitted_bytes_peak, used_bytes)
             return changed
 
-        while pending or queue or active or inflight or building or retiring:
+        def dealing():
+            return dealer is not None and not dealer.exhausted()
+
+        while pending or dealing() or queue or active or inflight or building or retiring:
             admit()
             collect()
             runnable = [a for a in active if a.remaining > 0]
             if runnable and len(inflight) < self.max_inflight:
                 # short rounds while requests still arrive (they join at round boundaries),
                 # longer ones once the stream has ended
-                rms = self.round_ms if (pending or queue or building) else max(self.round_ms, self.tail_round_ms)
+                rms = self.round_ms if (pending or dealing() or queue or building) else \
+                    max(self.round_ms, self.tail_round_ms)
                 inflight.append(self._launch_round(runnable, rms))
                 st.rounds += 1
                 st.max_active = max(st.max_active, len(runnable))
@@ -529,6 +609,8 @@ class Server:
                                    f'HBM budget of {self.hbm_budget} (or max_slots={self.max_slots} is 0)')
             if pending and realtime:
                 time.sleep(max(0.0, min(1e-3, pending[0].arrival - clock())))
+            elif dealing():
+                time.sleep(2e-4)
         st.makespan = clock()
         return results
 

@@ -2,6 +2,7 @@
 FIFO latency model, the seeded request stream, and the per-rank sharding of the stream,
 including a two-rank gloo run that checks the ranks agree on a disjoint, complete split."""
 import os
+import time
 import socket
 
 import numpy as np
@@ -179,6 +180,63 @@ def test_shard_requests_two_ranks_gloo():
     assert not (a & b)
     assert a | b == set(range(200))
     assert abs(len(a) - len(b)) < 100
+
+
+def _dealer_stream():
+    """120 equal requests, one every millisecond."""
+    return [S.SimRequest(i, dict(lattice='OOP_Square', n=64, T=300.0, seed=i), 1000, 1e-3 * i) for i in range(120)]
+
+
+def _dealer_main(rank, world, port, drain, realtime, out):
+    """One rank of a simulated serving run: held work drains at ``drain[rank]`` requests per
+    second of the shared clock, and the rank claims arrived requests through a RequestDealer
+    on a shared TCPStore."""
+    import datetime
+    os.environ.update(MASTER_ADDR='127.0.0.1', MASTER_PORT=str(port))
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        store = dist.TCPStore('127.0.0.1', port + 1, world, rank == 0, timeout=datetime.timedelta(seconds=60))
+        reqs = _dealer_stream()
+        unit = S.request_work(reqs[0])
+        dealer = S.RequestDealer(reqs, store, rank, world, grace_s=0.02, poll_s=0.0)
+        dist.barrier()
+        t0 = last = time.perf_counter()
+        held, got = 0.0, []
+        while not dealer.exhausted() or held > 0:
+            t = time.perf_counter()
+            held = max(0.0, held - drain[rank] * unit * (t - last))
+            last = t
+            for r in dealer.claim(t - t0 if realtime else float('inf'), held):
+                got.append(r.rid)
+                held += S.request_work(r)
+            time.sleep(2e-4)
+        gathered = [None] * world
+        dist.all_gather_object(gathered, got)
+        if rank == 0:
+            out.put(gathered)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize('realtime', [True, False])
+def test_request_dealer_two_ranks_gloo(realtime):
+    """Run-time placement over two gloo ranks: every request is dealt exactly once, each rank
+    receives its requests in arrival order, and the rank that works its load off ten times
+    faster receives more of them."""
+    ctx = mp.get_context('spawn')
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_dealer_main, args=(r, 2, port, [500.0, 50.0], realtime, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    gathered = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    a, b = gathered
+    assert sorted(a + b) == list(range(120))
+    assert a == sorted(a) and b == sorted(b)
+    assert len(a) > len(b)
 
 
 def test_segment_table_covers_packed_layout():
