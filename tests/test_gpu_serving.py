@@ -95,3 +95,23 @@ def test_building_a_request_does_not_synchronise():
     torch.cuda.synchronize()
     for mm in built:   # and the instances are complete: a summary reads back normally
         assert np.isfinite(mm.E_tot)
+
+
+def test_served_through_a_dealer_equals_alone():
+    """Server.serve with a RequestDealer (one rank on a local store) serves every request of
+    the stream, each with the same result as alone."""
+    import datetime
+    import socket
+    import torch.distributed as dist
+    reqs = _requests()
+    alone = {r.rid: S.Server(keep_state=True).serve([r], realtime=False)[0] for r in reqs}
+    with socket.socket() as s:
+        s.bind(('127.0.0.1', 0))
+        port = s.getsockname()[1]
+    store = dist.TCPStore('127.0.0.1', port, 1, True, timeout=datetime.timedelta(seconds=60))
+    dealer = S.RequestDealer(reqs, store, 0, 1)
+    srv = S.Server(keep_state=True, round_ms=0.05)
+    got = {r.rid: r for r in srv.serve([], realtime=True, dealer=dealer)}
+    assert sorted(got) == [r.rid for r in reqs]
+    for r in reqs:
+        _check_same(got[r.rid], alone[r.rid])
