@@ -35,6 +35,9 @@ namespace {
 #ifndef HS_UPD_SCAN
 #define HS_UPD_SCAN 2
 #endif
+#ifndef HS_UPD_PERSIST_MIN_TILES
+#define HS_UPD_PERSIST_MIN_TILES 296   // two tiles per SM of a B200 (148 SMs)
+#endif
 constexpr int UPD_WARPS = HS_UPD_WARPS;            // warps per CTA
 constexpr int UPD_RPW = HS_UPD_RPW;                // rows per warp
 constexpr int UPD_TY = UPD_WARPS * UPD_RPW;        // rows per tile
@@ -595,9 +598,12 @@ int hs_launch_dipolar_update(const HsLattice &L, const HsSwitchList &sw, const i
     const int TX = vec ? 128 : 32;
     const int tiles = ((L.nx + TX - 1) / TX) * ((L.ny + UPD_TY - 1) / UPD_TY);
     // a list that fits the shared-memory staging goes to the persistent kernel (a device-side
-    // count is bounded by the list's capacity)
+    // count is bounded by the list's capacity) when the lattice has tiles for at least two
+    // waves; smaller lattices give each CTA one tile, where the per-tile kernel's list scan
+    // costs less than staging the whole list in every CTA (512^2 pinwheel, Metropolis grid
+    // r = 20a: 14.6 -> 13.1 us per step)
     const int most = n_sw_dev ? sw.cap : n_host;
-    if (most <= UPD_PLOC && tiles <= 1 << 20) {
+    if (most <= UPD_PLOC && tiles <= 1 << 20 && tiles >= HS_UPD_PERSIST_MIN_TILES) {
         const int cap = std::max(most, 1);
         return vec ? launch_persist<4>(L, sw, n_sw_dev, n_host, semantics, C, tiles, cap, st)
                    : launch_persist<1>(L, sw, n_sw_dev, n_host, semantics, C, tiles, cap, st);
