@@ -56,7 +56,9 @@ def step_model(mm: Magnets) -> tuple[float, float, float]:
     part grows like c N^beta with the lattice's occupancy class (dense / half / sparse, which
     also carries the perpendicular channel of the in-plane lattices), Néel scans spread over the
     cluster like cs^0.62 and Metropolis steps like cs^0.5; a Wolff step grows its cluster on one
-    CTA and costs 10-17 us above the critical temperature."""
+    CTA and costs 10-17 us above the critical temperature. Inside a full batch the model ranks
+    runs less well (it underestimates how much two CTAs speed up a large Néel scan), so a
+    batch's launch plan is best measured (:meth:`BatchEngine.tune_split`)."""
     n = mm.nx * mm.ny
     f = mm.n / max(n, 1)
     cls = 0 if f >= 0.75 else (1 if f >= 0.45 else 2)
@@ -416,32 +418,38 @@ class BatchEngine:
                 best = min(best, e0.elapsed_time(e1))
             return best, prep
 
-        t_one, prep = timed(max(sizes), [True] * n)   # every instance on one CTA
-        d1 = np.zeros(n)
-        for p in prep:
-            ns = p.ns.cpu().numpy()
-            for slot, j in enumerate(p.order):
-                d1[j] = ns[slot]
-        order = np.argsort(-d1, kind='stable')
-        best = (t_one, max(sizes), 0)
-        for cs in sizes:
-            for k in ks:
-                flags = np.ones(n, dtype=bool)
-                flags[order[:k]] = False
-                t, _ = timed(cs, flags)
-                if t < best[0]:
-                    best = (t, cs, k)
-        t, cs, k = best
-        flags = np.ones(n, dtype=bool)
-        flags[order[:k]] = False
-        self._tuned = (tuple(steps_l), [cs] * n, [bool(f) for f in flags])
-        self._cache = None
-        segs, nseg, _, _ = self._segments(self.STATE_FIELDS)
-        _lib.check(self.lib.hs_segments_copy(saved.data_ptr(), segs.data_ptr(), nseg, 1, stream.cuda_stream),
-                   'hs_segments_copy')
-        stream.synchronize()
-        for mm in self.magnets:
-            mm._ctl = None
+        reps = max(1, int(reps))
+        try:
+            t_one, prep = timed(max(sizes), [True] * n)   # every instance on one CTA
+            d1 = np.zeros(n)
+            for p in prep:
+                ns = p.ns.cpu().numpy()
+                for slot, j in enumerate(p.order):
+                    d1[j] = ns[slot]
+            order = np.argsort(-d1, kind='stable')
+            best = (t_one, max(sizes), 0)
+            for cs in sizes:
+                for k in ks:
+                    flags = np.ones(n, dtype=bool)
+                    flags[order[:k]] = False
+                    t, _ = timed(cs, flags)
+                    if t < best[0]:
+                        best = (t, cs, k)
+            t, cs, k = best
+            flags = np.ones(n, dtype=bool)
+            flags[order[:k]] = False
+            self._tuned = (tuple(steps_l), [cs] * n, [bool(f) for f in flags])
+        except BaseException:
+            self._tuned = None
+            raise
+        finally:   # the instances' state as it was before tuning, whatever happened
+            self._cache = None
+            segs, nseg, _, _ = self._segments(self.STATE_FIELDS)
+            _lib.check(self.lib.hs_segments_copy(saved.data_ptr(), segs.data_ptr(), nseg, 1, stream.cuda_stream),
+                       'hs_segments_copy')
+            stream.synchronize()
+            for mm in self.magnets:
+                mm._ctl = None
         return cs, k, t
 
     def resync(self):
