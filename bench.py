@@ -497,6 +497,9 @@ def run_product(args):
     c3 = None
     if rank == 0 and args.c3_steps > 0:
         c3 = run_c3(dev, n=args.c3_n, steps=args.c3_steps)
+    c1_run = None
+    if rank == 0 and args.c1_steps > 0:
+        c1_run = run_c1(dev, stream, steps=args.c1_steps, cpu_seconds=0.0 if args.no_cpu_baseline else 5.0)
     reservoir = None
     if rank == 0 and args.reservoir_n > 0:
         reservoir = run_reservoir(dev, n=args.reservoir_n, cpu_seconds=0.0 if args.no_cpu_baseline else 10.0)
@@ -560,6 +563,8 @@ def run_product(args):
         line["reservoir"] = reservoir
     if c3 is not None:
         line["c3_poisson_resync"] = c3
+    if c1_run is not None:
+        line["c1_neel"] = c1_run
     if not args.no_cpu_baseline:
         v, secs, st, ni = oracle_sample(specs, seconds_per_instance=args.cpu_seconds)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
@@ -1139,6 +1144,51 @@ def _counters_dtype():
     return _lib.COUNTERS_DTYPE
 
 
+C1_WORKLOAD = ("OOP_Square 64x64 (4096 magnets), a=200nm, moment=1.1e-15, E_B=5e-20 J uniform, T=300K, DipolarEnergy "
+               "with the full untruncated kernel, iid +-1 start (p=0.5, seeded), Neel-Arrhenius single switches, "
+               "{steps} steps (FP32 increments into FP64 energies, FP64 simulated time)")
+
+
+def run_c1(dev, stream, steps=10000, cpu_seconds=5.0):
+    """The c1 workload: one 64 x 64 OOP square lattice with the full dipolar kernel, `steps`
+    Néel steps through Magnets.run on its autotuned single-instance path, timed with CUDA
+    events; beside it the NumPy oracle on the same lattice for a bounded sample of steps."""
+    import torch
+    import hotspice_b200 as hs
+    from hotspice_b200.engine import Autotuner
+    from oracle.geometry import oop_square
+    from oracle.hotspice_oracle import OracleDipolar, OracleMagnets
+    g = np.random.Generator(np.random.PCG64(SEED + 11))
+    m0 = g.integers(0, 2, size=(64, 64)) * 2 - 1
+    mm = hs.ASI.OOP_Square(200e-9, 64, T=300.0, E_B=5e-20, moment=1.1e-15, pattern=m0, energies=[hs.DipolarEnergy()],
+                           seed=SEED + 11, device=dev)
+    choice = Autotuner().tune(mm, steps=200, include_step_kernels=True)
+    mm.run(1000)
+    torch.cuda.synchronize(dev)
+    a0, s0 = mm.attempted_switches, mm.switches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    mm.run(steps)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    att = mm.attempted_switches - a0
+    mo = OracleMagnets(oop_square(200e-9, 64), m0, T=300.0, E_B=5e-20, moment=1.1e-15, energies=[OracleDipolar()],
+                       seed=SEED + 11)
+    mo.update()
+    k, t0 = 0, time.perf_counter()
+    while k < steps and time.perf_counter() - t0 < cpu_seconds:
+        mo.update()
+        k += 1
+    cpu_s = time.perf_counter() - t0
+    return {"workload": C1_WORKLOAD.format(steps=steps), "steps": steps, "ms": ms, "us_per_step": ms * 1e3 / steps,
+            "value": att / (ms * 1e-3), "unit": UNIT, "switches": int(mm.switches - s0),
+            "path": "per-step kernels (CUDA graphs)" if choice == 0 else f"engine cluster {choice}",
+            "cpu_baseline": {"value": k / cpu_s, "unit": UNIT, "cores": 1, "kind": "port",
+                             "sample": f"{k} Neel steps of the same lattice with the NumPy oracle ({cpu_s:.1f} s)"},
+            "gpu_over_cpu": (att / (ms * 1e-3)) / (k / cpu_s)}
+
+
 def run_single(dev, stream):
     """The 512 x 512 pinwheel instance, best single-instance path chosen by measurement."""
     import torch
@@ -1194,6 +1244,8 @@ def main():
     ap.add_argument('--c3-n', type=int, default=2048, help='lattice side of the Poisson-disc / resync workload')
     ap.add_argument('--c3-steps', type=int, default=5000, help='steps per temperature of that workload (0: skip)')
     ap.add_argument('--only-c3', action='store_true', help='run only the Poisson-disc / resync workload and print it')
+    ap.add_argument('--c1-steps', type=int, default=10000, help='Neel steps of the 64x64 full-kernel workload (0: skip)')
+    ap.add_argument('--only-c1', action='store_true', help='run only the 64x64 full-kernel Neel workload and print it')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)
@@ -1217,6 +1269,11 @@ def main():
         dev = torch.device('cuda', 0)
         torch.cuda.set_device(dev)
         print(json.dumps({"served": run_served(dev, args, None, 0, 1)}))
+    elif args.only_c1:
+        import torch
+        dev = torch.device('cuda', 0)
+        torch.cuda.set_device(dev)
+        print(json.dumps({"c1_neel": run_c1(dev, torch.cuda.current_stream(dev), steps=args.c1_steps)}))
     elif args.only_c3:
         import torch
         dev = torch.device('cuda', 0)
