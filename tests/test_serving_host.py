@@ -218,6 +218,20 @@ def _dealer_main(rank, world, port, drain, realtime, out):
         dist.destroy_process_group()
 
 
+def test_request_dealer_one_rank_follows_arrivals():
+    """One rank on a local store: arrived requests are dealt in arrival order and nothing that
+    has not arrived yet; the shared index records the claimer."""
+    import datetime
+    store = dist.TCPStore('127.0.0.1', _free_port(), 1, True, timeout=datetime.timedelta(seconds=30))
+    reqs = _dealer_stream()[:10]
+    d = S.RequestDealer(list(reversed(reqs)), store, 0, 1, poll_s=0.0)
+    assert [r.rid for r in d.claim(0.0035, 0.0)] == [0, 1, 2, 3]
+    assert d.claim(0.0035, 0.0) == [] and not d.exhausted()
+    assert [r.rid for r in d.claim(1.0, 0.0)] == list(range(4, 10))
+    assert d.exhausted() and store.get('hs_dealer/next').decode() == '10:0'
+    assert d.claim(2.0, 0.0) == []
+
+
 @pytest.mark.parametrize('realtime', [True, False])
 def test_request_dealer_two_ranks_gloo(realtime):
     """Run-time placement over two gloo ranks: every request is dealt exactly once, each rank
